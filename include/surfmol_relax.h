@@ -1,0 +1,199 @@
+/* surfmol_relax.h -- C ABI of the B200 multi-system UFF + GridFF FIRE relaxation library.
+ *
+ * One handle = one CUDA device + one stream; not thread-safe (callers serialise).
+ * The library owns device memory; the caller owns every host array.  Every
+ * function returns an int status (SMR_OK = 0, negative on error) and never
+ * aborts; smr_last_error() gives the message of the last failure.
+ *
+ * Reference interfaces each entry point replaces (paths inside ProkopHapala/SurfMol):
+ *   handle lifecycle ........ crates/libs/oclff/src/rrsp3.rs:742 (RRsp3Multi::new), :1085 (finish),
+ *                             crates/libs/molff/src/ffi_uff.rs:42,82 (uff_new / uff_free)
+ *   grid .................... crates/libs/oclff/src/surfff.rs:187-221 (GridFFBuildOcl / GridFFEvalOcl),
+ *                             opencl/gridff_build.cl:350-463, opencl/Surface.cl:716-906 (builders),
+ *                             opencl/UFF.cl:1524-1545 (BsplinePLQ, grid_ns, grid_invStep, grid_p0 arguments)
+ *   molecules / topology .... crates/libs/molff/src/ffi_uff.rs:42-80 (uff_new: elements + positions ->
+ *                             topology, UFF typing and parameters), crates/libs/molff/src/uff.rs:699-887
+ *   systems ................. crates/libs/oclff/src/rrsp3.rs:936 (upload_state_multi)
+ *   relaxation .............. crates/apps/molengine/src/main.rs:237-277 (relax_fire),
+ *                             crates/libs/molff/src/ffi_uff.rs:133 (uff_relax),
+ *                             crates/libs/oclff/src/rrsp3.rs:1028 (step_cluster_multi)
+ *   evaluation .............. crates/libs/molff/src/ffi_uff.rs:96 (uff_eval),
+ *                             crates/libs/surfmol/src/mol_world.rs:60-86 (eval_forces)
+ *   read-back ............... crates/libs/oclff/src/rrsp3.rs:976,991 (download_pos_multi / _replica),
+ *                             crates/libs/molff/src/ffi_uff.rs:109 (uff_get_pos)
+ */
+#ifndef SURFMOL_RELAX_H
+#define SURFMOL_RELAX_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SMR_OK               0
+#define SMR_ERR_ARG         -1   /* invalid argument (null pointer, bad size, bad id) */
+#define SMR_ERR_CUDA        -2   /* CUDA runtime error */
+#define SMR_ERR_CAPACITY    -3   /* slot / atom capacity or per-system size limit exceeded */
+#define SMR_ERR_STATE       -4   /* call out of order (e.g. relax before a grid is set) */
+#define SMR_ERR_UNSUPPORTED -5   /* option not implemented */
+#define SMR_ERR_TIMEOUT     -6   /* device work did not finish within the watchdog limit */
+
+/* per-system status word written by relaxation */
+#define SMR_ST_RUNNING    0      /* steps remain, not converged */
+#define SMR_ST_CONVERGED  1      /* max|F| < fconv */
+#define SMR_ST_MAXSTEPS   2      /* step budget of the system used up */
+#define SMR_ST_NONFINITE  3      /* a force or position became NaN/Inf; the system stopped */
+
+#define SMR_GRID_F32   0         /* float4 coefficients */
+#define SMR_GRID_F16   1         /* 4 x binary16, value = stored * scale[channel] */
+#define SMR_GRID_BF16  2         /* 4 x bfloat16, value = stored * scale[channel] */
+
+#define SMR_MODE_BATCHED 0       /* persistent kernel, all active systems, dynamic system scheduling */
+#define SMR_MODE_PLAIN   1       /* one launch per system per FIRE step, status read back each step */
+
+/* energy components returned per system (physical totals: each bond and NB pair once) */
+#define SMR_E_TOTAL 0
+#define SMR_E_BOND  1
+#define SMR_E_ANGLE 2
+#define SMR_E_DIH   3
+#define SMR_E_INV   4
+#define SMR_E_NB    5
+#define SMR_E_GRID  6
+#define SMR_E_NCOMP 8
+
+typedef struct smr_handle smr_handle;
+
+typedef struct {
+    int       device;        /* CUDA device ordinal */
+    int       max_systems;   /* slot capacity */
+    long long max_atoms;     /* atom capacity summed over all slots */
+    int       reserved[6];
+} smr_config;
+
+/* FIRE parameters: FireState (crates/libs/molff/src/raff.rs:1040-1062) + relax_fire's
+ * dt0/dt_max/fconv (crates/apps/molengine/src/main.rs:237).  flimit <= 0: no force clamp. */
+typedef struct {
+    double dt0, dt_max, alpha0, f_inc, f_dec, f_alpha;
+    int    n_min;
+    double fconv;
+    double flimit;
+} smr_fire_params;
+
+/* Non-bonded / grid-coupling parameters: GFFParams.x (rdamp), GFFParams.y (Morse alpha)
+ * of opencl/UFF.cl:1534-1545; rcut <= 0 keeps every intramolecular pair. */
+typedef struct {
+    float rdamp;
+    float alpha_morse;
+    float rcut;
+    int   reserved;
+} smr_nb_params;
+
+/* Grid build: Morse (Pauli, London) image sums + Ewald-2D Coulomb, exact B-spline fit. */
+typedef struct {
+    double alpha_morse;      /* Morse exponent of the substrate channels */
+    int    npbc;             /* lateral images each side for the Morse sums (make_MorseFF nPBC) */
+    double ewald_tol;        /* relative truncation of the reciprocal sum, e.g. 1e-12 */
+    int    dtype;            /* SMR_GRID_* storage of the result */
+    double morse_rcut;       /* <= 0: full image sum; > 0: skip ions farther than this (A) */
+    int    reserved[4];
+} smr_grid_build_params;
+
+/* Explicit topology (callers doing their own typing); local atom indices. */
+typedef struct {
+    int           natoms;
+    const double* req;       /* natoms x 4: R_vdW, sqrt(E_vdW), Q, H */
+    const int*    neighs;    /* natoms x 4, -1 padded */
+    const double* bond_kl;   /* natoms x 4 x 2: (k, l0) of the bond in each neighbour slot */
+    int nang;  const int* angs;  const double* angp;   /* nang x 3 (i, j centre, k); nang x 5 (K, c0..c3) */
+    int ndih;  const int* dihs;  const double* dihp;   /* ndih x 4; ndih x 3 (V, d, n) */
+    int ninv;  const int* invs;  const double* invp;   /* ninv x 4 (centre first); ninv x 4 (K, c0, c1, c2) */
+} smr_topology_desc;
+
+int         smr_create(const smr_config* cfg, smr_handle** out);
+int         smr_destroy(smr_handle* h);
+const char* smr_last_error(const smr_handle* h);
+const char* smr_version(void);
+
+int smr_set_nb_params(smr_handle* h, const smr_nb_params* p);
+
+/* Substrate grid: coef is a HOST array of nx*ny*nz*4 values (float for F32, uint16 for F16/BF16)
+ * in z-fastest order i = iz + nz*(iy + ny*ix), channels (Pauli, London, Coulomb, H).
+ * scale multiplies each stored channel (use 1 for F32). */
+int smr_set_grid(smr_handle* h, const void* coef, int dtype, const float scale[4],
+                 int nx, int ny, int nz, const double p0[3], const double step[3]);
+int smr_get_grid(smr_handle* h, void* coef_out, int* dtype, float scale[4], int dims[3], double p0[3], double step[3]);
+/* Build on the device from ions (x, y, z, q) and their Morse (R, sqrt(E)); the slab is periodic
+ * in an orthogonal Lx x Ly cell and lies entirely below p0[2]. */
+int smr_build_grid(smr_handle* h, int nions, const double* ions, const double* ion_re, double Lx, double Ly,
+                   int nx, int ny, int nz, const double p0[3], const double step[3],
+                   const smr_grid_build_params* p);
+/* Re-encode the current grid to another storage dtype with per-channel scales (max|c| mapping). */
+int smr_convert_grid(smr_handle* h, int dtype);
+
+/* Molecule -> bonds by cutoff, UFF typing, terms and parameters (host, native), upload. */
+int smr_add_molecule(smr_handle* h, int natoms, const int* Z, const double* pos, const double* charges,
+                     double bond_cut, int* topo_id);
+int smr_add_topology(smr_handle* h, const smr_topology_desc* d, int* topo_id);
+/* counts[6] = natoms, nbonds, nang, ndih, ninv, type-rounds (schedule length) */
+int smr_topology_counts(smr_handle* h, int topo_id, int counts[6]);
+/* Any output pointer may be null.  Layouts as the arrays of smr_topology_desc plus
+ * neighBs (natoms x 4 bond index), bonds (nbonds x 2), bparams (nbonds x 2), type ids (natoms). */
+int smr_topology_export(smr_handle* h, int topo_id, int* neighs, int* neighBs, int* bonds, double* bparams,
+                        int* angs, int* ang_ngs, double* angp, int* dihs, int* dih_ngs, double* dihp,
+                        int* invs, int* inv_ngs, double* invp, double* req, int* type_id);
+const char* smr_type_name(int type_id);
+
+/* Host-only molecule preparation (no device needed): the same pipeline smr_add_molecule
+ * runs, exposed so callers can inspect or cache topologies.  smr_topo_rounds packs the
+ * bonded terms into device rounds for a team size: rounds[3] = (angle, dihedral,
+ * inversion) round counts; the atom arrays (rounds x team x 4 shorts, -1 = empty) may be
+ * null to query the counts first. */
+typedef struct smr_topo smr_topo;
+int  smr_topo_build(int natoms, const int* Z, const double* pos, const double* charges, double bond_cut, smr_topo** out,
+                    char* err, int errlen);
+void smr_topo_free(smr_topo* t);
+int  smr_topo_counts(const smr_topo* t, int counts[5]);
+int  smr_topo_export(const smr_topo* t, int* neighs, int* neighBs, int* bonds, double* bparams,
+                     int* angs, int* ang_ngs, double* angp, int* dihs, int* dih_ngs, double* dihp,
+                     int* invs, int* inv_ngs, double* invp, double* req, int* type_id);
+int  smr_topo_rounds(const smr_topo* t, int team, int rounds[3], short* ang_at, short* dih_at, short* inv_at);
+int  smr_add_topo(smr_handle* h, const smr_topo* t, int* topo_id);
+
+/* Systems: one slot per system; positions are float32 x,y,z concatenated over the systems. */
+int smr_add_systems(smr_handle* h, int nsys, const int* topo_ids, const float* pos, int* slot_ids);
+int smr_remove_systems(smr_handle* h, int nsys, const int* slot_ids);
+int smr_set_positions(smr_handle* h, int nsys, const int* slot_ids, const float* pos);
+int smr_active_slots(smr_handle* h, int* nslots, int* slot_ids /* may be null */);
+
+/* One force evaluation of the given slots at their current positions.
+ * forces: sum(natoms) x 4 (fx, fy, fz, E_atom) with E_atom in the reference's per-atom
+ * convention (opencl/UFF.cl fapos.w: bond energy and NB pair energy on both atoms);
+ * energy: nsys x SMR_E_NCOMP doubles (physical totals).  Either output may be null. */
+int smr_eval_forces(smr_handle* h, int nsys, const int* slot_ids, float* forces, double* energy);
+
+/* Relax every active, not yet finished slot for at most max_steps further FIRE steps.
+ * A system's FIRE state (velocities, dt, alpha, n_pos, steps done) persists across calls,
+ * so repeated calls continue the same trajectory.  step_budget caps the total steps of
+ * each system (0 = no cap beyond max_steps).  nfinished (may be null) receives the
+ * number of slots whose status is no longer SMR_ST_RUNNING. */
+int smr_run_fire(smr_handle* h, int max_steps, int step_budget, const smr_fire_params* p, int mode, int* nfinished);
+/* Restart FIRE (zero velocity, dt0, alpha0, n_pos 0, steps 0, status running) on slots. */
+int smr_reset_fire(smr_handle* h, int nsys, const int* slot_ids);
+
+/* Read back results; any output may be null.  pos: sum(natoms) x 3 float; forces: x 4;
+ * energy: nsys x SMR_E_NCOMP (only SMR_E_TOTAL is maintained by relaxation: the energy at
+ * the last force evaluation); steps: FIRE steps done; status: SMR_ST_*. */
+int smr_download(smr_handle* h, int nsys, const int* slot_ids, float* pos, float* forces, double* energy,
+                 int* steps, int* status);
+
+/* Device time (ms, CUDA events on the handle's stream) of the last smr_run_fire /
+ * smr_eval_forces call, and the number of kernel launches it made. */
+int smr_last_timing(smr_handle* h, double* ms, long long* launches);
+
+/* Team configuration of the persistent kernel: threads per system team for systems of
+ * up to n atoms (0 = library default / autotuned). */
+int smr_set_team_size(smr_handle* h, int max_atoms, int threads);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SURFMOL_RELAX_H */

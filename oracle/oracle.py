@@ -1,0 +1,284 @@
+"""ctypes binding of the FP64 parity oracle (oracle/oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+cpu_baseline leg of bench.py as the checker.  The product library never uses it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+DP = C.POINTER(C.c_double)
+IP = C.POINTER(C.c_int)
+
+
+class OrcGrid(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                ("p0", C.c_double * 3), ("step", C.c_double * 3),
+                ("cf32", C.POINTER(C.c_float)), ("cf64", DP), ("scale", C.c_double * 4)]
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        L.orc_sys_from_molecule.restype = C.c_void_p
+        L.orc_sys_from_molecule.argtypes = [C.c_int, IP, DP, DP, C.c_double]
+        L.orc_sys_from_bonds.restype = C.c_void_p
+        L.orc_sys_from_bonds.argtypes = [C.c_int, C.c_int, IP, DP, DP]
+        L.orc_sys_free.argtypes = [C.c_void_p]
+        L.orc_sys_counts.argtypes = [C.c_void_p, IP]
+        L.orc_sys_export.argtypes = [C.c_void_p] + [IP, IP, IP, DP, IP, IP, DP, IP, IP, DP, IP, IP, DP, DP, IP]
+        L.orc_sys_set_params.argtypes = [C.c_void_p, DP, DP, DP]
+        L.orc_type_name.restype = C.c_char_p
+        L.orc_type_name.argtypes = [C.c_int]
+        L.orc_eval.argtypes = [C.c_void_p, DP, C.POINTER(OrcGrid), DP, DP, DP, DP]
+        L.orc_relax.restype = C.c_int
+        L.orc_relax.argtypes = [C.c_void_p, DP, C.POINTER(OrcGrid), DP, DP, C.c_int, DP, DP, DP, DP, IP]
+        L.orc_relax_batch.argtypes = [C.c_int, C.POINTER(C.c_void_p), C.POINTER(DP), C.POINTER(OrcGrid), DP, DP,
+                                      C.c_int, IP, DP, IP, DP, C.c_int]
+        L.orc_max_threads.restype = C.c_int
+        L.orc_morse_points.argtypes = [C.c_int, DP, C.c_int, DP, DP, DP, C.c_int, C.c_int, C.c_double, DP]
+        L.orc_ewald_points.argtypes = [C.c_int, DP, C.c_int, DP, C.c_double, C.c_double, C.c_double, DP]
+        L.orc_brute_coulomb_points.argtypes = [C.c_int, DP, C.c_int, DP, C.c_double, C.c_double, C.c_int, DP]
+        L.orc_bspline_fit.argtypes = [C.c_int, C.c_int, C.c_int, DP, DP]
+        L.orc_bspline_conv.argtypes = [C.c_int, C.c_int, C.c_int, DP, DP]
+        L.orc_build_grid.restype = C.c_int
+        L.orc_build_grid.argtypes = [C.c_int, DP, DP, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, DP, DP,
+                                     C.c_double, C.c_int, C.c_double, DP, DP]
+        L.orc_substrate_direct.argtypes = [C.c_int, DP, DP, C.c_int, DP, DP, C.c_double, C.c_double, C.c_int,
+                                           C.c_double, C.c_double, C.c_double, DP]
+        _lib = L
+    return _lib
+
+
+def _d(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _i(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _dp(a):
+    return a.ctypes.data_as(DP) if a is not None else None
+
+
+def _ip(a):
+    return a.ctypes.data_as(IP) if a is not None else None
+
+
+# Defaults: FireState (crates/libs/molff/src/raff.rs:1053-1055) with dt_max 0.05 as
+# the pentacene relaxation uses (crates/libs/surfmol/tests/relax_pentacene_uff.rs:259).
+FIRE_DEFAULT = dict(dt0=0.001, dt_max=0.05, alpha0=0.1, f_inc=1.1, f_dec=0.5, f_alpha=0.99, n_min=5,
+                    fconv=1e-3, flimit=0.0)
+NB_DEFAULT = dict(rdamp=1.0, alpha=1.5, rcut=0.0, excl13=0)
+
+
+def fire_vec(**kw):
+    p = dict(FIRE_DEFAULT)
+    p.update(kw)
+    return _d([p["dt0"], p["dt_max"], p["alpha0"], p["f_inc"], p["f_dec"], p["f_alpha"], p["n_min"], p["fconv"],
+               p["flimit"]])
+
+
+def nb_vec(**kw):
+    p = dict(NB_DEFAULT)
+    p.update(kw)
+    return _d([p["rdamp"], p["alpha"], p["rcut"], p["excl13"]])
+
+
+class Grid:
+    """Oracle view of a z-fastest float4 coefficient grid (float32 or float64 array (nx,ny,nz,4))."""
+
+    def __init__(self, coef, p0, step, scale=(1.0, 1.0, 1.0, 1.0)):
+        self.coef = np.ascontiguousarray(coef)
+        nx, ny, nz, _ = self.coef.shape
+        self.s = OrcGrid()
+        self.s.nx, self.s.ny, self.s.nz = nx, ny, nz
+        for k in range(3):
+            self.s.p0[k] = float(p0[k])
+            self.s.step[k] = float(step[k])
+        for k in range(4):
+            self.s.scale[k] = float(scale[k])
+        if self.coef.dtype == np.float32:
+            self.s.cf32 = self.coef.ctypes.data_as(C.POINTER(C.c_float))
+            self.s.cf64 = None
+        else:
+            self.coef = self.coef.astype(np.float64)
+            self.s.cf64 = self.coef.ctypes.data_as(DP)
+            self.s.cf32 = None
+
+    def ptr(self):
+        return C.byref(self.s)
+
+
+class System:
+    """One molecule in the oracle: topology, typing and parameters."""
+
+    def __init__(self, handle):
+        self.h = C.c_void_p(handle)
+        c = (C.c_int * 5)()
+        lib().orc_sys_counts(self.h, c)
+        self.n, self.nbonds, self.nang, self.ndih, self.ninv = list(c)
+
+    @classmethod
+    def from_molecule(cls, Z, pos, q=None, bond_cut=1.8):
+        Z = _i(Z)
+        pos = _d(pos)
+        q = _d(q) if q is not None else None
+        return cls(lib().orc_sys_from_molecule(len(Z), _ip(Z), _dp(pos), _dp(q), bond_cut))
+
+    @classmethod
+    def from_bonds(cls, n, bonds, bparams, req=None):
+        bonds = _i(bonds).reshape(-1, 2)
+        bp = _d(bparams).reshape(-1, 2)
+        req = _d(req) if req is not None else None
+        return cls(lib().orc_sys_from_bonds(n, len(bonds), _ip(bonds), _dp(bp), _dp(req)))
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().orc_sys_free(self.h)
+        except Exception:
+            pass
+
+    def export(self):
+        n, nb, na, nd, ni = self.n, self.nbonds, self.nang, self.ndih, self.ninv
+        out = dict(neighs=np.zeros((n, 4), np.int32), neighBs=np.zeros((n, 4), np.int32),
+                   bonds=np.zeros((nb, 2), np.int32), bparams=np.zeros((nb, 2)),
+                   angs=np.zeros((na, 3), np.int32), ang_ngs=np.zeros((na, 2), np.int32), angp=np.zeros((na, 5)),
+                   dihs=np.zeros((nd, 4), np.int32), dih_ngs=np.zeros((nd, 3), np.int32), dihp=np.zeros((nd, 3)),
+                   invs=np.zeros((ni, 4), np.int32), inv_ngs=np.zeros((ni, 3), np.int32), invp=np.zeros((ni, 4)),
+                   req=np.zeros((n, 4)), type_id=np.zeros(n, np.int32))
+        o = out
+        lib().orc_sys_export(self.h, _ip(o["neighs"]), _ip(o["neighBs"]), _ip(o["bonds"]), _dp(o["bparams"]),
+                             _ip(o["angs"]), _ip(o["ang_ngs"]), _dp(o["angp"]), _ip(o["dihs"]), _ip(o["dih_ngs"]),
+                             _dp(o["dihp"]), _ip(o["invs"]), _ip(o["inv_ngs"]), _dp(o["invp"]), _dp(o["req"]),
+                             _ip(o["type_id"]))
+        out["types"] = [lib().orc_type_name(int(t)).decode() for t in out["type_id"]]
+        return out
+
+    def set_params(self, angp=None, dihp=None, invp=None):
+        a = _d(angp) if angp is not None else None
+        d = _d(dihp) if dihp is not None else None
+        v = _d(invp) if invp is not None else None
+        lib().orc_sys_set_params(self.h, _dp(a), _dp(d), _dp(v))
+
+    def eval(self, pos, grid: Grid | None = None, **nb):
+        pos = _d(pos)
+        F = np.zeros((self.n, 3))
+        Ea = np.zeros(self.n)
+        Ec = np.zeros(8)
+        nbp = nb_vec(**nb)
+        lib().orc_eval(self.h, _dp(pos), grid.ptr() if grid is not None else None, _dp(nbp), _dp(F), _dp(Ea), _dp(Ec))
+        return F, Ea, Ec
+
+    def relax(self, pos, grid: Grid | None = None, max_steps=2000, nb=None, **fire):
+        pos = _d(pos).copy()
+        F = np.zeros((self.n, 3))
+        Ea = np.zeros(self.n)
+        Ec = np.zeros(8)
+        fmax = C.c_double()
+        conv = C.c_int()
+        steps = lib().orc_relax(self.h, _dp(pos), grid.ptr() if grid is not None else None, _dp(nb_vec(**(nb or {}))),
+                                _dp(fire_vec(**fire)), max_steps, _dp(F), _dp(Ea), _dp(Ec), C.byref(fmax),
+                                C.byref(conv))
+        return dict(pos=pos, F=F, Ea=Ea, Ec=Ec, steps=steps, fmax=fmax.value, conv=bool(conv.value))
+
+
+E_TOT, E_BOND, E_ANG, E_DIH, E_INV, E_NB, E_GRID = range(7)
+
+
+def relax_batch(systems, positions, grid=None, max_steps=2000, nthreads=0, nb=None, **fire):
+    """Relax many systems in parallel (OpenMP, one system per thread). Returns dict of arrays."""
+    ns = len(systems)
+    hs = (C.c_void_p * ns)(*[s.h.value for s in systems])
+    pos = [_d(p).copy() for p in positions]
+    pp = (DP * ns)(*[_dp(p) for p in pos])
+    steps = np.zeros(ns, np.int32)
+    fmax = np.zeros(ns)
+    conv = np.zeros(ns, np.int32)
+    etot = np.zeros(ns)
+    lib().orc_relax_batch(ns, hs, pp, grid.ptr() if grid is not None else None, _dp(nb_vec(**(nb or {}))),
+                          _dp(fire_vec(**fire)), max_steps, _ip(steps), _dp(fmax), _ip(conv), _dp(etot), nthreads)
+    return dict(pos=pos, steps=steps, fmax=fmax, conv=conv.astype(bool), etot=etot)
+
+
+def max_threads():
+    return lib().orc_max_threads()
+
+
+def morse_points(pts, ions, ion_req, Lx, Ly, npbc=1, alpha=1.5):
+    pts = _d(pts).reshape(-1, 3)
+    ions = _d(ions)
+    re = _d(ion_req)
+    cell = _d([Lx, 0.0, 0.0, Ly])
+    out = np.zeros((len(pts), 2))
+    lib().orc_morse_points(len(pts), _dp(pts), len(ions), _dp(ions), _dp(re), _dp(cell), npbc, npbc, alpha, _dp(out))
+    return out
+
+
+def ewald_points(pts, ions, Lx, Ly, gcut):
+    pts = _d(pts).reshape(-1, 3)
+    ions = _d(ions)
+    out = np.zeros(len(pts))
+    lib().orc_ewald_points(len(pts), _dp(pts), len(ions), _dp(ions), Lx, Ly, gcut, _dp(out))
+    return out
+
+
+def brute_coulomb_points(pts, ions, Lx, Ly, nrep):
+    pts = _d(pts).reshape(-1, 3)
+    ions = _d(ions)
+    out = np.zeros(len(pts))
+    lib().orc_brute_coulomb_points(len(pts), _dp(pts), len(ions), _dp(ions), Lx, Ly, nrep, _dp(out))
+    return out
+
+
+def bspline_fit(v):
+    v = _d(v)
+    nx, ny, nz = v.shape
+    c = np.zeros_like(v)
+    lib().orc_bspline_fit(nx, ny, nz, _dp(v), _dp(c))
+    return c
+
+
+def bspline_conv(c):
+    c = _d(c)
+    nx, ny, nz = c.shape
+    v = np.zeros_like(c)
+    lib().orc_bspline_conv(nx, ny, nz, _dp(c), _dp(v))
+    return v
+
+
+def build_grid(ions, ion_req, Lx, Ly, nx, ny, nz, p0, step, alpha=1.5, npbc=1, gcut=30.0, values=False):
+    ions = _d(ions)
+    re = _d(ion_req)
+    coef = np.zeros((nx, ny, nz, 4))
+    val = np.zeros((nx, ny, nz, 4)) if values else None
+    lib().orc_build_grid(len(ions), _dp(ions), _dp(re), Lx, Ly, nx, ny, nz, _dp(_d(p0)), _dp(_d(step)), alpha, npbc,
+                         gcut, _dp(coef), _dp(val))
+    return (coef, val) if values else coef
+
+
+def substrate_direct(pts, req_atom, ions, ion_req, Lx, Ly, npbc=1, alpha=1.5, gcut=30.0, h=1e-4):
+    pts = _d(pts).reshape(-1, 3)
+    ra = _d(req_atom).reshape(-1, 4)
+    out = np.zeros((len(pts), 4))
+    lib().orc_substrate_direct(len(pts), _dp(pts), _dp(ra), len(ions), _dp(_d(ions)), _dp(_d(ion_req)), Lx, Ly, npbc,
+                               alpha, gcut, h, _dp(out))
+    return out

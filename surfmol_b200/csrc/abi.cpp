@@ -1,0 +1,832 @@
+// abi.cpp -- the C ABI of include/surfmol_relax.h: handle, device arenas, slot
+// allocator, launches and transfers.  Host-side only; kernels live in relax.cu / grid.cu.
+#include <algorithm>
+#include <chrono>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <new>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/surfmol_relax.h"
+#include "smr_internal.h"
+
+using namespace smr;
+
+namespace smr {
+int launch_copy_segments(const int* d_src_off, const int* d_len, const int* d_dst_off, int n, const float4* src, float4* dst, cudaStream_t s);
+}
+
+namespace {
+
+template <class T>
+struct DArr {   // growable device array with a host mirror of the uploaded prefix
+    T* d = nullptr;
+    size_t cap = 0;
+    ~DArr() { if (d) cudaFree(d); }
+    cudaError_t reserve(size_t n, size_t keep) {
+        if (n <= cap) return cudaSuccess;
+        size_t nc = std::max(n, cap * 2 + 1024);
+        T* nd = nullptr;
+        cudaError_t e = cudaMalloc(&nd, nc * sizeof(T));
+        if (e != cudaSuccess) return e;
+        if (d && keep) { e = cudaMemcpy(nd, d, keep * sizeof(T), cudaMemcpyDeviceToDevice); if (e != cudaSuccess) { cudaFree(nd); return e; } }
+        if (d) cudaFree(d);
+        d = nd; cap = nc;
+        return cudaSuccess;
+    }
+};
+
+int default_team(int n) {
+    if (n <= 64) return 32;
+    if (n <= 160) return 64;
+    if (n <= 448) return 128;
+    if (n <= 1024) return 256;
+    return 512;
+}
+
+}  // namespace
+
+struct smr_handle {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int num_sms = 0;
+    size_t smem_optin = 0;
+    std::string err;
+
+    int max_systems = 0;
+    long long max_atoms = 0;
+
+    // per-atom system state and per-slot state
+    float4 *pos = nullptr, *vel = nullptr, *force = nullptr, *stage = nullptr;
+    SlotState* slots = nullptr;
+    int* work = nullptr;
+    int* counter = nullptr;
+    double* ecomp = nullptr;
+    int* xfer = nullptr;            // 3 * max_systems ints for gather / scatter descriptors
+    std::vector<SlotState> hs;      // host mirror of slots
+    std::vector<int> free_slots;
+    std::map<long long, long long> free_atoms;   // offset -> length
+    float4* pinned = nullptr;       // staging for uploads / downloads (max_atoms float4)
+
+    // topologies
+    std::vector<HostTopo> topos;
+    std::vector<TopoDev> htd;
+    DArr<TopoDev> dtd;
+    std::vector<float4> hreq, hbk, hbl;
+    std::vector<short4> hneigh;
+    std::vector<AngRec> hang; std::vector<DihRec> hdih; std::vector<InvRec> hinv;
+    DArr<float4> dreq, dbk, dbl; DArr<short4> dneigh;
+    DArr<AngRec> dang; DArr<DihRec> ddih; DArr<InvRec> dinv;
+    size_t up_atoms = 0, up_ang = 0, up_dih = 0, up_inv = 0, up_topo = 0;   // uploaded prefixes
+    std::map<int, int> team_override;   // max_atoms -> threads
+
+    // grid
+    void* grid = nullptr;
+    int grid_dtype = GRID_F32;
+    int gdim[3] = {0, 0, 0};
+    double gp0[3] = {0, 0, 0}, gstep[3] = {1, 1, 1};
+    float gscale[4] = {1, 1, 1, 1};
+    bool has_grid = false;
+
+    smr_nb_params nb{1.0f, 1.5f, 0.0f, 0};
+
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double last_ms = 0.0;
+    long long last_launches = 0;
+};
+
+namespace {
+
+int fail(smr_handle* h, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (h) h->err = buf;
+    return code;
+}
+
+#define CU(h, x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) return fail(h, SMR_ERR_CUDA, "%s: %s", #x, cudaGetErrorString(e_)); } while (0)
+
+int team_for(const smr_handle* h, int n) {
+    for (auto& kv : h->team_override) if (n <= kv.first) return kv.second;
+    return default_team(n);
+}
+
+// append a topology's device records (packed for its team) to the arenas
+void append_topology(smr_handle* h, const HostTopo& T) {
+    TopoDev td{};
+    td.natoms = T.n;
+    td.atom_off = (int)h->hreq.size();
+    td.team = team_for(h, T.n);
+    for (int a = 0; a < T.n; a++) {
+        const double* r = &T.req[4 * a];
+        h->hreq.push_back(make_float4((float)r[0], (float)r[1], (float)r[2], (float)r[3]));
+        h->hneigh.push_back(make_short4((short)T.neighs[4 * a], (short)T.neighs[4 * a + 1], (short)T.neighs[4 * a + 2], (short)T.neighs[4 * a + 3]));
+        const double* kl = &T.bond_kl[8 * a];
+        h->hbk.push_back(make_float4((float)kl[0], (float)kl[2], (float)kl[4], (float)kl[6]));
+        h->hbl.push_back(make_float4((float)kl[1], (float)kl[3], (float)kl[5], (float)kl[7]));
+    }
+    PackedTerms P;
+    pack_rounds(T, td.team, P);
+    td.ang_off = (int)h->hang.size(); td.ang_rounds = P.ang_rounds; h->hang.insert(h->hang.end(), P.ang.begin(), P.ang.end());
+    td.dih_off = (int)h->hdih.size(); td.dih_rounds = P.dih_rounds; h->hdih.insert(h->hdih.end(), P.dih.begin(), P.dih.end());
+    td.inv_off = (int)h->hinv.size(); td.inv_rounds = P.inv_rounds; h->hinv.insert(h->hinv.end(), P.inv.begin(), P.inv.end());
+    h->htd.push_back(td);
+}
+
+template <class T>
+cudaError_t sync_arr(DArr<T>& d, const std::vector<T>& hv, size_t& up, cudaStream_t s) {
+    if (hv.size() == up) return cudaSuccess;
+    cudaError_t e = d.reserve(hv.size(), up);
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpyAsync(d.d + up, hv.data() + up, (hv.size() - up) * sizeof(T), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) up = hv.size();
+    return e;
+}
+
+int upload_all(smr_handle* h) {
+    cudaStream_t s = h->stream;
+    size_t ua = h->up_atoms;
+    size_t t;
+    t = ua; CU(h, sync_arr(h->dreq, h->hreq, t, s));
+    t = ua; CU(h, sync_arr(h->dneigh, h->hneigh, t, s));
+    t = ua; CU(h, sync_arr(h->dbk, h->hbk, t, s));
+    t = ua; CU(h, sync_arr(h->dbl, h->hbl, t, s));
+    h->up_atoms = h->hreq.size();
+    CU(h, sync_arr(h->dang, h->hang, h->up_ang, s));
+    CU(h, sync_arr(h->ddih, h->hdih, h->up_dih, s));
+    CU(h, sync_arr(h->dinv, h->hinv, h->up_inv, s));
+    CU(h, sync_arr(h->dtd, h->htd, h->up_topo, s));
+    return 0;
+}
+
+// repack every topology for the current team mapping (after smr_set_team_size)
+int repack_all(smr_handle* h) {
+    h->htd.clear(); h->hreq.clear(); h->hneigh.clear(); h->hbk.clear(); h->hbl.clear();
+    h->hang.clear(); h->hdih.clear(); h->hinv.clear();
+    h->up_atoms = h->up_ang = h->up_dih = h->up_inv = h->up_topo = 0;
+    for (const HostTopo& T : h->topos) append_topology(h, T);
+    return upload_all(h);
+}
+
+long long alloc_atoms(smr_handle* h, long long n) {
+    for (auto it = h->free_atoms.begin(); it != h->free_atoms.end(); ++it) {
+        if (it->second >= n) {
+            long long off = it->first, len = it->second;
+            h->free_atoms.erase(it);
+            if (len > n) h->free_atoms[off + n] = len - n;
+            return off;
+        }
+    }
+    return -1;
+}
+
+void free_atoms(smr_handle* h, long long off, long long n) {
+    auto it = h->free_atoms.emplace(off, n).first;
+    auto nx = std::next(it);
+    if (nx != h->free_atoms.end() && it->first + it->second == nx->first) { it->second += nx->second; h->free_atoms.erase(nx); }
+    if (it != h->free_atoms.begin()) {
+        auto pv = std::prev(it);
+        if (pv->first + pv->second == it->first) { pv->second += it->second; h->free_atoms.erase(it); }
+    }
+}
+
+bool valid_slot(const smr_handle* h, int s) { return s >= 0 && s < h->max_systems && h->hs[s].active; }
+
+int wait_stream(smr_handle* h, double timeout_s) {
+    cudaEvent_t e;
+    CU(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    cudaEventRecord(e, h->stream);
+    auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        cudaError_t q = cudaEventQuery(e);
+        if (q == cudaSuccess) break;
+        if (q != cudaErrorNotReady) { cudaEventDestroy(e); return fail(h, SMR_ERR_CUDA, "stream: %s", cudaGetErrorString(q)); }
+        double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (dt > timeout_s) { cudaEventDestroy(e); return fail(h, SMR_ERR_TIMEOUT, "device work not finished after %.0f s", timeout_s); }
+        std::this_thread::sleep_for(std::chrono::microseconds(dt < 0.01 ? 5 : 200));
+    }
+    cudaEventDestroy(e);
+    return 0;
+}
+
+int download_slots(smr_handle* h) {
+    CU(h, cudaMemcpyAsync(h->hs.data(), h->slots, h->hs.size() * sizeof(SlotState), cudaMemcpyDeviceToHost, h->stream));
+    return wait_stream(h, 3600.0);
+}
+
+int upload_slots(smr_handle* h, const std::vector<int>& ids) {
+    for (int s : ids) CU(h, cudaMemcpyAsync(h->slots + s, &h->hs[s], sizeof(SlotState), cudaMemcpyHostToDevice, h->stream));
+    return 0;
+}
+
+KernelArgs base_args(smr_handle* h) {
+    KernelArgs a{};
+    a.counter = h->counter;
+    a.slots = h->slots;
+    a.topos = h->dtd.d;
+    a.req = h->dreq.d; a.neigh = h->dneigh.d; a.bk = h->dbk.d; a.bl = h->dbl.d;
+    a.angs = h->dang.d; a.dihs = h->ddih.d; a.invs = h->dinv.d;
+    a.pos = h->pos; a.vel = h->vel; a.force = h->force;
+    a.has_grid = h->has_grid ? 1 : 0;
+    a.grid.data = h->grid;
+    a.grid.dtype = h->grid_dtype;
+    a.grid.nx = h->gdim[0]; a.grid.ny = h->gdim[1]; a.grid.nz = h->gdim[2];
+    for (int k = 0; k < 3; k++) { a.grid.p0[k] = (float)h->gp0[k]; a.grid.inv_step[k] = (float)(1.0 / h->gstep[k]); }
+    for (int k = 0; k < 4; k++) a.grid.scale[k] = h->has_grid ? h->gscale[k] : 1.f;
+    a.R2damp = h->nb.rdamp * h->nb.rdamp;
+    a.alpha_morse = h->nb.alpha_morse;
+    a.rc2 = h->nb.rcut > 0 ? h->nb.rcut * h->nb.rcut : 3.0e38f;
+    return a;
+}
+
+// group slots by team size; returns (team, begin, end, nmax) segments of the reordered list
+struct Seg { int team, begin, end, nmax; };
+std::vector<Seg> group_by_team(smr_handle* h, std::vector<int>& ids) {
+    std::stable_sort(ids.begin(), ids.end(), [&](int a, int b) {
+        return h->htd[h->hs[a].topo].team < h->htd[h->hs[b].topo].team;
+    });
+    std::vector<Seg> segs;
+    for (int i = 0; i < (int)ids.size(); i++) {
+        int t = h->htd[h->hs[ids[i]].topo].team, n = h->hs[ids[i]].natoms;
+        if (segs.empty() || segs.back().team != t) segs.push_back({t, i, i + 1, n});
+        else { segs.back().end = i + 1; segs.back().nmax = std::max(segs.back().nmax, n); }
+    }
+    return segs;
+}
+
+// a batch of slots must be distinct, active and fit the staging buffers
+int check_batch(smr_handle* h, int nsys, const int* ids) {
+    if (nsys > h->max_systems) return fail(h, SMR_ERR_CAPACITY, "%d slots requested, capacity %d", nsys, h->max_systems);
+    std::vector<char> seen(h->max_systems, 0);
+    for (int i = 0; i < nsys; i++) {
+        int s = ids[i];
+        if (!valid_slot(h, s)) return fail(h, SMR_ERR_ARG, "slot %d not active", s);
+        if (seen[s]) return fail(h, SMR_ERR_ARG, "slot %d listed twice", s);
+        seen[s] = 1;
+    }
+    return 0;
+}
+
+int check_smem(smr_handle* h, const Seg& g) {
+    size_t need = team_smem_bytes(g.nmax) * (g.team == 32 ? 4 : 1);
+    if (need > h->smem_optin)
+        return fail(h, SMR_ERR_CAPACITY, "systems of %d atoms need %zu B of shared memory per block (device limit %zu); "
+                    "use a larger team or smaller systems", g.nmax, need, h->smem_optin);
+    return 0;
+}
+
+}  // namespace
+
+// ====================================================================== API
+extern "C" {
+
+const char* smr_version(void) { return "surfmol_b200 0.1 (sm_100a)"; }
+
+const char* smr_last_error(const smr_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+int smr_create(const smr_config* cfg, smr_handle** out) {
+    if (!cfg || !out) return SMR_ERR_ARG;
+    *out = nullptr;
+    if (cfg->max_systems <= 0 || cfg->max_atoms <= 0 || cfg->max_atoms > (1LL << 31) - 1) return SMR_ERR_ARG;
+    smr_handle* h = new (std::nothrow) smr_handle();
+    if (!h) return SMR_ERR_CAPACITY;
+    h->device = cfg->device;
+    h->max_systems = cfg->max_systems;
+    h->max_atoms = cfg->max_atoms;
+    auto bail = [&](int code) { smr_destroy(h); return code; };
+    if (cudaSetDevice(h->device) != cudaSuccess) return bail(SMR_ERR_CUDA);
+    int v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, h->device); h->num_sms = v;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device); h->smem_optin = (size_t)v;
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(SMR_ERR_CUDA);
+    size_t na = (size_t)cfg->max_atoms, ns = (size_t)cfg->max_systems;
+    if (cudaMalloc(&h->pos, na * 16) || cudaMalloc(&h->vel, na * 16) || cudaMalloc(&h->force, na * 16) ||
+        cudaMalloc(&h->stage, na * 16) || cudaMalloc(&h->slots, ns * sizeof(SlotState)) ||
+        cudaMalloc(&h->work, ns * 4) || cudaMalloc(&h->counter, 64) || cudaMalloc(&h->ecomp, ns * 8 * 8) ||
+        cudaMalloc(&h->xfer, ns * 3 * 4) || cudaMallocHost(&h->pinned, na * 16))
+        return bail(SMR_ERR_CUDA);
+    cudaMemset(h->slots, 0, ns * sizeof(SlotState));
+    cudaMemset(h->vel, 0, na * 16);
+    h->hs.assign(ns, SlotState{});
+    for (int s = (int)ns - 1; s >= 0; s--) h->free_slots.push_back(s);
+    h->free_atoms[0] = (long long)na;
+    cudaEventCreate(&h->ev0);
+    cudaEventCreate(&h->ev1);
+    *out = h;
+    return SMR_OK;
+}
+
+int smr_destroy(smr_handle* h) {
+    if (!h) return SMR_ERR_ARG;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    cudaFree(h->pos); cudaFree(h->vel); cudaFree(h->force); cudaFree(h->stage); cudaFree(h->slots);
+    cudaFree(h->work); cudaFree(h->counter); cudaFree(h->ecomp); cudaFree(h->xfer);
+    if (h->pinned) cudaFreeHost(h->pinned);
+    if (h->grid) cudaFree(h->grid);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return SMR_OK;
+}
+
+int smr_set_nb_params(smr_handle* h, const smr_nb_params* p) {
+    if (!h || !p) return SMR_ERR_ARG;
+    if (!(p->rdamp >= 0.f) || !(p->alpha_morse > 0.f)) return fail(h, SMR_ERR_ARG, "rdamp must be >= 0 and alpha_morse > 0");
+    h->nb = *p;
+    return SMR_OK;
+}
+
+int smr_set_team_size(smr_handle* h, int max_atoms, int threads) {
+    if (!h) return SMR_ERR_ARG;
+    if (threads != 0 && threads != 32 && threads != 64 && threads != 128 && threads != 256 && threads != 512)
+        return fail(h, SMR_ERR_ARG, "team size must be 32, 64, 128, 256 or 512");
+    if (threads == 0) h->team_override.erase(max_atoms);
+    else h->team_override[max_atoms] = threads;
+    return repack_all(h);
+}
+
+static size_t voxel_bytes(int dtype) { return dtype == SMR_GRID_F32 ? 16 : 8; }
+
+int smr_set_grid(smr_handle* h, const void* coef, int dtype, const float scale[4], int nx, int ny, int nz,
+                 const double p0[3], const double step[3]) {
+    if (!h || !coef || !p0 || !step) return SMR_ERR_ARG;
+    if (dtype < 0 || dtype > 2) return fail(h, SMR_ERR_ARG, "unknown grid dtype %d", dtype);
+    if (nx < 4 || ny < 4 || nz < 4) return fail(h, SMR_ERR_ARG, "grid must be at least 4x4x4 (got %dx%dx%d)", nx, ny, nz);
+    if (!(step[0] > 0 && step[1] > 0 && step[2] > 0)) return fail(h, SMR_ERR_ARG, "grid steps must be positive");
+    size_t nv = (size_t)nx * ny * nz, bytes = nv * voxel_bytes(dtype);
+    void* d = nullptr;
+    CU(h, cudaMalloc(&d, bytes));
+    cudaError_t e = cudaMemcpy(d, coef, bytes, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) { cudaFree(d); return fail(h, SMR_ERR_CUDA, "grid upload: %s", cudaGetErrorString(e)); }
+    if (h->grid) cudaFree(h->grid);
+    h->grid = d; h->grid_dtype = dtype; h->has_grid = true;
+    h->gdim[0] = nx; h->gdim[1] = ny; h->gdim[2] = nz;
+    for (int k = 0; k < 3; k++) { h->gp0[k] = p0[k]; h->gstep[k] = step[k]; }
+    for (int k = 0; k < 4; k++) h->gscale[k] = scale ? scale[k] : 1.f;
+    return SMR_OK;
+}
+
+int smr_get_grid(smr_handle* h, void* coef_out, int* dtype, float scale[4], int dims[3], double p0[3], double step[3]) {
+    if (!h) return SMR_ERR_ARG;
+    if (!h->has_grid) return fail(h, SMR_ERR_STATE, "no grid set");
+    if (dtype) *dtype = h->grid_dtype;
+    if (scale) for (int k = 0; k < 4; k++) scale[k] = h->gscale[k];
+    if (dims) for (int k = 0; k < 3; k++) dims[k] = h->gdim[k];
+    if (p0) for (int k = 0; k < 3; k++) p0[k] = h->gp0[k];
+    if (step) for (int k = 0; k < 3; k++) step[k] = h->gstep[k];
+    if (coef_out) {
+        size_t bytes = (size_t)h->gdim[0] * h->gdim[1] * h->gdim[2] * voxel_bytes(h->grid_dtype);
+        CU(h, cudaMemcpy(coef_out, h->grid, bytes, cudaMemcpyDeviceToHost));
+    }
+    return SMR_OK;
+}
+
+int smr_convert_grid(smr_handle* h, int dtype) {
+    if (!h) return SMR_ERR_ARG;
+    if (!h->has_grid) return fail(h, SMR_ERR_STATE, "no grid set");
+    if (dtype == h->grid_dtype) return SMR_OK;
+    size_t nv = (size_t)h->gdim[0] * h->gdim[1] * h->gdim[2];
+    float4* f32 = nullptr;
+    if (h->grid_dtype == SMR_GRID_F32) f32 = (float4*)h->grid;
+    else {
+        CU(h, cudaMalloc(&f32, nv * 16));
+        if (decode_grid_16(h->grid, f32, nv, h->grid_dtype, h->gscale, h->stream)) { cudaFree(f32); return fail(h, SMR_ERR_CUDA, "grid decode failed"); }
+    }
+    void* out = nullptr;
+    float sc[4] = {1, 1, 1, 1};
+    if (dtype == SMR_GRID_F32) out = f32;
+    else {
+        cudaError_t e = cudaMalloc(&out, nv * 8);
+        if (e != cudaSuccess) { if ((void*)f32 != h->grid) cudaFree(f32); return fail(h, SMR_ERR_CUDA, "grid alloc: %s", cudaGetErrorString(e)); }
+        if (encode_grid_16(f32, out, nv, dtype, sc, h->stream)) { cudaFree(out); return fail(h, SMR_ERR_CUDA, "grid encode failed"); }
+        if ((void*)f32 != h->grid) cudaFree(f32);
+    }
+    CU(h, cudaStreamSynchronize(h->stream));
+    if (out != h->grid) cudaFree(h->grid);
+    h->grid = out; h->grid_dtype = dtype;
+    for (int k = 0; k < 4; k++) h->gscale[k] = sc[k];
+    return SMR_OK;
+}
+
+int smr_build_grid(smr_handle* h, int nions, const double* ions, const double* ion_re, double Lx, double Ly,
+                   int nx, int ny, int nz, const double p0[3], const double step[3], const smr_grid_build_params* p) {
+    if (!h || !ions || !ion_re || !p0 || !step || !p || nions <= 0) return SMR_ERR_ARG;
+    if (nx < 4 || ny < 4 || nz < 4) return fail(h, SMR_ERR_ARG, "grid must be at least 4x4x4");
+    if (!(Lx > 0 && Ly > 0)) return fail(h, SMR_ERR_ARG, "cell must be positive");
+    if (p->dtype < 0 || p->dtype > 2) return fail(h, SMR_ERR_ARG, "unknown grid dtype");
+    double *dions = nullptr, *dre = nullptr;
+    float4* out = nullptr;
+    size_t nv = (size_t)nx * ny * nz;
+    CU(h, cudaMalloc(&dions, (size_t)nions * 32));
+    cudaError_t e = cudaMalloc(&dre, (size_t)nions * 32);
+    if (e == cudaSuccess) e = cudaMalloc(&out, nv * 16);
+    if (e == cudaSuccess) e = cudaMemcpy(dions, ions, (size_t)nions * 32, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        std::vector<double> re4(4 * (size_t)nions, 0.0);
+        for (int i = 0; i < nions; i++) { re4[4 * i] = ion_re[2 * i]; re4[4 * i + 1] = ion_re[2 * i + 1]; }
+        e = cudaMemcpy(dre, re4.data(), re4.size() * 8, cudaMemcpyHostToDevice);
+    }
+    if (e != cudaSuccess) { cudaFree(dions); cudaFree(dre); cudaFree(out); return fail(h, SMR_ERR_CUDA, "grid build alloc: %s", cudaGetErrorString(e)); }
+    GridBuildArgs A{};
+    A.nions = nions; A.ions = dions; A.ion_re = dre; A.Lx = Lx; A.Ly = Ly; A.nx = nx; A.ny = ny; A.nz = nz;
+    for (int k = 0; k < 3; k++) { A.p0[k] = p0[k]; A.step[k] = step[k]; }
+    A.alpha = p->alpha_morse; A.npbc = p->npbc; A.ewald_tol = p->ewald_tol; A.morse_rcut = p->morse_rcut;
+    char msg[400] = {0};
+    int r = build_grid_device(A, out, h->stream, msg, sizeof(msg));
+    cudaFree(dions); cudaFree(dre);
+    if (r) { cudaFree(out); return fail(h, SMR_ERR_ARG, "grid build: %s", msg); }
+    if (h->grid) cudaFree(h->grid);
+    h->grid = out; h->grid_dtype = SMR_GRID_F32; h->has_grid = true;
+    h->gdim[0] = nx; h->gdim[1] = ny; h->gdim[2] = nz;
+    for (int k = 0; k < 3; k++) { h->gp0[k] = p0[k]; h->gstep[k] = step[k]; }
+    for (int k = 0; k < 4; k++) h->gscale[k] = 1.f;
+    if (p->dtype != SMR_GRID_F32) return smr_convert_grid(h, p->dtype);
+    return SMR_OK;
+}
+
+int smr_add_molecule(smr_handle* h, int natoms, const int* Z, const double* pos, const double* charges,
+                     double bond_cut, int* topo_id) {
+    if (!h || !Z || !pos || !topo_id) return SMR_ERR_ARG;
+    HostTopo T;
+    char msg[300] = {0};
+    if (build_molecule_topology(natoms, Z, pos, charges, bond_cut > 0 ? bond_cut : 1.8, T, msg, sizeof(msg)))
+        return fail(h, SMR_ERR_ARG, "molecule: %s", msg);
+    h->topos.push_back(std::move(T));
+    append_topology(h, h->topos.back());
+    int r = upload_all(h);
+    if (r) return r;
+    *topo_id = (int)h->topos.size() - 1;
+    return SMR_OK;
+}
+
+int smr_add_topology(smr_handle* h, const smr_topology_desc* d, int* topo_id) {
+    if (!h || !d || !topo_id || !d->req || !d->neighs || !d->bond_kl) return SMR_ERR_ARG;
+    if ((d->nang && (!d->angs || !d->angp)) || (d->ndih && (!d->dihs || !d->dihp)) || (d->ninv && (!d->invs || !d->invp)))
+        return fail(h, SMR_ERR_ARG, "term arrays missing");
+    HostTopo T;
+    char msg[300] = {0};
+    if (build_desc_topology(d->natoms, d->req, d->neighs, d->bond_kl, d->nang, d->angs, d->angp, d->ndih, d->dihs, d->dihp,
+                            d->ninv, d->invs, d->invp, T, msg, sizeof(msg)))
+        return fail(h, SMR_ERR_ARG, "topology: %s", msg);
+    h->topos.push_back(std::move(T));
+    append_topology(h, h->topos.back());
+    int r = upload_all(h);
+    if (r) return r;
+    *topo_id = (int)h->topos.size() - 1;
+    return SMR_OK;
+}
+
+int smr_topology_counts(smr_handle* h, int id, int c[6]) {
+    if (!h || !c || id < 0 || id >= (int)h->topos.size()) return SMR_ERR_ARG;
+    const HostTopo& T = h->topos[id];
+    const TopoDev& td = h->htd[id];
+    c[0] = T.n; c[1] = (int)T.bonds.size() / 2; c[2] = (int)T.angs.size() / 3; c[3] = (int)T.dihs.size() / 4;
+    c[4] = (int)T.invs.size() / 4; c[5] = td.ang_rounds + td.dih_rounds + td.inv_rounds;
+    return SMR_OK;
+}
+
+int smr_topology_export(smr_handle* h, int id, int* neighs, int* neighBs, int* bonds, double* bparams,
+                        int* angs, int* ang_ngs, double* angp, int* dihs, int* dih_ngs, double* dihp,
+                        int* invs, int* inv_ngs, double* invp, double* req, int* type_id) {
+    if (!h || id < 0 || id >= (int)h->topos.size()) return SMR_ERR_ARG;
+    const HostTopo& T = h->topos[id];
+    auto cp = [](auto* dst, const auto& v) { if (dst) std::copy(v.begin(), v.end(), dst); };
+    cp(neighs, T.neighs); cp(neighBs, T.neighBs); cp(bonds, T.bonds); cp(bparams, T.bparams);
+    cp(angs, T.angs); cp(ang_ngs, T.ang_ngs); cp(angp, T.angp);
+    cp(dihs, T.dihs); cp(dih_ngs, T.dih_ngs); cp(dihp, T.dihp);
+    cp(invs, T.invs); cp(inv_ngs, T.inv_ngs); cp(invp, T.invp);
+    cp(req, T.req); cp(type_id, T.type_id);
+    return SMR_OK;
+}
+
+const char* smr_type_name(int id) { return type_name(id); }
+
+int smr_add_systems(smr_handle* h, int nsys, const int* topo_ids, const float* pos, int* slot_ids) {
+    if (!h || nsys < 0 || (nsys && (!topo_ids || !pos || !slot_ids))) return SMR_ERR_ARG;
+    if ((int)h->free_slots.size() < nsys) return fail(h, SMR_ERR_CAPACITY, "only %zu free slots for %d systems", h->free_slots.size(), nsys);
+    long long need = 0;
+    for (int i = 0; i < nsys; i++) {
+        if (topo_ids[i] < 0 || topo_ids[i] >= (int)h->topos.size()) return fail(h, SMR_ERR_ARG, "system %d: unknown topology %d", i, topo_ids[i]);
+        need += h->topos[topo_ids[i]].n;
+    }
+    std::vector<int> ids(nsys), src(nsys), len(nsys), dst(nsys);
+    long long p = 0;
+    for (int i = 0; i < nsys; i++) {
+        int n = h->topos[topo_ids[i]].n;
+        long long off = alloc_atoms(h, n);
+        if (off < 0) {
+            for (int k = 0; k < i; k++) { free_atoms(h, h->hs[ids[k]].atom_off, h->hs[ids[k]].natoms); h->hs[ids[k]].active = 0; h->free_slots.push_back(ids[k]); }
+            return fail(h, SMR_ERR_CAPACITY, "atom capacity exhausted (%lld atoms requested)", need);
+        }
+        int s = h->free_slots.back();
+        h->free_slots.pop_back();
+        SlotState& st = h->hs[s];
+        st = SlotState{};
+        st.topo = topo_ids[i]; st.atom_off = (int)off; st.natoms = n; st.active = 1; st.dt = -1.0;
+        ids[i] = s; src[i] = (int)p; len[i] = n; dst[i] = (int)off;
+        for (int a = 0; a < n; a++) h->pinned[p + a] = make_float4(pos[3 * (p + a)], pos[3 * (p + a) + 1], pos[3 * (p + a) + 2], 0.f);
+        p += n;
+    }
+    if (nsys == 0) return SMR_OK;
+    cudaStream_t s = h->stream;
+    CU(h, cudaMemcpyAsync(h->stage, h->pinned, p * 16, cudaMemcpyHostToDevice, s));
+    std::vector<int> desc(3 * nsys);
+    std::copy(src.begin(), src.end(), desc.begin()); std::copy(len.begin(), len.end(), desc.begin() + nsys); std::copy(dst.begin(), dst.end(), desc.begin() + 2 * nsys);
+    CU(h, cudaMemcpyAsync(h->xfer, desc.data(), desc.size() * 4, cudaMemcpyHostToDevice, s));
+    if (launch_copy_segments(h->xfer, h->xfer + nsys, h->xfer + 2 * nsys, nsys, h->stage, h->pos, s)) return fail(h, SMR_ERR_CUDA, "scatter launch failed");
+    // zero velocities of the new ranges
+    for (int i = 0; i < nsys; i++) CU(h, cudaMemsetAsync(h->vel + dst[i], 0, (size_t)len[i] * 16, s));
+    int r = upload_slots(h, ids);
+    if (r) return r;
+    r = wait_stream(h, 600.0);
+    if (r) return r;
+    std::copy(ids.begin(), ids.end(), slot_ids);
+    return SMR_OK;
+}
+
+int smr_remove_systems(smr_handle* h, int nsys, const int* slot_ids) {
+    if (!h || nsys < 0 || (nsys && !slot_ids)) return SMR_ERR_ARG;
+    for (int i = 0; i < nsys; i++) if (!valid_slot(h, slot_ids[i])) return fail(h, SMR_ERR_ARG, "slot %d not active", slot_ids[i]);
+    std::vector<int> ids(slot_ids, slot_ids + nsys);
+    for (int s : ids) {
+        free_atoms(h, h->hs[s].atom_off, h->hs[s].natoms);
+        h->hs[s] = SlotState{};
+        h->free_slots.push_back(s);
+    }
+    return upload_slots(h, ids);
+}
+
+int smr_set_positions(smr_handle* h, int nsys, const int* slot_ids, const float* pos) {
+    if (!h || nsys < 0 || (nsys && (!slot_ids || !pos))) return SMR_ERR_ARG;
+    { int r = check_batch(h, nsys, slot_ids); if (r) return r; }
+    std::vector<int> src(nsys), len(nsys), dst(nsys);
+    long long p = 0;
+    for (int i = 0; i < nsys; i++) {
+        if (!valid_slot(h, slot_ids[i])) return fail(h, SMR_ERR_ARG, "slot %d not active", slot_ids[i]);
+        const SlotState& st = h->hs[slot_ids[i]];
+        src[i] = (int)p; len[i] = st.natoms; dst[i] = st.atom_off;
+        for (int a = 0; a < st.natoms; a++) h->pinned[p + a] = make_float4(pos[3 * (p + a)], pos[3 * (p + a) + 1], pos[3 * (p + a) + 2], 0.f);
+        p += st.natoms;
+    }
+    if (!nsys) return SMR_OK;
+    std::vector<int> desc(3 * nsys);
+    std::copy(src.begin(), src.end(), desc.begin()); std::copy(len.begin(), len.end(), desc.begin() + nsys); std::copy(dst.begin(), dst.end(), desc.begin() + 2 * nsys);
+    CU(h, cudaMemcpyAsync(h->stage, h->pinned, p * 16, cudaMemcpyHostToDevice, h->stream));
+    CU(h, cudaMemcpyAsync(h->xfer, desc.data(), desc.size() * 4, cudaMemcpyHostToDevice, h->stream));
+    if (launch_copy_segments(h->xfer, h->xfer + nsys, h->xfer + 2 * nsys, nsys, h->stage, h->pos, h->stream)) return fail(h, SMR_ERR_CUDA, "scatter launch failed");
+    return wait_stream(h, 600.0);
+}
+
+int smr_active_slots(smr_handle* h, int* n, int* ids) {
+    if (!h || !n) return SMR_ERR_ARG;
+    int c = 0;
+    for (int s = 0; s < h->max_systems; s++) if (h->hs[s].active) { if (ids) ids[c] = s; c++; }
+    *n = c;
+    return SMR_OK;
+}
+
+int smr_reset_fire(smr_handle* h, int nsys, const int* slot_ids) {
+    if (!h || nsys < 0 || (nsys && !slot_ids)) return SMR_ERR_ARG;
+    std::vector<int> ids;
+    for (int i = 0; i < nsys; i++) {
+        int s = slot_ids[i];
+        if (!valid_slot(h, s)) return fail(h, SMR_ERR_ARG, "slot %d not active", s);
+        SlotState& st = h->hs[s];
+        st.status = 0; st.steps = 0; st.npos = 0; st.dt = -1.0; st.alpha = 0; st.energy = 0; st.fmax = 0;
+        CU(h, cudaMemsetAsync(h->vel + st.atom_off, 0, (size_t)st.natoms * 16, h->stream));
+        ids.push_back(s);
+    }
+    int r = upload_slots(h, ids);
+    if (r) return r;
+    return wait_stream(h, 600.0);
+}
+
+int smr_eval_forces(smr_handle* h, int nsys, const int* slot_ids, float* forces, double* energy) {
+    if (!h || nsys < 0 || (nsys && !slot_ids)) return SMR_ERR_ARG;
+    { int r = check_batch(h, nsys, slot_ids); if (r) return r; }
+    for (int i = 0; i < nsys; i++) if (!valid_slot(h, slot_ids[i])) return fail(h, SMR_ERR_ARG, "slot %d not active", slot_ids[i]);
+    if (nsys == 0) return SMR_OK;
+    std::vector<int> ids(slot_ids, slot_ids + nsys);
+    std::vector<int> order(nsys);
+    for (int i = 0; i < nsys; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return h->htd[h->hs[ids[a]].topo].team < h->htd[h->hs[ids[b]].topo].team; });
+    std::vector<int> sorted(nsys);
+    for (int i = 0; i < nsys; i++) sorted[i] = ids[order[i]];
+    std::vector<int> tmp = sorted;
+    auto segs = group_by_team(h, tmp);
+    for (auto& g : segs) { int r = check_smem(h, g); if (r) return r; }
+    cudaStream_t s = h->stream;
+    CU(h, cudaMemcpyAsync(h->work, sorted.data(), nsys * 4, cudaMemcpyHostToDevice, s));
+    KernelArgs a = base_args(h);
+    h->last_launches = 0;
+    cudaEventRecord(h->ev0, s);
+    for (auto& g : segs) {
+        a.work = h->work + g.begin; a.nwork = g.end - g.begin; a.nmax = g.nmax;
+        a.ecomp = h->ecomp + (size_t)g.begin * 8;
+        CU(h, cudaMemsetAsync(h->counter, 0, 4, s));
+        int r = launch_relax(a, g.team, 1, s, h->num_sms, &h->last_launches);
+        if (r) return fail(h, SMR_ERR_CUDA, "eval launch: %s", cudaGetErrorString((cudaError_t)r));
+    }
+    cudaEventRecord(h->ev1, s);
+    int r = wait_stream(h, 600.0);
+    if (r) return r;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    h->last_ms = ms;
+    if (energy) {
+        std::vector<double> e((size_t)nsys * 8);
+        CU(h, cudaMemcpy(e.data(), h->ecomp, e.size() * 8, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < nsys; i++) std::copy(&e[(size_t)i * 8], &e[(size_t)i * 8 + 8], energy + (size_t)order[i] * 8);
+    }
+    if (forces) {
+        r = smr_download(h, nsys, slot_ids, nullptr, forces, nullptr, nullptr, nullptr);
+        if (r) return r;
+    }
+    return SMR_OK;
+}
+
+int smr_run_fire(smr_handle* h, int max_steps, int step_budget, const smr_fire_params* p, int mode, int* nfinished) {
+    if (!h || !p || max_steps < 0) return SMR_ERR_ARG;
+    if (mode != SMR_MODE_BATCHED && mode != SMR_MODE_PLAIN) return fail(h, SMR_ERR_ARG, "unknown mode %d", mode);
+    if (!(p->dt0 > 0 && p->dt_max > 0 && p->f_dec > 0 && p->f_inc > 0)) return fail(h, SMR_ERR_ARG, "invalid FIRE parameters");
+    std::vector<int> ids, fresh;
+    for (int s = 0; s < h->max_systems; s++) {
+        SlotState& st = h->hs[s];
+        if (!st.active || st.status != SMR_ST_RUNNING) continue;
+        if (st.dt < 0) { st.dt = p->dt0; st.alpha = p->alpha0; st.npos = 0; st.steps = 0; fresh.push_back(s); }
+        ids.push_back(s);
+    }
+    int r = upload_slots(h, fresh);
+    if (r) return r;
+    h->last_launches = 0;
+    cudaStream_t s = h->stream;
+    KernelArgs a = base_args(h);
+    a.fire = FireDev{p->dt0, p->dt_max, p->alpha0, p->f_inc, p->f_dec, p->f_alpha, p->fconv, p->flimit, p->n_min};
+    a.step_budget = step_budget;
+    auto segs = group_by_team(h, ids);
+    for (auto& g : segs) { r = check_smem(h, g); if (r) return r; }
+    if (!ids.empty()) CU(h, cudaMemcpyAsync(h->work, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice, s));
+    cudaEventRecord(h->ev0, s);
+    if (mode == SMR_MODE_BATCHED) {
+        a.max_steps = max_steps;
+        for (auto& g : segs) {
+            a.work = h->work + g.begin; a.nwork = g.end - g.begin; a.nmax = g.nmax;
+            CU(h, cudaMemsetAsync(h->counter, 0, 4, s));
+            int e = launch_relax(a, g.team, 0, s, h->num_sms, &h->last_launches);
+            if (e) return fail(h, SMR_ERR_CUDA, "relax launch: %s", cudaGetErrorString((cudaError_t)e));
+        }
+    } else {
+        // plain form: one launch per system per FIRE step, status read back after each step
+        a.max_steps = 1;
+        for (auto& g : segs) {
+            a.nmax = g.nmax; a.nwork = 1;
+            for (int k = g.begin; k < g.end; k++) {
+                a.work = h->work + k;
+                const int slot = ids[k];
+                for (int step = 0; step < max_steps; step++) {
+                    CU(h, cudaMemsetAsync(h->counter, 0, 4, s));
+                    int e = launch_relax(a, g.team, 0, s, h->num_sms, &h->last_launches);
+                    if (e) return fail(h, SMR_ERR_CUDA, "relax launch: %s", cudaGetErrorString((cudaError_t)e));
+                    int st = 0;
+                    CU(h, cudaMemcpyAsync(&st, &h->slots[slot].status, 4, cudaMemcpyDeviceToHost, s));
+                    CU(h, cudaStreamSynchronize(s));
+                    if (st != SMR_ST_RUNNING) break;
+                }
+            }
+        }
+    }
+    cudaEventRecord(h->ev1, s);
+    r = wait_stream(h, 3600.0);
+    if (r) return r;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    h->last_ms = ms;
+    r = download_slots(h);
+    if (r) return r;
+    if (nfinished) {
+        int c = 0;
+        for (int s2 = 0; s2 < h->max_systems; s2++) if (h->hs[s2].active && h->hs[s2].status != SMR_ST_RUNNING) c++;
+        *nfinished = c;
+    }
+    return SMR_OK;
+}
+
+int smr_download(smr_handle* h, int nsys, const int* slot_ids, float* pos, float* forces, double* energy, int* steps, int* status) {
+    if (!h || nsys < 0 || (nsys && !slot_ids)) return SMR_ERR_ARG;
+    { int r = check_batch(h, nsys, slot_ids); if (r) return r; }
+    for (int i = 0; i < nsys; i++) if (!valid_slot(h, slot_ids[i])) return fail(h, SMR_ERR_ARG, "slot %d not active", slot_ids[i]);
+    if (!nsys) return SMR_OK;
+    int r = download_slots(h);
+    if (r) return r;
+    std::vector<int> src(nsys), len(nsys), dst(nsys);
+    long long p = 0;
+    for (int i = 0; i < nsys; i++) {
+        const SlotState& st = h->hs[slot_ids[i]];
+        src[i] = st.atom_off; len[i] = st.natoms; dst[i] = (int)p;
+        p += st.natoms;
+        if (energy) { energy[(size_t)i * SMR_E_NCOMP] = st.energy; for (int c = 1; c < SMR_E_NCOMP; c++) energy[(size_t)i * SMR_E_NCOMP + c] = 0.0; }
+        if (steps) steps[i] = st.steps;
+        if (status) status[i] = st.status;
+    }
+    std::vector<int> desc(3 * nsys);
+    std::copy(src.begin(), src.end(), desc.begin()); std::copy(len.begin(), len.end(), desc.begin() + nsys); std::copy(dst.begin(), dst.end(), desc.begin() + 2 * nsys);
+    cudaStream_t s = h->stream;
+    CU(h, cudaMemcpyAsync(h->xfer, desc.data(), desc.size() * 4, cudaMemcpyHostToDevice, s));
+    for (int which = 0; which < 2; which++) {
+        float* out = which == 0 ? pos : forces;
+        if (!out) continue;
+        if (launch_copy_segments(h->xfer, h->xfer + nsys, h->xfer + 2 * nsys, nsys, which == 0 ? h->pos : h->force, h->stage, s))
+            return fail(h, SMR_ERR_CUDA, "gather launch failed");
+        CU(h, cudaMemcpyAsync(h->pinned, h->stage, p * 16, cudaMemcpyDeviceToHost, s));
+        r = wait_stream(h, 600.0);
+        if (r) return r;
+        if (which == 0) for (long long a = 0; a < p; a++) { out[3 * a] = h->pinned[a].x; out[3 * a + 1] = h->pinned[a].y; out[3 * a + 2] = h->pinned[a].z; }
+        else std::memcpy(out, h->pinned, p * 16);
+    }
+    return SMR_OK;
+}
+
+struct smr_topo { HostTopo T; };
+
+int smr_topo_build(int natoms, const int* Z, const double* pos, const double* charges, double bond_cut, smr_topo** out,
+                   char* err, int errlen) {
+    if (!Z || !pos || !out) return SMR_ERR_ARG;
+    *out = nullptr;
+    smr_topo* t = new (std::nothrow) smr_topo();
+    if (!t) return SMR_ERR_CAPACITY;
+    char msg[300] = {0};
+    if (build_molecule_topology(natoms, Z, pos, charges, bond_cut > 0 ? bond_cut : 1.8, t->T, msg, sizeof(msg))) {
+        if (err && errlen > 0) std::snprintf(err, errlen, "%s", msg);
+        delete t;
+        return SMR_ERR_ARG;
+    }
+    *out = t;
+    return SMR_OK;
+}
+
+void smr_topo_free(smr_topo* t) { delete t; }
+
+int smr_topo_counts(const smr_topo* t, int c[5]) {
+    if (!t || !c) return SMR_ERR_ARG;
+    c[0] = t->T.n; c[1] = (int)t->T.bonds.size() / 2; c[2] = (int)t->T.angs.size() / 3;
+    c[3] = (int)t->T.dihs.size() / 4; c[4] = (int)t->T.invs.size() / 4;
+    return SMR_OK;
+}
+
+int smr_topo_export(const smr_topo* t, int* neighs, int* neighBs, int* bonds, double* bparams,
+                    int* angs, int* ang_ngs, double* angp, int* dihs, int* dih_ngs, double* dihp,
+                    int* invs, int* inv_ngs, double* invp, double* req, int* type_id) {
+    if (!t) return SMR_ERR_ARG;
+    const HostTopo& T = t->T;
+    auto cp = [](auto* dst, const auto& v) { if (dst) std::copy(v.begin(), v.end(), dst); };
+    cp(neighs, T.neighs); cp(neighBs, T.neighBs); cp(bonds, T.bonds); cp(bparams, T.bparams);
+    cp(angs, T.angs); cp(ang_ngs, T.ang_ngs); cp(angp, T.angp);
+    cp(dihs, T.dihs); cp(dih_ngs, T.dih_ngs); cp(dihp, T.dihp);
+    cp(invs, T.invs); cp(inv_ngs, T.inv_ngs); cp(invp, T.invp);
+    cp(req, T.req); cp(type_id, T.type_id);
+    return SMR_OK;
+}
+
+int smr_topo_rounds(const smr_topo* t, int team, int rounds[3], short* ang_at, short* dih_at, short* inv_at) {
+    if (!t || !rounds || team <= 0) return SMR_ERR_ARG;
+    PackedTerms P;
+    pack_rounds(t->T, team, P);
+    rounds[0] = P.ang_rounds; rounds[1] = P.dih_rounds; rounds[2] = P.inv_rounds;
+    auto put = [](short* dst, const auto& recs) {
+        if (!dst) return;
+        for (size_t i = 0; i < recs.size(); i++) {
+            dst[4 * i] = recs[i].at.x; dst[4 * i + 1] = recs[i].at.y; dst[4 * i + 2] = recs[i].at.z; dst[4 * i + 3] = recs[i].at.w;
+        }
+    };
+    put(ang_at, P.ang); put(dih_at, P.dih); put(inv_at, P.inv);
+    return SMR_OK;
+}
+
+int smr_add_topo(smr_handle* h, const smr_topo* t, int* topo_id) {
+    if (!h || !t || !topo_id) return SMR_ERR_ARG;
+    h->topos.push_back(t->T);
+    append_topology(h, h->topos.back());
+    int r = upload_all(h);
+    if (r) return r;
+    *topo_id = (int)h->topos.size() - 1;
+    return SMR_OK;
+}
+
+int smr_last_timing(smr_handle* h, double* ms, long long* launches) {
+    if (!h) return SMR_ERR_ARG;
+    if (ms) *ms = h->last_ms;
+    if (launches) *launches = h->last_launches;
+    return SMR_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,480 @@
+// grid.cu -- substrate grid build on the device.
+//
+// Output: B-spline coefficients of (Pauli, London, Coulomb, 0) packed as float4 in the
+// z-fastest layout i = iz + nz*(iy + ny*ix) that the relaxation kernel samples.
+//
+//   Morse channels .... Pauli = sum_j E_j exp(-2a(r - R_j)), London = sum_j -2 E_j exp(-a(r - R_j))
+//                       over ions and (2 npbc + 1)^2 lateral images (opencl/gridff_build.cl:217-347,
+//                       make_MorseFF); FP32 terms, FP64 accumulation.
+//   Coulomb channel ... Ewald-2D for a slab below the grid (opencl/Surface.cl:716-906):
+//                         phi = K [ -(2pi/A) sum_i q_i (z - z_i)
+//                                   + Re sum_{G != 0} (2pi/(A|G|)) S_G exp(iG.rho) exp(-|G|(z - z0)) ]
+//                       with S_G = sum_i q_i exp(-iG.rho_i) exp(-|G|(z0 - z_i)), all in FP64.  S_G is
+//                       built per ion layer from separable phase tables; phi on each z plane is a
+//                       two-stage partial DFT (over h, then over k), skipping G whose amplitude is
+//                       below ewald_tol of the largest.
+//   B-spline fit ...... exact solution of Conv(c) = V for the forward operator of BsplineConv3D
+//                       (opencl/gridff_build.cl:8-61): separable tridiag(1/6, 2/3, 1/6) solves, cyclic
+//                       (Sherman-Morrison) in x and y, zero-padded in z; FP64.
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <cuda_bf16.h>
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <vector>
+
+#include "smr_internal.h"
+
+namespace smr {
+namespace {
+
+constexpr double kCoulombD = 14.3996448915;
+constexpr double kPi = 3.14159265358979323846;
+
+#define GB_CHECK(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) { std::snprintf(err, errlen, "%s: %s", #x, cudaGetErrorString(e_)); return -1; } } while (0)
+
+// ---------------------------------------------------------------- Morse
+__global__ void morse_kernel(int nions, const double* __restrict__ ions, const double* __restrict__ re,
+                             double Lx, double Ly, int npbc, int nx, int ny, int nz, double p0x, double p0y, double p0z,
+                             double sx, double sy, double sz, float alpha, float rcut2, double* __restrict__ paul,
+                             double* __restrict__ lond) {
+    __shared__ float4 sI[128];
+    __shared__ float2 sR[128];
+    const size_t N = (size_t)nx * ny * nz;
+    const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = idx < N;
+    const int iz = (int)(idx % nz), iy = (int)((idx / nz) % ny), ix = (int)(idx / ((size_t)nz * ny));
+    // grid point relative coordinates in FP64, then FP32 per term
+    const double px = p0x + ix * sx, py = p0y + iy * sy, pz = p0z + iz * sz;
+    double P = 0.0, Lo = 0.0;
+    for (int j0 = 0; j0 < nions; j0 += 128) {
+        const int j = j0 + threadIdx.x;
+        if (threadIdx.x < 128) {
+            if (j < nions) {
+                sI[threadIdx.x] = make_float4((float)ions[4 * j], (float)ions[4 * j + 1], (float)ions[4 * j + 2], 0.f);
+                sR[threadIdx.x] = make_float2((float)re[4 * j], (float)re[4 * j + 1]);
+            }
+        }
+        __syncthreads();
+        const int m = min(128, nions - j0);
+        if (live) {
+            for (int k = 0; k < m; k++) {
+                const float4 a = sI[k];
+                const float2 r = sR[k];
+                // displacement to the nearest copy handled by summing all images explicitly
+                const float dx0 = (float)(px - (double)a.x), dy0 = (float)(py - (double)a.y), dz = (float)(pz - (double)a.z);
+                float sp = 0.f, sl = 0.f;
+                for (int jy = -npbc; jy <= npbc; jy++)
+                    for (int jx = -npbc; jx <= npbc; jx++) {
+                        const float dx = dx0 + jx * (float)Lx, dy = dy0 + jy * (float)Ly;
+                        const float r2 = dx * dx + dy * dy + dz * dz;
+                        if (r2 > rcut2) continue;
+                        const float rr = sqrtf(r2 + 1e-32f);
+                        const float e = expf(-alpha * (rr - r.x));
+                        const float eM = r.y * e;
+                        sp += eM * e;
+                        sl += -2.0f * eM;
+                    }
+                P += (double)sp; Lo += (double)sl;
+            }
+        }
+        __syncthreads();
+    }
+    if (live) { paul[idx] = P; lond[idx] = Lo; }
+}
+
+// ---------------------------------------------------------------- Ewald-2D
+// phase tables: X[i*(2H+1) + (h+H)] = exp(-i h g1 x_i), Y[i*(2K+1) + (k+K)] = exp(-i k g2 y_i)
+__global__ void phase_table_kernel(int nions, const double* __restrict__ ions, int comp, double g, int H, double2* __restrict__ X) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int w = 2 * H + 1;
+    if (t >= nions * w) return;
+    const int i = t / w, h = t % w - H;
+    double s, c;
+    sincos(-(double)h * g * ions[4 * i + comp], &s, &c);
+    X[t] = make_double2(c, s);
+}
+
+// S[(k+K)*(2H+1) + (h+H)] = sum_layers exp(-|G| d_l) sum_{i in l} q_i X_i(h) Y_i(k)
+__global__ void structure_factor_kernel(int nions, const double* __restrict__ ions, const double* __restrict__ dz_ion,
+                                        const double2* __restrict__ X, const double2* __restrict__ Y, int H, int K,
+                                        double g1, double g2, double2* __restrict__ S) {
+    const int w = 2 * H + 1;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= w * (2 * K + 1)) return;
+    const int hh = t % w, kk = t / w;
+    const double Gx = (hh - H) * g1, Gy = (kk - K) * g2, Gn = sqrt(Gx * Gx + Gy * Gy);
+    double sr = 0.0, si = 0.0;
+    for (int i = 0; i < nions; i++) {
+        const double2 a = X[(size_t)i * w + hh];
+        const double2 b = Y[(size_t)i * (2 * K + 1) + kk];
+        const double q = ions[4 * i + 3] * exp(-Gn * dz_ion[i]);
+        sr += q * (a.x * b.x - a.y * b.y);
+        si += q * (a.x * b.y + a.y * b.x);
+    }
+    S[t] = make_double2(sr, si);
+}
+
+// phase table out[r*n + i] = exp(i m_r g (p0 + i s)) for integer multipliers m_r
+__global__ void line_phase_kernel(int nrows, const int* __restrict__ mult, int n, double p0, double st, double g,
+                                  double2* __restrict__ out) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nrows * n) return;
+    const int r = t / n, i = t % n;
+    double s, c;
+    sincos((double)mult[r] * g * (p0 + i * st), &s, &c);
+    out[t] = make_double2(c, s);
+}
+
+// amplitudes of one z plane: amp0 * exp(-|G| (z - z0)), zeroed below the pruning threshold
+__global__ void plane_amp_kernel(int ne, const double2* __restrict__ amp0, const double* __restrict__ gnorm, double dzp,
+                                 double thresh, double2* __restrict__ out) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= ne) return;
+    const double d = exp(-gnorm[e] * dzp);
+    const double2 a = amp0[e];
+    out[e] = ((fabs(a.x) + fabs(a.y)) * d < thresh) ? make_double2(0.0, 0.0) : make_double2(a.x * d, a.y * d);
+}
+
+// Stage 1: B[r*nx + ix] = sum_{e in row r} amp[e] * Ex[hidx[e]*nx + ix]
+__global__ void ewald_stage1(int nrows, const int* __restrict__ rowptr, const int* __restrict__ hidx,
+                             const double2* __restrict__ amp, const double2* __restrict__ Ex, int nx, double2* __restrict__ B) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nrows * nx) return;
+    const int r = t / nx, ix = t % nx;
+    double br = 0.0, bi = 0.0;
+    for (int e = rowptr[r]; e < rowptr[r + 1]; e++) {
+        const double2 a = amp[e];
+        const double2 c = Ex[(size_t)hidx[e] * nx + ix];
+        br += a.x * c.x - a.y * c.y;
+        bi += a.x * c.y + a.y * c.x;
+    }
+    B[t] = make_double2(br, bi);
+}
+
+// Stage 2: phi(ix, iy) = K (phi0 + Re sum_r B[r, ix] Ey[r, iy])
+__global__ void ewald_stage2(int nrows, const double2* __restrict__ B, const double2* __restrict__ Ey, int nx, int ny,
+                             double phi0, int iz, int nz, double* __restrict__ out) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nx * ny) return;
+    const int iy = t % ny, ix = t / ny;
+    double acc = 0.0;
+    for (int r = 0; r < nrows; r++) {
+        const double2 b = B[(size_t)r * nx + ix];
+        const double2 c = Ey[(size_t)r * ny + iy];
+        acc += b.x * c.x - b.y * c.y;
+    }
+    out[(size_t)iz + (size_t)nz * ((size_t)iy + (size_t)ny * ix)] = kCoulombD * (phi0 + acc);
+}
+
+// ---------------------------------------------------------------- B-spline fit
+// Line solve of tridiag(a, b, a) x = d with precomputed forward coefficients cp[] and
+// pivots m[]: d'[0] = d[0]/m[0], d'[i] = (d[i] - a d'[i-1]) / m[i]; x[i] = d'[i] - cp[i] x[i+1].
+__device__ __forceinline__ void thomas_line(double* x, size_t st, int n, const double* cp, const double* m) {
+    const double a = 1.0 / 6.0;
+    double prev = x[0] / m[0];
+    x[0] = prev;
+    for (int i = 1; i < n; i++) { prev = (x[(size_t)i * st] - a * prev) / m[i]; x[(size_t)i * st] = prev; }
+    double nxt = x[(size_t)(n - 1) * st];
+    for (int i = n - 2; i >= 0; i--) { nxt = x[(size_t)i * st] - cp[i] * nxt; x[(size_t)i * st] = nxt; }
+}
+
+// periodic correction: x -= fact * u with fact = (x0 + a x_{n-1}/gamma) / den
+__device__ __forceinline__ void cyclic_fix(double* x, size_t st, int n, const double* u, double gamma, double den) {
+    const double a = 1.0 / 6.0;
+    const double fact = (x[0] + a * x[(size_t)(n - 1) * st] / gamma) / den;
+    for (int i = 0; i < n; i++) x[(size_t)i * st] -= fact * u[i];
+}
+
+struct LineCoef { double* cp; double* m; double* u; double gamma, den; int n; bool periodic; };
+
+__global__ void fit_z(double* v, int nx, int ny, int nz, const double* cp, const double* m) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nx * ny) return;
+    thomas_line(v + (size_t)t * nz, 1, nz, cp, m);
+}
+__global__ void fit_y(double* v, int nx, int ny, int nz, const double* cp, const double* m, const double* u, double gamma, double den) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nx * nz) return;
+    const int iz = t % nz, ix = t / nz;
+    double* x = v + iz + (size_t)nz * ny * ix;
+    thomas_line(x, nz, ny, cp, m);
+    cyclic_fix(x, nz, ny, u, gamma, den);
+}
+__global__ void fit_x(double* v, int nx, int ny, int nz, const double* cp, const double* m, const double* u, double gamma, double den) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ny * nz) return;
+    const int iz = t % nz, iy = t / nz;
+    double* x = v + iz + (size_t)nz * iy;
+    thomas_line(x, (size_t)nz * ny, nx, cp, m);
+    cyclic_fix(x, (size_t)nz * ny, nx, u, gamma, den);
+}
+
+__global__ void pack_kernel(size_t N, const double* __restrict__ c0, const double* __restrict__ c1, const double* __restrict__ c2,
+                            float4* __restrict__ out) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    out[i] = make_float4((float)c0[i], (float)c1[i], (float)c2[i], 0.f);
+}
+
+// host: Thomas coefficients of tridiag(1/6, b0|2/3..|bn, 1/6)
+void thomas_coefs(int n, double b0, double bn, std::vector<double>& cp, std::vector<double>& m) {
+    const double a = 1.0 / 6.0, b = 2.0 / 3.0;
+    cp.assign(n, 0.0); m.assign(n, 0.0);
+    m[0] = b0; cp[0] = a / m[0];
+    for (int i = 1; i < n; i++) {
+        const double di = (i == n - 1) ? bn : b;
+        m[i] = di - a * cp[i - 1];
+        cp[i] = a / m[i];
+    }
+}
+void thomas_host(std::vector<double>& x, const std::vector<double>& cp, const std::vector<double>& m) {
+    const double a = 1.0 / 6.0;
+    int n = (int)x.size();
+    x[0] /= m[0];
+    for (int i = 1; i < n; i++) x[i] = (x[i] - a * x[i - 1]) / m[i];
+    for (int i = n - 2; i >= 0; i--) x[i] -= cp[i] * x[i + 1];
+}
+
+struct DevBuf {
+    std::vector<void*> ptrs;
+    ~DevBuf() { for (void* p : ptrs) cudaFree(p); }
+    template <class T> cudaError_t alloc(T** p, size_t n) {
+        cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(n, 1) * sizeof(T));
+        if (e == cudaSuccess) ptrs.push_back(*p);
+        return e;
+    }
+};
+
+int fit_channel(double* d, int nx, int ny, int nz, cudaStream_t s, DevBuf& buf, char* err, int errlen) {
+    const double a = 1.0 / 6.0, b = 2.0 / 3.0;
+    // z: open (zero padded)
+    {
+        std::vector<double> cp, m;
+        thomas_coefs(nz, b, b, cp, m);
+        double *dcp, *dm;
+        GB_CHECK(buf.alloc(&dcp, nz)); GB_CHECK(buf.alloc(&dm, nz));
+        GB_CHECK(cudaMemcpyAsync(dcp, cp.data(), nz * 8, cudaMemcpyHostToDevice, s));
+        GB_CHECK(cudaMemcpyAsync(dm, m.data(), nz * 8, cudaMemcpyHostToDevice, s));
+        fit_z<<<(nx * ny + 127) / 128, 128, 0, s>>>(d, nx, ny, nz, dcp, dm);
+        GB_CHECK(cudaGetLastError());
+        GB_CHECK(cudaStreamSynchronize(s));
+    }
+    // y and x: cyclic, gamma = -b (tridiagonal part with modified corners + rank-one correction)
+    for (int axis = 0; axis < 2; axis++) {
+        const int n = axis == 0 ? ny : nx;
+        const double gamma = -b;
+        std::vector<double> cp, m, u(n, 0.0);
+        thomas_coefs(n, b - gamma, b - a * a / gamma, cp, m);
+        u[0] = gamma; u[n - 1] = a;
+        thomas_host(u, cp, m);
+        const double den = 1.0 + u[0] + a * u[n - 1] / gamma;
+        double *dcp, *dm, *du;
+        GB_CHECK(buf.alloc(&dcp, n)); GB_CHECK(buf.alloc(&dm, n)); GB_CHECK(buf.alloc(&du, n));
+        GB_CHECK(cudaMemcpyAsync(dcp, cp.data(), n * 8, cudaMemcpyHostToDevice, s));
+        GB_CHECK(cudaMemcpyAsync(dm, m.data(), n * 8, cudaMemcpyHostToDevice, s));
+        GB_CHECK(cudaMemcpyAsync(du, u.data(), n * 8, cudaMemcpyHostToDevice, s));
+        if (axis == 0) fit_y<<<(nx * nz + 127) / 128, 128, 0, s>>>(d, nx, ny, nz, dcp, dm, du, gamma, den);
+        else fit_x<<<(ny * nz + 127) / 128, 128, 0, s>>>(d, nx, ny, nz, dcp, dm, du, gamma, den);
+        GB_CHECK(cudaGetLastError());
+        GB_CHECK(cudaStreamSynchronize(s));
+    }
+    return 0;
+}
+
+// ---------------------------------------------------------------- 16-bit encoding
+__global__ void absmax_kernel(size_t N, const float4* __restrict__ src, unsigned int* __restrict__ mx) {
+    float m[4] = {0.f, 0.f, 0.f, 0.f};
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x) {
+        const float4 v = src[i];
+        m[0] = fmaxf(m[0], fabsf(v.x)); m[1] = fmaxf(m[1], fabsf(v.y)); m[2] = fmaxf(m[2], fabsf(v.z)); m[3] = fmaxf(m[3], fabsf(v.w));
+    }
+    for (int c = 0; c < 4; c++) {
+        float v = m[c];
+        for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if ((threadIdx.x & 31) == 0) atomicMax(mx + c, __float_as_uint(v));   // non-negative floats order as uints
+    }
+}
+__global__ void encode_kernel(size_t N, const float4* __restrict__ src, uint2* __restrict__ dst, int dtype, float4 inv) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const float4 v = src[i];
+    uint2 o;
+    if (dtype == GRID_F16) {
+        __half2 a = __floats2half2_rn(v.x * inv.x, v.y * inv.y), b = __floats2half2_rn(v.z * inv.z, v.w * inv.w);
+        o.x = *reinterpret_cast<unsigned*>(&a); o.y = *reinterpret_cast<unsigned*>(&b);
+    } else {
+        __nv_bfloat162 a = __floats2bfloat162_rn(v.x * inv.x, v.y * inv.y), b = __floats2bfloat162_rn(v.z * inv.z, v.w * inv.w);
+        o.x = *reinterpret_cast<unsigned*>(&a); o.y = *reinterpret_cast<unsigned*>(&b);
+    }
+    dst[i] = o;
+}
+__global__ void decode_kernel(size_t N, const uint2* __restrict__ src, float4* __restrict__ dst, int dtype, float4 sc) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const uint2 u = src[i];
+    float2 a, b;
+    if (dtype == GRID_F16) { a = __half22float2(*reinterpret_cast<const __half2*>(&u.x)); b = __half22float2(*reinterpret_cast<const __half2*>(&u.y)); }
+    else { a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.x)); b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.y)); }
+    dst[i] = make_float4(a.x * sc.x, a.y * sc.y, b.x * sc.z, b.y * sc.w);
+}
+
+}  // namespace
+
+int encode_grid_16(const float4* src, void* dst, size_t nvox, int dtype, float scale_out[4], cudaStream_t s) {
+    unsigned int* dmx;
+    if (cudaMalloc(&dmx, 16) != cudaSuccess) return -1;
+    cudaMemsetAsync(dmx, 0, 16, s);
+    absmax_kernel<<<1024, 256, 0, s>>>(nvox, src, dmx);
+    unsigned int hm[4];
+    cudaMemcpyAsync(hm, dmx, 16, cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) { cudaFree(dmx); return -1; }
+    cudaFree(dmx);
+    float inv[4];
+    for (int c = 0; c < 4; c++) {
+        float m;
+        std::memcpy(&m, &hm[c], 4);
+        // power-of-two scale: fp16 maps max|c| to [16384, 32768) (headroom below 65504, full
+        // normal range below); bf16 has the fp32 exponent range and only needs max|c| ~ 1.
+        float sc = 1.f;
+        if (m > 0.f) sc = std::ldexp(1.0f, (int)std::ceil(std::log2((double)m)) - (dtype == GRID_F16 ? 15 : 0));
+        scale_out[c] = sc;
+        inv[c] = 1.f / sc;
+    }
+    encode_kernel<<<(unsigned)((nvox + 255) / 256), 256, 0, s>>>(nvox, src, (uint2*)dst, dtype, make_float4(inv[0], inv[1], inv[2], inv[3]));
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int decode_grid_16(const void* src, float4* dst, size_t nvox, int dtype, const float scale[4], cudaStream_t s) {
+    decode_kernel<<<(unsigned)((nvox + 255) / 256), 256, 0, s>>>(nvox, (const uint2*)src, dst, dtype, make_float4(scale[0], scale[1], scale[2], scale[3]));
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int build_grid_device(const GridBuildArgs& A, float4* out, cudaStream_t s, char* err, int errlen) {
+    const int nx = A.nx, ny = A.ny, nz = A.nz;
+    const size_t N = (size_t)nx * ny * nz;
+    DevBuf buf;
+    // host copy of ions for layer grouping and the geometry checks
+    std::vector<double> hion(4 * (size_t)A.nions);
+    GB_CHECK(cudaMemcpy(hion.data(), A.ions, hion.size() * 8, cudaMemcpyDeviceToHost));
+    double ztop = -1e300, qsum = 0.0, qz = 0.0;
+    for (int i = 0; i < A.nions; i++) { ztop = std::max(ztop, hion[4 * i + 2]); qsum += hion[4 * i + 3]; qz += hion[4 * i + 3] * hion[4 * i + 2]; }
+    const double dmin = A.p0[2] - ztop;
+    if (!(dmin > 0.05)) { std::snprintf(err, errlen, "grid bottom z=%g must lie above the top ion z=%g", A.p0[2], ztop); return -1; }
+    if (std::fabs(qsum) > 1e-6 * std::max(1.0, (double)A.nions)) { std::snprintf(err, errlen, "slab charge %g is not neutral", qsum); return -1; }
+
+    double *paul, *lond, *coul;
+    GB_CHECK(buf.alloc(&paul, N)); GB_CHECK(buf.alloc(&lond, N)); GB_CHECK(buf.alloc(&coul, N));
+
+    // Morse channels
+    {
+        const float rc2 = A.morse_rcut > 0 ? (float)(A.morse_rcut * A.morse_rcut) : 3.0e38f;
+        const unsigned blocks = (unsigned)((N + 127) / 128);
+        morse_kernel<<<blocks, 128, 0, s>>>(A.nions, A.ions, A.ion_re, A.Lx, A.Ly, A.npbc, nx, ny, nz, A.p0[0], A.p0[1], A.p0[2],
+                                            A.step[0], A.step[1], A.step[2], (float)A.alpha, rc2, paul, lond);
+        GB_CHECK(cudaGetLastError());
+    }
+
+    // Ewald-2D
+    {
+        const double g1 = 2.0 * kPi / A.Lx, g2 = 2.0 * kPi / A.Ly, area = A.Lx * A.Ly;
+        const double tol = A.ewald_tol > 0 ? A.ewald_tol : 1e-12;
+        const double gmax = -std::log(tol) / dmin;
+        const int H = std::max(1, (int)std::floor(gmax / g1)), K = std::max(1, (int)std::floor(gmax / g2));
+        const int w = 2 * H + 1, nk = 2 * K + 1;
+        std::vector<double> hdz(A.nions);
+        for (int i = 0; i < A.nions; i++) hdz[i] = A.p0[2] - hion[4 * i + 2];
+        double* ddz;
+        double2 *X, *Y, *S;
+        GB_CHECK(buf.alloc(&ddz, A.nions));
+        GB_CHECK(cudaMemcpyAsync(ddz, hdz.data(), A.nions * 8, cudaMemcpyHostToDevice, s));
+        GB_CHECK(buf.alloc(&X, (size_t)A.nions * w)); GB_CHECK(buf.alloc(&Y, (size_t)A.nions * nk)); GB_CHECK(buf.alloc(&S, (size_t)w * nk));
+        phase_table_kernel<<<(A.nions * w + 255) / 256, 256, 0, s>>>(A.nions, A.ions, 0, g1, H, X);
+        phase_table_kernel<<<(A.nions * nk + 255) / 256, 256, 0, s>>>(A.nions, A.ions, 1, g2, K, Y);
+        structure_factor_kernel<<<(w * nk + 127) / 128, 128, 0, s>>>(A.nions, A.ions, ddz, X, Y, H, K, g1, g2, S);
+        GB_CHECK(cudaGetLastError());
+        std::vector<double2> hS((size_t)w * nk);
+        GB_CHECK(cudaMemcpy(hS.data(), S, hS.size() * sizeof(double2), cudaMemcpyDeviceToHost));
+        // amplitudes at the grid bottom and their pruning threshold
+        std::vector<double2> amp;
+        std::vector<int> hcol, rowptr(1, 0), krow;
+        std::vector<double> gn;
+        double amax = 0.0;
+        for (int kk = 0; kk < nk; kk++)
+            for (int hh = 0; hh < w; hh++) {
+                if (hh == H && kk == K) continue;
+                const double Gx = (hh - H) * g1, Gy = (kk - K) * g2, G = std::sqrt(Gx * Gx + Gy * Gy);
+                if (G > gmax) continue;
+                const double2 v = hS[(size_t)kk * w + hh];
+                amax = std::max(amax, (std::fabs(v.x) + std::fabs(v.y)) * 2.0 * kPi / (area * G));
+            }
+        const double thresh = tol * std::max(amax, 1e-300);
+        for (int kk = 0; kk < nk; kk++) {
+            bool any = false;
+            for (int hh = 0; hh < w; hh++) {
+                if (hh == H && kk == K) continue;
+                const double Gx = (hh - H) * g1, Gy = (kk - K) * g2, G = std::sqrt(Gx * Gx + Gy * Gy);
+                if (G > gmax) continue;
+                const double2 v = hS[(size_t)kk * w + hh];
+                const double pref = 2.0 * kPi / (area * G);
+                if ((std::fabs(v.x) + std::fabs(v.y)) * pref < thresh) continue;
+                amp.push_back(make_double2(v.x * pref, v.y * pref));
+                hcol.push_back(hh - H);
+                gn.push_back(G);
+                any = true;
+            }
+            if (any) { rowptr.push_back((int)amp.size()); krow.push_back(kk - K); }
+        }
+        const int nrows = (int)krow.size();
+        const int ne = (int)amp.size();
+        // h multipliers used anywhere -> compact column index into the x phase table
+        std::vector<int> hmul;
+        for (int h = -H; h <= H; h++) hmul.push_back(h);
+        std::vector<int> hidx(ne);
+        for (int e = 0; e < ne; e++) hidx[e] = hcol[e] + H;
+        int *drow, *dhidx, *dk, *dhm;
+        double2 *damp, *dampz, *B, *Ex, *Ey;
+        double* dgn;
+        GB_CHECK(buf.alloc(&drow, rowptr.size())); GB_CHECK(buf.alloc(&dhidx, ne)); GB_CHECK(buf.alloc(&dk, nrows));
+        GB_CHECK(buf.alloc(&dhm, hmul.size()));
+        GB_CHECK(buf.alloc(&damp, ne)); GB_CHECK(buf.alloc(&dampz, ne)); GB_CHECK(buf.alloc(&dgn, ne));
+        GB_CHECK(buf.alloc(&B, (size_t)std::max(nrows, 1) * nx));
+        GB_CHECK(buf.alloc(&Ex, hmul.size() * (size_t)nx)); GB_CHECK(buf.alloc(&Ey, (size_t)std::max(nrows, 1) * ny));
+        GB_CHECK(cudaMemcpyAsync(drow, rowptr.data(), rowptr.size() * 4, cudaMemcpyHostToDevice, s));
+        GB_CHECK(cudaMemcpyAsync(dhm, hmul.data(), hmul.size() * 4, cudaMemcpyHostToDevice, s));
+        line_phase_kernel<<<(unsigned)((hmul.size() * nx + 255) / 256), 256, 0, s>>>((int)hmul.size(), dhm, nx, A.p0[0], A.step[0], g1, Ex);
+        if (ne > 0) {
+            GB_CHECK(cudaMemcpyAsync(dhidx, hidx.data(), ne * 4, cudaMemcpyHostToDevice, s));
+            GB_CHECK(cudaMemcpyAsync(damp, amp.data(), ne * sizeof(double2), cudaMemcpyHostToDevice, s));
+            GB_CHECK(cudaMemcpyAsync(dgn, gn.data(), ne * 8, cudaMemcpyHostToDevice, s));
+            GB_CHECK(cudaMemcpyAsync(dk, krow.data(), nrows * 4, cudaMemcpyHostToDevice, s));
+            line_phase_kernel<<<(unsigned)(((size_t)nrows * ny + 255) / 256), 256, 0, s>>>(nrows, dk, ny, A.p0[1], A.step[1], g2, Ey);
+        }
+        GB_CHECK(cudaGetLastError());
+        for (int iz = 0; iz < nz; iz++) {
+            const double z = A.p0[2] + iz * A.step[2];
+            const double phi0 = -(2.0 * kPi / area) * (qsum * z - qz);
+            if (nrows > 0) {
+                plane_amp_kernel<<<(ne + 255) / 256, 256, 0, s>>>(ne, damp, dgn, iz * A.step[2], thresh, dampz);
+                ewald_stage1<<<(nrows * nx + 127) / 128, 128, 0, s>>>(nrows, drow, dhidx, dampz, Ex, nx, B);
+            }
+            ewald_stage2<<<(nx * ny + 127) / 128, 128, 0, s>>>(nrows, B, Ey, nx, ny, phi0, iz, nz, coul);
+            GB_CHECK(cudaGetLastError());
+        }
+        GB_CHECK(cudaStreamSynchronize(s));
+    }
+
+    // exact B-spline fit of each channel, then pack
+    if (fit_channel(paul, nx, ny, nz, s, buf, err, errlen)) return -1;
+    if (fit_channel(lond, nx, ny, nz, s, buf, err, errlen)) return -1;
+    if (fit_channel(coul, nx, ny, nz, s, buf, err, errlen)) return -1;
+    pack_kernel<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(N, paul, lond, coul, out);
+    GB_CHECK(cudaGetLastError());
+    GB_CHECK(cudaStreamSynchronize(s));
+    return 0;
+}
+
+}  // namespace smr

@@ -1,0 +1,127 @@
+// smr_internal.h -- layouts shared by the host runtime (abi.cpp, topology.cpp) and
+// the CUDA kernels (relax.cu, grid.cu).  Device memory is laid out as:
+//
+//   per atom of a topology (arena, indexed by TopoDev::atom_off + local atom):
+//     float4 req   (R_vdW, sqrt(E_vdW), Q, H)
+//     short4 neigh (up to 4 bonded neighbours, -1 padded; local indices)
+//     float4 bk, bl (bond k and l0 of each neighbour slot)
+//   per term, in "rounds" of T records (T = team size of the topology's class):
+//     AngRec / DihRec / InvRec, 32 B each; within one round the atoms in each
+//     role are pairwise distinct, so a team adds the round's force pieces to its
+//     shared-memory force array without atomics and in a fixed order.
+//   per atom of a system (state arena, indexed by SlotState::atom_off + local atom):
+//     float4 pos, vel, force (force.w = per-atom energy)
+//   per system: SlotState (FIRE state, status, energy)
+//   grid: z-fastest i = iz + nz*(iy + ny*ix), float4 or 4 x 16-bit per voxel.
+#pragma once
+#include <cstdint>
+#include <vector>
+#include <cuda_runtime.h>
+
+namespace smr {
+
+struct __align__(16) AngRec { short4 at; short4 sl; float4 p; };   // at (i,j,k,-) sl (ji,jk,-,-) p (K*c0..K*c3)
+struct __align__(16) DihRec { short4 at; short4 sl; float4 p; };   // at (i,j,k,l) sl (ji,jk,kl,-) p (V, d, n, -)
+struct __align__(16) InvRec { short4 at; short4 sl; float4 p; };   // at (i,j,k,l) sl (ij,ik,il,-) p (K, c0, c1, c2)
+
+static_assert(sizeof(AngRec) == 32 && sizeof(DihRec) == 32 && sizeof(InvRec) == 32, "record size");
+
+struct TopoDev {
+    int natoms;
+    int atom_off;                 // into req / neigh / bk / bl
+    int ang_off, ang_rounds;      // into the AngRec arena; ang_rounds * team records
+    int dih_off, dih_rounds;
+    int inv_off, inv_rounds;
+    int team;                     // team size the rounds were packed for
+    int pad[3];
+};
+
+struct SlotState {
+    int topo;                     // topology id
+    int atom_off;                 // into pos / vel / force
+    int natoms;
+    int status;                   // SMR_ST_*
+    int steps;                    // FIRE steps done
+    int npos;                     // FIRE consecutive uphill-free steps
+    int active;                   // slot in use
+    int pad0;
+    double dt, alpha;             // FIRE adaptive state
+    double energy;                // total physical energy at the last force evaluation
+    float fmax;                   // max |F| at the last force evaluation
+    float pad1;
+};
+
+enum GridDtype { GRID_F32 = 0, GRID_F16 = 1, GRID_BF16 = 2 };
+
+struct GridView {
+    const void* data;
+    int dtype;
+    int nx, ny, nz;
+    float p0[3];
+    float inv_step[3];
+    float scale[4];
+};
+
+struct FireDev {
+    double dt0, dt_max, alpha0, f_inc, f_dec, f_alpha, fconv, flimit;
+    int n_min;
+};
+
+struct KernelArgs {
+    const int* work; int nwork; int* counter;
+    SlotState* slots;
+    const TopoDev* topos;
+    const float4* req; const short4* neigh; const float4* bk; const float4* bl;
+    const AngRec* angs; const DihRec* dihs; const InvRec* invs;
+    float4* pos; float4* vel; float4* force;
+    GridView grid; int has_grid;
+    float R2damp, alpha_morse, rc2;
+    FireDev fire;
+    int max_steps;                // steps this launch
+    int step_budget;              // cap on SlotState::steps (<=0: none)
+    double* ecomp;                // eval mode: per work item x 8 energy components
+    int nmax;                     // max atoms of a system in this launch (shared-memory sizing)
+};
+
+// ---- host topology (topology.cpp)
+struct HostTopo {
+    int n = 0;
+    std::vector<int> neighs, neighBs;                 // 4n
+    std::vector<int> bonds; std::vector<double> bparams;
+    std::vector<int> angs, ang_ngs; std::vector<double> angp;   // 3, 2, 5 per angle
+    std::vector<int> dihs, dih_ngs; std::vector<double> dihp;   // 4, 3, 3
+    std::vector<int> invs, inv_ngs; std::vector<double> invp;   // 4, 3, 4
+    std::vector<double> req;                          // 4n
+    std::vector<double> bond_kl;                      // 8n: (k, l0) per neighbour slot
+    std::vector<int> type_id;                         // n
+};
+
+struct PackedTerms {
+    std::vector<AngRec> ang; std::vector<DihRec> dih; std::vector<InvRec> inv;
+    int ang_rounds = 0, dih_rounds = 0, inv_rounds = 0;
+};
+
+// topology.cpp
+int build_molecule_topology(int n, const int* Z, const double* pos, const double* q, double bond_cut, HostTopo& T,
+                            char* err, int errlen);
+int build_desc_topology(int natoms, const double* req, const int* neighs, const double* bond_kl,
+                        int nang, const int* angs, const double* angp, int ndih, const int* dihs, const double* dihp,
+                        int ninv, const int* invs, const double* invp, HostTopo& T, char* err, int errlen);
+void pack_rounds(const HostTopo& T, int team, PackedTerms& out);
+const char* type_name(int id);
+
+// relax.cu
+int launch_relax(const KernelArgs& a, int team, int eval_only, cudaStream_t s, int num_sms, long long* launches);
+size_t team_smem_bytes(int nmax);
+
+// grid.cu
+struct GridBuildArgs {
+    int nions; const double* ions; const double* ion_re;   // device pointers, 4 doubles per ion
+    double Lx, Ly; int nx, ny, nz; double p0[3], step[3];
+    double alpha; int npbc; double ewald_tol; double morse_rcut;
+};
+int build_grid_device(const GridBuildArgs& a, float4* out_f32, cudaStream_t s, char* err, int errlen);
+int encode_grid_16(const float4* src, void* dst, size_t nvox, int dtype, float scale_out[4], cudaStream_t s);
+int decode_grid_16(const void* src, float4* dst, size_t nvox, int dtype, const float scale[4], cudaStream_t s);
+
+}  // namespace smr

@@ -1,0 +1,334 @@
+"""Python host interface over the C ABI: the multi-system relaxation driver.
+
+``RelaxMulti`` mirrors the shape of the reference's multi-replica GPU harness
+(crates/libs/oclff/src/rrsp3.rs:699-1088, RRsp3Multi: new / upload_* /
+step_*_multi / download_* / finish) for the UFF + GridFF FIRE path: upload
+molecules and systems, set or build the substrate grid, run FIRE steps,
+read back positions, forces and energies.  All numerics run in the CUDA
+library; this module only marshals arrays.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+
+GRID_F32, GRID_F16, GRID_BF16 = 0, 1, 2
+MODE_BATCHED, MODE_PLAIN = 0, 1
+ST_RUNNING, ST_CONVERGED, ST_MAXSTEPS, ST_NONFINITE = 0, 1, 2, 3
+E_TOTAL, E_BOND, E_ANGLE, E_DIH, E_INV, E_NB, E_GRID = range(7)
+
+# FireState defaults (crates/libs/molff/src/raff.rs:1053-1055), dt_max 0.05 as the
+# pentacene relaxation uses (crates/libs/surfmol/tests/relax_pentacene_uff.rs:259).
+FIRE_DEFAULT = dict(dt0=0.001, dt_max=0.05, alpha0=0.1, f_inc=1.1, f_dec=0.5, f_alpha=0.99, n_min=5,
+                    fconv=1e-3, flimit=0.0)
+
+
+class SmrError(RuntimeError):
+    pass
+
+
+def _d(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _f(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _i(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _p(a, t):
+    return None if a is None else a.ctypes.data_as(t)
+
+
+def fire_params(**kw) -> N.SmrFireParams:
+    p = dict(FIRE_DEFAULT)
+    p.update(kw)
+    return N.SmrFireParams(p["dt0"], p["dt_max"], p["alpha0"], p["f_inc"], p["f_dec"], p["f_alpha"], int(p["n_min"]),
+                           p["fconv"], p["flimit"])
+
+
+_EXPORT_SHAPES = [("neighs", 4, np.int32), ("neighBs", 4, np.int32), ("bonds", 2, np.int32),
+                  ("bparams", 2, np.float64), ("angs", 3, np.int32), ("ang_ngs", 2, np.int32),
+                  ("angp", 5, np.float64), ("dihs", 4, np.int32), ("dih_ngs", 3, np.int32),
+                  ("dihp", 3, np.float64), ("invs", 4, np.int32), ("inv_ngs", 3, np.int32),
+                  ("invp", 4, np.float64), ("req", 4, np.float64), ("type_id", 1, np.int32)]
+_COUNT_OF = {"neighs": 0, "neighBs": 0, "bonds": 1, "bparams": 1, "angs": 2, "ang_ngs": 2, "angp": 2, "dihs": 3,
+             "dih_ngs": 3, "dihp": 3, "invs": 4, "inv_ngs": 4, "invp": 4, "req": 0, "type_id": 0}
+
+
+def _export_arrays(counts):
+    out = {}
+    for name, w, dt in _EXPORT_SHAPES:
+        n = counts[_COUNT_OF[name]]
+        out[name] = np.zeros((n, w) if w > 1 else n, dtype=dt)
+    return out
+
+
+def _export_ptrs(out):
+    ptrs = []
+    for name, _, dt in _EXPORT_SHAPES:
+        ptrs.append(out[name].ctypes.data_as(N.IP if dt == np.int32 else N.DP))
+    return ptrs
+
+
+def type_name(tid: int) -> str:
+    return N.lib().smr_type_name(int(tid)).decode()
+
+
+class Topology:
+    """Host-only molecule preparation (bonds by cutoff, UFF typing, terms, parameters)."""
+
+    def __init__(self, Z, pos, charges=None, bond_cut=1.8):
+        L = N.lib()
+        Z = _i(Z)
+        pos = _d(pos)
+        q = _d(charges) if charges is not None else None
+        h = N.VP()
+        err = C.create_string_buffer(300)
+        r = L.smr_topo_build(len(Z), _p(Z, N.IP), _p(pos, N.DP), _p(q, N.DP), bond_cut, C.byref(h), err, 300)
+        if r != 0:
+            raise SmrError(f"smr_topo_build: {err.value.decode()}")
+        self.h = h
+        c = (C.c_int * 5)()
+        L.smr_topo_counts(self.h, c)
+        self.counts = list(c)
+        self.n = self.counts[0]
+
+    def __del__(self):
+        try:
+            if self.h:
+                N.lib().smr_topo_free(self.h)
+        except Exception:
+            pass
+
+    def export(self):
+        out = _export_arrays(self.counts)
+        N.lib().smr_topo_export(self.h, *_export_ptrs(out))
+        out["types"] = [type_name(t) for t in out["type_id"]]
+        return out
+
+    def rounds(self, team):
+        L = N.lib()
+        r = (C.c_int * 3)()
+        L.smr_topo_rounds(self.h, team, r, None, None, None)
+        arrs = [np.zeros((r[k] * team, 4), np.int16) for k in range(3)]
+        L.smr_topo_rounds(self.h, team, r, *[a.ctypes.data_as(N.SP) for a in arrs])
+        return list(r), arrs
+
+
+class RelaxMulti:
+    """Many molecules relaxed by FIRE in parallel over one substrate grid, on one GPU."""
+
+    def __init__(self, max_systems: int, max_atoms: int, device: int = 0):
+        self.L = N.lib()
+        cfg = N.SmrConfig(device, int(max_systems), int(max_atoms))
+        h = N.VP()
+        r = self.L.smr_create(C.byref(cfg), C.byref(h))
+        if r != 0:
+            raise SmrError(f"smr_create failed ({r}): CUDA device {device} unavailable or out of memory")
+        self.h = h
+        self.natoms_of = {}     # slot -> natoms
+        self.topo_n = []        # topology id -> natoms
+
+    # -- lifecycle
+    def finish(self):
+        if self.h:
+            self.L.smr_destroy(self.h)
+            self.h = None
+
+    close = finish
+
+    def __del__(self):
+        try:
+            self.finish()
+        except Exception:
+            pass
+
+    def _chk(self, r, what):
+        if r != 0:
+            raise SmrError(f"{what} ({r}): {self.L.smr_last_error(self.h).decode()}")
+
+    # -- parameters and grid
+    def set_nb(self, rdamp=1.0, alpha_morse=1.5, rcut=0.0):
+        p = N.SmrNbParams(rdamp, alpha_morse, rcut, 0)
+        self._chk(self.L.smr_set_nb_params(self.h, C.byref(p)), "smr_set_nb_params")
+
+    def set_grid(self, coef, p0, step, dtype=GRID_F32, scale=(1, 1, 1, 1)):
+        """coef: (nx, ny, nz, 4) float32 (F32) or uint16 (F16/BF16 bit patterns), z-fastest."""
+        coef = np.ascontiguousarray(coef)
+        nx, ny, nz, _ = coef.shape
+        sc = _f(scale)
+        self._chk(self.L.smr_set_grid(self.h, coef.ctypes.data_as(N.VP), dtype, _p(sc, N.FP), nx, ny, nz,
+                                      _p(_d(p0), N.DP), _p(_d(step), N.DP)), "smr_set_grid")
+
+    def get_grid(self):
+        dt = C.c_int()
+        sc = (C.c_float * 4)()
+        dims = (C.c_int * 3)()
+        p0 = (C.c_double * 3)()
+        st = (C.c_double * 3)()
+        self._chk(self.L.smr_get_grid(self.h, None, C.byref(dt), sc, dims, p0, st), "smr_get_grid")
+        shape = (dims[0], dims[1], dims[2], 4)
+        buf = np.zeros(shape, np.float32 if dt.value == GRID_F32 else np.uint16)
+        self._chk(self.L.smr_get_grid(self.h, buf.ctypes.data_as(N.VP), None, None, None, None, None), "smr_get_grid")
+        return dict(coef=buf, dtype=dt.value, scale=np.array(list(sc)), p0=np.array(list(p0)), step=np.array(list(st)))
+
+    def build_grid(self, ions, ion_re, Lx, Ly, nx, ny, nz, p0, step, alpha_morse=1.5, npbc=1, ewald_tol=1e-12,
+                   dtype=GRID_F32, morse_rcut=0.0):
+        ions = _d(ions)
+        re = _d(np.asarray(ion_re)[:, :2])
+        p = N.SmrGridBuildParams(alpha_morse, npbc, ewald_tol, dtype, morse_rcut)
+        self._chk(self.L.smr_build_grid(self.h, len(ions), _p(ions, N.DP), _p(re, N.DP), Lx, Ly, nx, ny, nz,
+                                        _p(_d(p0), N.DP), _p(_d(step), N.DP), C.byref(p)), "smr_build_grid")
+
+    def convert_grid(self, dtype):
+        self._chk(self.L.smr_convert_grid(self.h, dtype), "smr_convert_grid")
+
+    def set_team_size(self, max_atoms, threads):
+        self._chk(self.L.smr_set_team_size(self.h, max_atoms, threads), "smr_set_team_size")
+
+    # -- molecules
+    def add_molecule(self, Z, pos, charges=None, bond_cut=1.8) -> int:
+        Z = _i(Z)
+        pos = _d(pos)
+        q = _d(charges) if charges is not None else None
+        tid = C.c_int()
+        self._chk(self.L.smr_add_molecule(self.h, len(Z), _p(Z, N.IP), _p(pos, N.DP), _p(q, N.DP), bond_cut,
+                                          C.byref(tid)), "smr_add_molecule")
+        self.topo_n.append(len(Z))
+        return tid.value
+
+    def add_topo(self, topo: Topology) -> int:
+        tid = C.c_int()
+        self._chk(self.L.smr_add_topo(self.h, topo.h, C.byref(tid)), "smr_add_topo")
+        self.topo_n.append(topo.n)
+        return tid.value
+
+    def add_topology(self, req, neighs, bond_kl, angs=None, angp=None, dihs=None, dihp=None, invs=None, invp=None):
+        req = _d(req)
+        n = len(req)
+        keep = []
+
+        def arr(a, w, f):
+            if a is None or len(a) == 0:
+                return 0, None
+            a = f(a).reshape(-1, w)
+            keep.append(a)
+            return len(a), a.ctypes.data_as(N.IP if f is _i else N.DP)
+
+        ng = _i(neighs)
+        bkl = _d(bond_kl).reshape(n, 8)
+        na, pa = arr(angs, 3, _i)
+        _, ppa = arr(angp, 5, _d)
+        nd, pd = arr(dihs, 4, _i)
+        _, ppd = arr(dihp, 3, _d)
+        ni, pi = arr(invs, 4, _i)
+        _, ppi = arr(invp, 4, _d)
+        desc = N.SmrTopologyDesc(n, req.ctypes.data_as(N.DP), ng.ctypes.data_as(N.IP), bkl.ctypes.data_as(N.DP),
+                                 na, pa, ppa, nd, pd, ppd, ni, pi, ppi)
+        tid = C.c_int()
+        self._chk(self.L.smr_add_topology(self.h, C.byref(desc), C.byref(tid)), "smr_add_topology")
+        self.topo_n.append(n)
+        return tid.value
+
+    def topology(self, tid):
+        c = (C.c_int * 6)()
+        self._chk(self.L.smr_topology_counts(self.h, tid, c), "smr_topology_counts")
+        out = _export_arrays(list(c)[:5])
+        self._chk(self.L.smr_topology_export(self.h, tid, *_export_ptrs(out)), "smr_topology_export")
+        out["types"] = [type_name(t) for t in out["type_id"]]
+        out["rounds"] = c[5]
+        return out
+
+    # -- systems
+    def add_systems(self, topo_ids, positions) -> np.ndarray:
+        topo_ids = _i(topo_ids)
+        pos = _f(np.concatenate([np.asarray(p, dtype=np.float64).reshape(-1, 3) for p in positions]))
+        slots = np.zeros(len(topo_ids), np.int32)
+        self._chk(self.L.smr_add_systems(self.h, len(topo_ids), _p(topo_ids, N.IP), _p(pos, N.FP), _p(slots, N.IP)),
+                  "smr_add_systems")
+        for s, t in zip(slots, topo_ids):
+            self.natoms_of[int(s)] = self.topo_n[int(t)]
+        return slots
+
+    upload_state_multi = add_systems
+
+    def remove_systems(self, slots):
+        slots = _i(slots)
+        self._chk(self.L.smr_remove_systems(self.h, len(slots), _p(slots, N.IP)), "smr_remove_systems")
+        for s in slots:
+            self.natoms_of.pop(int(s), None)
+
+    def set_positions(self, slots, positions):
+        slots = _i(slots)
+        pos = _f(np.concatenate([np.asarray(p).reshape(-1, 3) for p in positions]))
+        self._chk(self.L.smr_set_positions(self.h, len(slots), _p(slots, N.IP), _p(pos, N.FP)), "smr_set_positions")
+
+    def reset_fire(self, slots):
+        slots = _i(slots)
+        self._chk(self.L.smr_reset_fire(self.h, len(slots), _p(slots, N.IP)), "smr_reset_fire")
+
+    def _split(self, slots, flat, w):
+        out, k = [], 0
+        for s in slots:
+            n = self.natoms_of[int(s)]
+            out.append(flat[k:k + n].reshape(n, w) if w > 1 else flat[k:k + n])
+            k += n
+        return out
+
+    def eval_forces(self, slots):
+        """One force evaluation: list of (n, 4) float32 arrays (fx, fy, fz, E_atom), energies (nsys, 8)."""
+        slots = _i(slots)
+        tot = sum(self.natoms_of[int(s)] for s in slots)
+        F = np.zeros((tot, 4), np.float32)
+        E = np.zeros((len(slots), 8))
+        self._chk(self.L.smr_eval_forces(self.h, len(slots), _p(slots, N.IP), _p(F, N.FP), _p(E, N.DP)),
+                  "smr_eval_forces")
+        return self._split(slots, F, 4), E
+
+    def run_fire(self, max_steps, step_budget=0, mode=MODE_BATCHED, **fire) -> int:
+        p = fire_params(**fire)
+        nf = C.c_int()
+        self._chk(self.L.smr_run_fire(self.h, int(max_steps), int(step_budget), C.byref(p), mode, C.byref(nf)),
+                  "smr_run_fire")
+        return nf.value
+
+    step_multi = run_fire
+
+    def download(self, slots, pos=True, forces=True):
+        slots = _i(slots)
+        tot = sum(self.natoms_of[int(s)] for s in slots)
+        P = np.zeros((tot, 3), np.float32) if pos else None
+        F = np.zeros((tot, 4), np.float32) if forces else None
+        E = np.zeros((len(slots), 8))
+        steps = np.zeros(len(slots), np.int32)
+        status = np.zeros(len(slots), np.int32)
+        self._chk(self.L.smr_download(self.h, len(slots), _p(slots, N.IP), _p(P, N.FP), _p(F, N.FP), _p(E, N.DP),
+                                      _p(steps, N.IP), _p(status, N.IP)), "smr_download")
+        return dict(pos=self._split(slots, P, 3) if pos else None, forces=self._split(slots, F, 4) if forces else None,
+                    energy=E[:, 0], steps=steps, status=status)
+
+    def download_pos_multi(self, slots):
+        return self.download(slots, pos=True, forces=False)["pos"]
+
+    def download_pos_replica(self, slot):
+        return self.download([slot], pos=True, forces=False)["pos"][0]
+
+    def last_timing(self):
+        ms = C.c_double()
+        n = C.c_longlong()
+        self._chk(self.L.smr_last_timing(self.h, C.byref(ms), C.byref(n)), "smr_last_timing")
+        return ms.value, n.value
+
+    def active_slots(self):
+        n = C.c_int()
+        self.L.smr_active_slots(self.h, C.byref(n), None)
+        ids = np.zeros(n.value, np.int32)
+        self.L.smr_active_slots(self.h, C.byref(n), _p(ids, N.IP))
+        return ids

@@ -1,0 +1,277 @@
+"""Seeded synthetic workloads: planar polyaromatic molecules over a rock-salt slab.
+
+The reference measures nothing on a public dataset; these generators stand in
+for its inputs with the shapes of the relaxation configurations:
+
+* ``polyaromatic_40`` -- one 40-atom planar polyaromatic: a hexacene
+  skeleton (26 ring sites at 1.40 A: 24 C + 2 pyridinic N on edge sites) with
+  14 edge substituents (12 H at 1.09 A, 2 carbonyl O at 1.22 A).
+* ``ragged_molecule`` -- parallelogram hexagonal cores of a target size with
+  H capping, C:H:N:O near 60:30:5:5 (N pyridinic on edge sites, O carbonyl).
+* ``rocksalt_slab`` -- (100) slab, a = 5.64 A, +-q ions, 4 ions per cell and
+  layer, top layer at z = 0.
+
+All geometry is float64 and fully determined by the integer seed.  Typing of
+these molecules by the reference's hybridisation rule
+(crates/libs/moltopo/src/assign_uff.rs:8-125) is clean: ring C -> C_R,
+edge N (2 neighbours) -> N_R, carbonyl O (1 neighbour) -> O_2, H -> H_.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+Z_H, Z_C, Z_N, Z_O, Z_NA, Z_CL = 1, 6, 7, 8, 11, 17
+
+B_CC = 1.40      # ring bond length (A)
+B_CH = 1.09      # C-H (A)
+B_CO = 1.22      # C=O (A)
+BOND_CUT = 1.8   # bond-by-cutoff radius used by the reference topology builder
+MIN_NONBONDED = 2.0    # geometric margin so the 1.8 A cutoff finds exactly the intended bonds
+JITTER_CLIP = 0.05     # per-component clip of the Gaussian jitter: distances move by < 0.18 A
+
+# (R_vdW, E_vdW) of the substrate ions, rows "Na" and "Cl" of the reference's
+# data/AtomTypes.dat; Morse uses (R, sqrt(E)).
+ION_RE = {Z_NA: (1.4915, 0.00130092313), Z_CL: (1.9735, 0.00984365166)}
+
+_HEX_DIRS = [(1, 0), (1, -1), (0, -1), (-1, 0), (-1, 1), (0, 1)]
+
+
+@dataclass
+class Molecule:
+    Z: np.ndarray          # (n,) int32 atomic numbers
+    pos: np.ndarray        # (n,3) float64, molecule frame (centroid at origin, z=0)
+    bonds: list = field(default_factory=list)   # construction bonds (i<j)
+
+    @property
+    def n(self) -> int:
+        return int(self.Z.shape[0])
+
+
+def _hex_vertices(hexes):
+    """Vertices (rounded keys) of a set of axial hexagon centres, and the hex count per vertex."""
+    verts = {}
+    for (q, r) in hexes:
+        cx = math.sqrt(3.0) * B_CC * (q + 0.5 * r)
+        cy = 1.5 * B_CC * r
+        for k in range(6):
+            th = math.radians(30.0 + 60.0 * k)
+            x, y = cx + B_CC * math.cos(th), cy + B_CC * math.sin(th)
+            key = (round(x * 1000), round(y * 1000))
+            if key not in verts:
+                verts[key] = [x, y, 0]
+            verts[key][2] += 1
+    return verts
+
+
+def _ring_graph(hexes):
+    v = _hex_vertices(hexes)
+    keys = sorted(v.keys())
+    xy = np.array([[v[k][0], v[k][1]] for k in keys], dtype=np.float64)
+    n = len(keys)
+    d = np.linalg.norm(xy[:, None, :] - xy[None, :, :], axis=-1)
+    adj = (d < B_CC * 1.05) & (d > 0.1)
+    return xy, adj
+
+
+def _assemble(rng, xy, adj, n_N, n_O):
+    """Ring sites + substituents.  Returns Molecule or None if the geometry is crowded."""
+    nring = xy.shape[0]
+    deg = adj.sum(1)
+    edge = [i for i in range(nring) if deg[i] == 2]
+    if len(edge) < n_N + n_O + 1:
+        return None
+    perm = list(rng.permutation(edge))
+    n_sites = []
+    for i in perm:
+        if len(n_sites) == n_N:
+            break
+        if not any(adj[i, j] for j in n_sites):
+            n_sites.append(int(i))
+    if len(n_sites) < n_N:
+        return None
+    rest = [int(i) for i in perm if i not in n_sites]
+    o_sites = rest[:n_O]
+    Z = [Z_N if i in n_sites else Z_C for i in range(nring)]
+    P = [[xy[i, 0], xy[i, 1], 0.0] for i in range(nring)]
+    bonds = [(i, j) for i in range(nring) for j in range(i + 1, nring) if adj[i, j]]
+    for i in edge:
+        if i in n_sites:
+            continue
+        nb = np.nonzero(adj[i])[0]
+        d = (xy[i] - xy[nb[0]]) + (xy[i] - xy[nb[1]])
+        d /= np.linalg.norm(d)
+        if i in o_sites:
+            z, b = Z_O, B_CO
+        else:
+            z, b = Z_H, B_CH
+        bonds.append((i, len(Z)))
+        Z.append(z)
+        P.append([xy[i, 0] + b * d[0], xy[i, 1] + b * d[1], 0.0])
+    P = np.array(P, dtype=np.float64)
+    n = len(Z)
+    bonded = np.zeros((n, n), dtype=bool)
+    for i, j in bonds:
+        bonded[i, j] = bonded[j, i] = True
+    dd = np.linalg.norm(P[:, None, :] - P[None, :, :], axis=-1)
+    np.fill_diagonal(dd, 1e9)
+    if np.any(dd[~bonded] < MIN_NONBONDED):
+        return None
+    P -= P.mean(0)
+    return Molecule(np.array(Z, dtype=np.int32), P, bonds)
+
+
+def parallelogram_core(A: int, B: int):
+    """Ring graph of an A x B parallelogram of hexagons (acenes for B=1).
+
+    Parallelogram benzenoids have zigzag edges only: no bay or fjord regions,
+    so with C-H = 1.09 A every non-bonded distance stays above 2.16 A and the
+    1.8 A bond cutoff recovers exactly the construction bonds."""
+    return _ring_graph([(q, r) for q in range(A) for r in range(B)])
+
+
+def polyaromatic_40(rng) -> Molecule:
+    """Hexacene skeleton (26 ring sites: 24 C + 2 pyridinic N), 12 H + 2 carbonyl O = 40 atoms."""
+    xy, adj = parallelogram_core(6, 1)
+    for _ in range(1000):
+        m = _assemble(rng, xy, adj, n_N=2, n_O=2)
+        if m is not None and m.n == 40:
+            return m
+    raise RuntimeError("could not generate the 40-atom polyaromatic")
+
+
+def ragged_molecule(rng, target: int) -> Molecule:
+    """Parallelogram core (1 or 2 hexagon rows) with H capping near ``target`` atoms.
+
+    One row gives C:H ~ 2:1, two rows ~ 3:1; N (pyridinic, edge sites) and
+    carbonyl O each make ~5 % of the atoms."""
+    target = max(int(target), 12)
+    for _ in range(1000):
+        B = 1 + int(rng.integers(2))
+        A = max(1, int(round((target - 6) / 6.0)) if B == 1 else int(round((target - 10) / 8.0)))
+        xy, adj = parallelogram_core(A, B)
+        tot = xy.shape[0] + int((adj.sum(1) == 2).sum())
+        m = _assemble(rng, xy, adj, n_N=int(round(0.05 * tot)), n_O=int(round(0.05 * tot)))
+        if m is not None:
+            return m
+    raise RuntimeError("could not generate a ragged molecule")
+
+
+def charges(rng, n: int, sigma: float = 0.15) -> np.ndarray:
+    q = rng.normal(0.0, sigma, n)
+    return q - q.mean()
+
+
+def place(rng, mol: Molecule, xy0, height: float, jitter: float = 0.05, z_top: float = 0.0):
+    """Rotate about z (uniform angle), translate to (x0, y0, z_top+height), add clipped Gaussian jitter."""
+    th = rng.uniform(0.0, 2.0 * math.pi)
+    c, s = math.cos(th), math.sin(th)
+    R = np.array([[c, -s, 0.0], [s, c, 0.0], [0.0, 0.0, 1.0]])
+    p = mol.pos @ R.T
+    p += np.array([xy0[0], xy0[1], z_top + height])
+    if jitter > 0:
+        p += np.clip(rng.normal(0.0, jitter, p.shape), -JITTER_CLIP, JITTER_CLIP)
+    return p
+
+
+@dataclass
+class Slab:
+    ions: np.ndarray       # (m,4) x, y, z, q
+    Z: np.ndarray          # (m,) int32
+    Lx: float
+    Ly: float
+    z_top: float
+
+    def req(self) -> np.ndarray:
+        """(m,4) Morse parameters per ion: (R, sqrt(E), q, 0)."""
+        out = np.zeros((self.Z.shape[0], 4))
+        for k, z in enumerate(self.Z):
+            R, E = ION_RE[int(z)]
+            out[k] = (R, math.sqrt(E), self.ions[k, 3], 0.0)
+        return out
+
+
+def rocksalt_slab(ncell: int, nlayers: int, a: float = 5.64, q: float = 0.9, z_top: float = 0.0) -> Slab:
+    ions, Zs = [], []
+    for L in range(nlayers):
+        z = z_top - L * 0.5 * a
+        for ix in range(ncell):
+            for iy in range(ncell):
+                for (fx, fy, cat) in ((0.0, 0.0, True), (0.5, 0.5, True), (0.5, 0.0, False), (0.0, 0.5, False)):
+                    na = cat if (L % 2 == 0) else (not cat)
+                    ions.append([(ix + fx) * a, (iy + fy) * a, z, q if na else -q])
+                    Zs.append(Z_NA if na else Z_CL)
+    return Slab(np.array(ions, dtype=np.float64), np.array(Zs, dtype=np.int32), ncell * a, ncell * a, z_top)
+
+
+@dataclass
+class GridSpec:
+    nx: int
+    ny: int
+    nz: int
+    p0: tuple
+    step: tuple
+
+
+def grid_for(slab: Slab, nz: int, dz: float = 0.1, z_gap: float = 1.0, h: float = 0.1) -> GridSpec:
+    """Periodic x,y grid covering exactly one slab cell at ~h spacing; z from z_top+z_gap upward."""
+    nx = int(round(slab.Lx / h))
+    ny = int(round(slab.Ly / h))
+    return GridSpec(nx, ny, nz, (0.0, 0.0, slab.z_top + z_gap), (slab.Lx / nx, slab.Ly / ny, dz))
+
+
+@dataclass
+class Workload:
+    Z: list            # per system (n,) int32
+    pos: list          # per system (n,3) float64
+    q: list            # per system (n,) float64
+    topo_of: np.ndarray  # per system: index of its molecule template (replicas share one)
+    slab: Slab
+    grid: GridSpec
+    seed: int
+
+
+def config0(seed: int = 0) -> Workload:
+    """One 40-atom polyaromatic 3.0 A above a 2-layer 4x4-cell slab; grid 0.1 A, 12 A of z."""
+    rng = np.random.default_rng(seed)
+    mol = polyaromatic_40(rng)
+    q = charges(rng, mol.n)
+    slab = rocksalt_slab(4, 2)
+    g = grid_for(slab, nz=121)
+    p = place(rng, mol, (0.5 * slab.Lx, 0.5 * slab.Ly), 3.0)
+    return Workload([mol.Z], [p], [q], np.zeros(1, np.int32), slab, g, seed)
+
+
+def config1(seed: int = 0, nsys: int = 4096) -> Workload:
+    """``nsys`` replicas of the config-0 molecule: random lateral offset, z rotation, height U[2.5,4]."""
+    rng = np.random.default_rng(seed)
+    mol = polyaromatic_40(rng)
+    q = charges(rng, mol.n)
+    slab = rocksalt_slab(4, 2)
+    g = grid_for(slab, nz=121)
+    Zs, Ps, Qs = [], [], []
+    for _ in range(nsys):
+        xy0 = (rng.uniform(0, slab.Lx), rng.uniform(0, slab.Ly))
+        Ps.append(place(rng, mol, xy0, rng.uniform(2.5, 4.0)))
+        Zs.append(mol.Z)
+        Qs.append(q)
+    return Workload(Zs, Ps, Qs, np.zeros(nsys, np.int32), slab, g, seed)
+
+
+def ragged(seed: int, nsys: int, nmin: int = 20, nmax: int = 400, ncell: int = 8, nlayers: int = 3,
+           nz: int = 161) -> Workload:
+    """Ragged batch: atom counts log-uniform in [nmin, nmax], each molecule distinct."""
+    rng = np.random.default_rng(seed)
+    slab = rocksalt_slab(ncell, nlayers)
+    g = grid_for(slab, nz=nz)
+    Zs, Ps, Qs = [], [], []
+    for _ in range(nsys):
+        target = int(round(math.exp(rng.uniform(math.log(nmin), math.log(nmax)))))
+        mol = ragged_molecule(rng, target)
+        Qs.append(charges(rng, mol.n))
+        xy0 = (rng.uniform(0, slab.Lx), rng.uniform(0, slab.Ly))
+        Ps.append(place(rng, mol, xy0, rng.uniform(2.5, 4.0)))
+        Zs.append(mol.Z)
+    return Workload(Zs, Ps, Qs, np.arange(nsys, dtype=np.int32), slab, g, seed)

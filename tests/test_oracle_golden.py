@@ -1,0 +1,112 @@
+"""The FP64 oracle against the reference's own known answers (CPU)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def load(name):
+    return json.load(open(os.path.join(GOLD, name)))
+
+
+def test_h2_bond(oracle):
+    """crates/libs/oclff/tests/test_uff_cl.rs:8-56: k=100, l0=0.9, r=1 -> fx=+-20, E=1 per atom."""
+    g = load("h2.json")
+    S = oracle.System.from_bonds(2, [[0, 1]], [[g["k"], g["l0"]]])
+    F, Ea, Ec = S.eval(np.array(g["pos"], float), rcut=1e-6)
+    assert abs(F[0, 0] - g["fx"][0]) < g["tol"] and abs(F[1, 0] - g["fx"][1]) < g["tol"]
+    assert np.all(np.abs(F[:, 1:]) < g["tol"])
+    assert abs(Ea[0] - g["E_atom"][0]) < g["tol"] and abs(Ea[1] - g["E_atom"][1]) < g["tol"]
+
+
+def _pentacene(oracle):
+    d = load("pentacene.json")
+    Z = np.array(d["Z"])
+    P = np.array(d["pos"])
+    return d, P, oracle.System.from_molecule(Z, P)
+
+
+def test_pentacene_topology_counts(oracle):
+    d, P, S = _pentacene(oracle)
+    c = d["counts"]
+    assert (S.nbonds, S.nang, S.ndih, S.ninv) == (c["bonds"], c["angles"], c["dihedrals"], c["inversions"])
+    assert set(S.export()["types"]) == {"C_R", "H_"}
+
+
+def test_pentacene_planar_energies(oracle):
+    """Planar pentacene, bonded terms only: E_bond (summed over atoms) 3.834, E_angle 0.010, E_dih 0, E_inv 0."""
+    d, P, S = _pentacene(oracle)
+    F, Ea, Ec = S.eval(P, rcut=1e-6)
+    ref = d["planar"]
+    assert abs(2 * Ec[oracle.E_BOND] - ref["E_bond"]) < 5e-4
+    assert abs(Ec[oracle.E_ANG] - ref["E_angle"]) < 5e-4
+    assert abs(Ec[oracle.E_DIH] - ref["E_dih"]) < 5e-4
+    assert abs(Ec[oracle.E_INV] - ref["E_inv"]) < 5e-4
+
+
+def test_pentacene_out_of_plane(oracle):
+    """Atom 0 lifted 0.5 A.  E_bond, E_angle, E_inv match the documented values directly.
+    The documented E_dih (2.634) and Fz (-11.72) are reproduced with the dihedral
+    prefactor doubled: the code (crates/libs/molff/src/uff.rs:838-843) divides V by
+    0.5*(nb2-1)*(nb3-1), the run that produced the numbers used twice that V.  The
+    oracle follows the code; this test pins the dihedral form through the doubled case."""
+    d, P, S = _pentacene(oracle)
+    ref = d["displaced"]
+    P2 = P.copy()
+    P2[ref["atom"], 2] = ref["z"]
+    F, Ea, Ec = S.eval(P2, rcut=1e-6)
+    assert abs(2 * Ec[oracle.E_BOND] - ref["E_bond"]) < 5e-4
+    assert abs(Ec[oracle.E_ANG] - ref["E_angle"]) < 5e-4
+    assert abs(Ec[oracle.E_INV] - ref["E_inv"]) < 5e-4
+    dihp = S.export()["dihp"]
+    S.set_params(dihp=dihp * np.array([2.0, 1.0, 1.0]))
+    F2, _, Ec2 = S.eval(P2, rcut=1e-6)
+    assert abs(Ec2[oracle.E_DIH] - ref["E_dih"]) < 5e-4
+    assert abs(F2[ref["atom"], 2] - ref["Fz"]) < 5e-3
+    assert abs(Ec2[oracle.E_DIH] - 2 * Ec[oracle.E_DIH]) < 1e-12
+
+
+def test_pentacene_relaxes_to_planar(oracle):
+    """relax_pentacene_uff.rs:392-397 asserts: pyramidalised pentacene relaxes (FIRE) back to planar."""
+    d, P, S = _pentacene(oracle)
+    rng = np.random.default_rng(0)
+    P2 = P + np.c_[np.zeros((len(P), 2)), rng.normal(0, 0.05, len(P))]
+    r = S.relax(P2, max_steps=3000, nb=dict(rcut=1e-6), fconv=1e-3)
+    assert r["conv"] and r["fmax"] < 1e-3
+    zc = r["pos"][:, 2] - r["pos"][:, 2].mean()
+    assert np.sqrt(np.mean(zc ** 2)) < 0.05
+
+
+def test_parameter_rows_match_reference_tables(oracle):
+    """The oracle's element/type rows equal the parsed reference .dat rows (uff_rows.json)."""
+    rows = load("uff_rows.json")
+    # the oracle exposes REQ = (RvdW, sqrt(EvdW), Qbase, Hb) of typed atoms
+    mol = {"C_R": ([6, 6, 6, 6, 6, 6, 1, 1, 1, 1, 1, 1], None)}
+    ang = np.radians(np.arange(6) * 60.0)
+    ring = np.c_[1.4 * np.cos(ang), 1.4 * np.sin(ang), np.zeros(6)]
+    hs = np.c_[2.49 * np.cos(ang), 2.49 * np.sin(ang), np.zeros(6)]
+    S = oracle.System.from_molecule(mol["C_R"][0], np.r_[ring, hs])
+    e = S.export()
+    for t, req in zip(e["types"], e["req"]):
+        r = rows["atom_types"][t]
+        assert req[0] == r["r_vdw"] and abs(req[1] - np.sqrt(r["e_vdw"])) < 1e-15 and req[3] == r["h_b"]
+
+
+def test_bspline_fit_reproduces_nodes(oracle):
+    rng = np.random.default_rng(1)
+    v = rng.normal(size=(7, 9, 11))
+    c = oracle.bspline_fit(v)
+    assert np.abs(oracle.bspline_conv(c) - v).max() < 1e-12
+
+
+def test_ewald_matches_direct_image_sum(oracle):
+    """Ewald-2D (Surface.cl:834-906) vs the direct circular image sum (Surface.cl:911-954)."""
+    from surfmol_b200 import synth
+    slab = synth.rocksalt_slab(1, 2)
+    pts = np.array([[0.3, 0.7, 1.5], [2.0, 1.1, 2.5], [4.1, 3.3, 4.0]])
+    pe = oracle.ewald_points(pts, slab.ions, slab.Lx, slab.Ly, gcut=40.0)
+    pb = oracle.brute_coulomb_points(pts, slab.ions, slab.Lx, slab.Ly, nrep=60)
+    assert np.allclose(pe, pb, atol=2e-3)
