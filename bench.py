@@ -1,0 +1,330 @@
+#!/usr/bin/env python
+"""Benchmark: relaxed systems per second on one B200 (per rank), JSON line on stdout.
+
+Workload (default): 4096 replicas of the 40-atom polyaromatic (random lateral
+offset, z rotation, height U[2.5, 4] A, 0.05 A jitter) over a 2-layer 4x4-cell
+NaCl(100) slab, FP32 B-spline grid 226x226x121 (0.1 A) built on the device;
+FIRE (dt0 0.001, dt_max 0.05) to max|F| < 1e-3 eV/A or 2000 steps.
+
+One bench step = relaxing the whole batch from its start positions.  The device
+time of each step is taken with CUDA events on the library's stream around the
+relaxation launch; L2 is flushed (256 MB write) before every step.  Under
+torchrun each rank relaxes its own batch (weak scaling, no collective on the
+data path); the reported time is the max over ranks.
+
+--impl reference times the FP64 CPU restatement of the same path (oracle/), the
+reference's own algorithm, on all host cores, on a bounded sample per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "relaxed systems/sec at ≤1e-4 eV/Å force error; p50/p99 relax latency; HBM GB/s"
+FIRE = dict(dt0=0.001, dt_max=0.05, fconv=1e-3)
+MAX_STEPS = 2000
+SEED = 20261203
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if p[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return ws, rank, local
+
+
+def barrier_max(ws, value):
+    """Barrier + max over ranks of a float (device time)."""
+    if ws == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def make_workload(seed, nsys):
+    from surfmol_b200 import synth
+    return synth.config1(seed, nsys)
+
+
+def workload_desc(w, nsys):
+    g = w.grid
+    return (f"config1: {nsys} replicas of a 40-atom polyaromatic (24 C, 12 H, 2 N, 2 O) over NaCl(100) "
+            f"2 layers 4x4 cells, fp32 B-spline grid {g.nx}x{g.ny}x{g.nz} at 0.1 A; FIRE to max|F|<1e-3 or {MAX_STEPS} steps")
+
+
+# ---------------------------------------------------------------------------------------- reference arm
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    w = make_workload(SEED, args.nsys)
+    slab, g = w.slab, w.grid
+    t0 = time.perf_counter()
+    coef = O.build_grid_fast(slab.ions, slab.req(), slab.Lx, slab.Ly, g.nx, g.ny, g.nz, g.p0, g.step)
+    tgrid = time.perf_counter() - t0
+    grid = O.Grid(coef.astype(np.float32), g.p0, g.step)
+    sys0 = O.System.from_molecule(w.Z[0], w.pos[0], w.q[0])
+    threads = os.cpu_count() or 1
+    sample = max(threads, args.ref_sample)
+
+    def one(k0):
+        idx = [(k0 + i) % args.nsys for i in range(sample)]
+        t = time.perf_counter()
+        r = O.relax_batch([sys0] * sample, [w.pos[i] for i in idx], grid, max_steps=MAX_STEPS, nthreads=threads,
+                          **FIRE)
+        return time.perf_counter() - t, r
+
+    for k in range(args.warmup):
+        one(k * sample)
+    tt, conv, steps = 0.0, 0, []
+    for k in range(args.steps):
+        dt, r = one((args.warmup + k) * sample)
+        tt += dt
+        conv += int(r["conv"].sum())
+        steps += list(r["steps"])
+    v = sample * args.steps / tt
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "systems/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * tt / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": workload_desc(w, args.nsys), "sample_per_step": sample,
+                       "grid_build_s": round(tgrid, 2), "converged_fraction": conv / (sample * args.steps),
+                       "fire_steps_p50": float(np.percentile(steps, 50)), "fire_steps_p99": float(np.percentile(steps, 99))},
+            "cpu_baseline": {"value": v, "unit": "systems/s", "cores": threads, "kind": "port",
+                             "sample": f"{sample} systems of the workload per step, FP64 oracle (oracle/oracle.cpp), "
+                                       f"OpenMP one system per thread"},
+            "e2e": {"value": v, "unit": "systems/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------------------- our arm
+def cpu_baseline(w, coef, p0, step, budget_s=15.0):
+    from oracle import oracle as O
+    grid = O.Grid(coef, p0, step)
+    sys0 = O.System.from_molecule(w.Z[0], w.pos[0], w.q[0])
+    threads = os.cpu_count() or 1
+    chunk = max(threads, 16)
+    done, t_total, k = 0, 0.0, 0
+    while t_total < budget_s and done < len(w.pos):
+        idx = [(k + i) % len(w.pos) for i in range(chunk)]
+        t = time.perf_counter()
+        O.relax_batch([sys0] * chunk, [w.pos[i] for i in idx], grid, max_steps=MAX_STEPS, nthreads=threads, **FIRE)
+        t_total += time.perf_counter() - t
+        done += chunk
+        k += chunk
+    return {"value": done / t_total, "unit": "systems/s", "cores": threads, "kind": "port",
+            "sample": f"{done} systems of the same workload (relaxed to convergence or {MAX_STEPS} steps), FP64 oracle, "
+                      f"OpenMP one system per thread, {t_total:.1f} s"}
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+    from surfmol_b200 import RelaxMulti
+
+    dev = local
+    torch.cuda.set_device(dev)
+    w = make_workload(SEED + 7919 * rank, args.nsys)
+    slab, g = w.slab, w.grid
+    natoms = sum(len(p) for p in w.pos)
+    R = RelaxMulti(max_systems=args.nsys, max_atoms=natoms, device=dev)
+    R.set_nb(rdamp=1.0, alpha_morse=1.5)
+    t0 = time.perf_counter()
+    R.build_grid(slab.ions, slab.req()[:, :2], slab.Lx, slab.Ly, g.nx, g.ny, g.nz, g.p0, g.step, alpha_morse=1.5, npbc=1)
+    torch.cuda.synchronize()
+    tgrid = time.perf_counter() - t0
+    tid = R.add_molecule(w.Z[0], w.pos[0], w.q[0])
+    slots = R.add_systems([tid] * args.nsys, w.pos)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MB > 126 MB L2
+
+    def reset():
+        R.set_positions(slots, w.pos)
+        R.reset_fire(slots)
+
+    def step():
+        reset()
+        flush.zero_()
+        torch.cuda.synchronize()
+        R.run_fire(args.max_steps, step_budget=args.max_steps, **FIRE)
+        ms, launches = R.last_timing()
+        return ms, launches
+
+    for _ in range(args.warmup):
+        step()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    dev_ms, launches, atom_steps, steps_all, conv = 0.0, 0, 0, [], 0
+    with ClockSampler(dev) as clk:
+        for _ in range(args.steps):
+            ms, nl = step()
+            dev_ms += ms
+            launches += nl
+            out = R.download(slots, pos=False, forces=False)
+            atom_steps += int(out["steps"].sum()) * 40
+            steps_all += list(out["steps"])
+            conv += int((out["status"] == 1).sum())
+        torch.cuda.synchronize()
+    dev_ms = barrier_max(ws, dev_ms)
+    clocks = clk.summary()
+    ms_step = dev_ms / args.steps
+    value = ws * args.nsys / (ms_step * 1e-3)
+
+    if args.profile:
+        R.finish()
+        if rank == 0:
+            print(json.dumps({"profile_run": True, "ms_per_step": ms_step, "atom_steps": atom_steps, "launches": launches}))
+        return 0
+    # end to end through the public API with host buffers: H2D positions, relax, D2H positions + results
+    e2e_k = max(1, min(args.steps, 3))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_k):
+        R.set_positions(slots, w.pos)
+        R.reset_fire(slots)
+        R.run_fire(MAX_STEPS, step_budget=MAX_STEPS, **FIRE)
+        res = R.download(slots, pos=True, forces=False)
+    torch.cuda.synchronize()
+    t_e2e = barrier_max(ws, time.perf_counter() - t0)
+    slot_bytes = 64 * args.nsys
+    e2e = {"value": ws * args.nsys * e2e_k / t_e2e, "unit": "systems/s",
+           "h2d_bytes_per_step": 16 * natoms + slot_bytes + 12 * args.nsys,
+           "d2h_bytes_per_step": 16 * natoms + 2 * slot_bytes}
+
+    hbm, peak_kind = peaks()
+    algo_bytes = 1024.0 * atom_steps / args.steps          # 64 fp32 float4 voxels per atom-step
+    achieved = algo_bytes / (ms_step * 1e-3) / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "relax_config1_traffic.json")
+    if os.path.exists(prof):
+        pj = json.load(open(prof))
+        traffic = pj.get("dram_bytes_per_launch")
+    line = {"metric": METRIC, "value": value, "unit": "systems/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": workload_desc(w, args.nsys), "nsys_per_gpu": args.nsys, "atoms_per_system": 40,
+                       "parallelism": f"systems sharded over {ws} GPU(s), no collective",
+                       "l2": "flushed (256 MB write) before every timed step", "grid_build_s": round(tgrid, 3),
+                       "converged_fraction": conv / (args.nsys * args.steps),
+                       "fire_steps_p50": float(np.percentile(steps_all, 50)),
+                       "fire_steps_p99": float(np.percentile(steps_all, 99)),
+                       "mode": "batched persistent kernel (one launch per team class)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                         "traffic": traffic, "peak_source": peak_kind,
+                         "algorithmic_bytes": "1024 B per atom-step (64 float4 grid voxels), state resident in shared memory"},
+            "e2e": e2e, "gpu_launches": launches, "clocks": clocks}
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        gd = R.get_grid()
+        line["cpu_baseline"] = cpu_baseline(w, gd["coef"], gd["p0"], gd["step"], budget_s=args.cpu_budget)
+    R.finish()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nsys", type=int, default=4096)
+    ap.add_argument("--ref-sample", type=int, default=64)
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--max-steps", type=int, default=MAX_STEPS, help="FIRE step cap per system (profiling runs)")
+    ap.add_argument("--profile", action="store_true", help="timed steps only: no e2e leg, no CPU baseline")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        ws = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        return run_reference(args, ws, rank)
+    ws, rank, local = dist_init()
+    return run_ours(args, ws, rank, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

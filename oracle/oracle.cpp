@@ -948,4 +948,81 @@ void orc_substrate_direct(int np, const double* pts, const double* req_atom /*np
     }
 }
 
+// Same grid as orc_build_grid for a slab entirely below the grid, with the Ewald-2D
+// reciprocal sum evaluated plane by plane as a separable partial DFT (structure factors
+// S_G = sum_i q_i exp(-iG.rho_i) exp(-|G|(z0 - z_i)), pruned below gtol of the largest
+// amplitude).  Same formula as ewald_point, evaluated faster; used to build full-size
+// grids for the CPU baseline.
+int orc_build_grid_fast(int nions, const double* ions, const double* re, double Lx, double Ly,
+                        int nx, int ny, int nz, const double* p0, const double* step, double alpha, int npbc, double gtol,
+                        double* coef) {
+    const size_t N = (size_t)nx * ny * nz;
+    double ztop = -1e300, qsum = 0, qz = 0;
+    for (int i = 0; i < nions; i++) { ztop = std::max(ztop, ions[4 * i + 2]); qsum += ions[4 * i + 3]; qz += ions[4 * i + 3] * ions[4 * i + 2]; }
+    const double dmin = p0[2] - ztop;
+    if (!(dmin > 0)) return -1;
+    std::vector<double> ch(3 * N);
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 1)
+#endif
+    for (int ix = 0; ix < nx; ix++)
+        for (int iy = 0; iy < ny; iy++)
+            for (int iz = 0; iz < nz; iz++) {
+                V3 p{p0[0] + ix * step[0], p0[1] + iy * step[1], p0[2] + iz * step[2]};
+                size_t i = iz + (size_t)nz * (iy + (size_t)ny * ix);
+                double P_, L_;
+                morse_point(p, nions, ions, re, Lx, 0.0, 0.0, Ly, npbc, npbc, alpha, P_, L_);
+                ch[i] = P_; ch[N + i] = L_;
+            }
+    const double g1 = 2 * M_PI / Lx, g2 = 2 * M_PI / Ly, A = Lx * Ly;
+    const double gmax = -std::log(gtol) / dmin;
+    const int H = (int)std::floor(gmax / g1), K = (int)std::floor(gmax / g2);
+    struct GT { int h, k; double G, ar, ai; };
+    std::vector<GT> gs;
+    double amax = 0;
+    for (int h = -H; h <= H; h++)
+        for (int k = -K; k <= K; k++) {
+            if (!h && !k) continue;
+            double Gx = h * g1, Gy = k * g2, G = std::sqrt(Gx * Gx + Gy * Gy);
+            if (G > gmax) continue;
+            double sr = 0, si = 0;
+            for (int i = 0; i < nions; i++) {
+                double ph = -(Gx * ions[4 * i] + Gy * ions[4 * i + 1]);
+                double w = ions[4 * i + 3] * std::exp(-G * (p0[2] - ions[4 * i + 2]));
+                sr += w * std::cos(ph); si += w * std::sin(ph);
+            }
+            double pref = 2 * M_PI / (A * G);
+            gs.push_back({h, k, G, sr * pref, si * pref});
+            amax = std::max(amax, (std::fabs(sr) + std::fabs(si)) * pref);
+        }
+    std::vector<GT> act;
+    for (auto& g : gs) if ((std::fabs(g.ar) + std::fabs(g.ai)) >= gtol * amax) act.push_back(g);
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 1)
+#endif
+    for (int iz = 0; iz < nz; iz++) {
+        const double z = p0[2] + iz * step[2], dz = iz * step[2];
+        const double phi0 = -(2 * M_PI / A) * (qsum * z - qz);
+        std::vector<double> cx, sx, cy, sy;
+        for (int ix = 0; ix < nx; ix++)
+            for (int iy = 0; iy < ny; iy++) {
+                double x = p0[0] + ix * step[0], y = p0[1] + iy * step[1], acc = 0;
+                for (auto& g : act) {
+                    double d = std::exp(-g.G * dz);
+                    if ((std::fabs(g.ar) + std::fabs(g.ai)) * d < gtol * amax) continue;
+                    double ph = g.h * g1 * x + g.k * g2 * y;
+                    acc += d * (g.ar * std::cos(ph) - g.ai * std::sin(ph));
+                }
+                ch[2 * N + iz + (size_t)nz * (iy + (size_t)ny * ix)] = COULOMB_K * (phi0 + acc);
+            }
+    }
+    std::vector<double> cf(N);
+    for (int c = 0; c < 3; c++) {
+        orc_bspline_fit(nx, ny, nz, ch.data() + c * N, cf.data());
+        for (size_t i = 0; i < N; i++) coef[4 * i + c] = cf[i];
+    }
+    for (size_t i = 0; i < N; i++) coef[4 * i + 3] = 0.0;
+    return 0;
+}
+
 }  // extern "C"

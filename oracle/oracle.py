@@ -60,6 +60,9 @@ def lib():
         L.orc_build_grid.restype = C.c_int
         L.orc_build_grid.argtypes = [C.c_int, DP, DP, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, DP, DP,
                                      C.c_double, C.c_int, C.c_double, DP, DP]
+        L.orc_build_grid_fast.restype = C.c_int
+        L.orc_build_grid_fast.argtypes = [C.c_int, DP, DP, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, DP, DP,
+                                          C.c_double, C.c_int, C.c_double, DP]
         L.orc_substrate_direct.argtypes = [C.c_int, DP, DP, C.c_int, DP, DP, C.c_double, C.c_double, C.c_int,
                                            C.c_double, C.c_double, C.c_double, DP]
         _lib = L
@@ -282,3 +285,13 @@ def substrate_direct(pts, req_atom, ions, ion_req, Lx, Ly, npbc=1, alpha=1.5, gc
     lib().orc_substrate_direct(len(pts), _dp(pts), _dp(ra), len(ions), _dp(_d(ions)), _dp(_d(ion_req)), Lx, Ly, npbc,
                                alpha, gcut, h, _dp(out))
     return out
+
+
+def build_grid_fast(ions, ion_req, Lx, Ly, nx, ny, nz, p0, step, alpha=1.5, npbc=1, gtol=1e-12):
+    """orc_build_grid for a slab below the grid, with the separable Ewald evaluation (full-size grids)."""
+    coef = np.zeros((nx, ny, nz, 4))
+    r = lib().orc_build_grid_fast(len(ions), _dp(_d(ions)), _dp(_d(ion_req)), Lx, Ly, nx, ny, nz, _dp(_d(p0)),
+                                  _dp(_d(step)), alpha, npbc, gtol, _dp(coef))
+    if r != 0:
+        raise ValueError("grid must lie above the slab")
+    return coef

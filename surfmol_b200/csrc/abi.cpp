@@ -224,8 +224,12 @@ int download_slots(smr_handle* h) {
 }
 
 int upload_slots(smr_handle* h, const std::vector<int>& ids) {
+    if (ids.size() > 32) {   // many slots: one copy of the whole table
+        CU(h, cudaMemcpyAsync(h->slots, h->hs.data(), h->hs.size() * sizeof(SlotState), cudaMemcpyHostToDevice, h->stream));
+        return wait_stream(h, 600.0);   // hs is pageable host memory: finish before it can change
+    }
     for (int s : ids) CU(h, cudaMemcpyAsync(h->slots + s, &h->hs[s], sizeof(SlotState), cudaMemcpyHostToDevice, h->stream));
-    return 0;
+    return wait_stream(h, 600.0);
 }
 
 KernelArgs base_args(smr_handle* h) {
@@ -544,8 +548,6 @@ int smr_add_systems(smr_handle* h, int nsys, const int* topo_ids, const float* p
     std::copy(src.begin(), src.end(), desc.begin()); std::copy(len.begin(), len.end(), desc.begin() + nsys); std::copy(dst.begin(), dst.end(), desc.begin() + 2 * nsys);
     CU(h, cudaMemcpyAsync(h->xfer, desc.data(), desc.size() * 4, cudaMemcpyHostToDevice, s));
     if (launch_copy_segments(h->xfer, h->xfer + nsys, h->xfer + 2 * nsys, nsys, h->stage, h->pos, s)) return fail(h, SMR_ERR_CUDA, "scatter launch failed");
-    // zero velocities of the new ranges
-    for (int i = 0; i < nsys; i++) CU(h, cudaMemsetAsync(h->vel + dst[i], 0, (size_t)len[i] * 16, s));
     int r = upload_slots(h, ids);
     if (r) return r;
     r = wait_stream(h, 600.0);
@@ -603,12 +605,9 @@ int smr_reset_fire(smr_handle* h, int nsys, const int* slot_ids) {
         if (!valid_slot(h, s)) return fail(h, SMR_ERR_ARG, "slot %d not active", s);
         SlotState& st = h->hs[s];
         st.status = 0; st.steps = 0; st.npos = 0; st.dt = -1.0; st.alpha = 0; st.energy = 0; st.fmax = 0;
-        CU(h, cudaMemsetAsync(h->vel + st.atom_off, 0, (size_t)st.natoms * 16, h->stream));
         ids.push_back(s);
     }
-    int r = upload_slots(h, ids);
-    if (r) return r;
-    return wait_stream(h, 600.0);
+    return upload_slots(h, ids);
 }
 
 int smr_eval_forces(smr_handle* h, int nsys, const int* slot_ids, float* forces, double* energy) {
@@ -659,15 +658,12 @@ int smr_run_fire(smr_handle* h, int max_steps, int step_budget, const smr_fire_p
     if (!h || !p || max_steps < 0) return SMR_ERR_ARG;
     if (mode != SMR_MODE_BATCHED && mode != SMR_MODE_PLAIN) return fail(h, SMR_ERR_ARG, "unknown mode %d", mode);
     if (!(p->dt0 > 0 && p->dt_max > 0 && p->f_dec > 0 && p->f_inc > 0)) return fail(h, SMR_ERR_ARG, "invalid FIRE parameters");
-    std::vector<int> ids, fresh;
+    std::vector<int> ids;
     for (int s = 0; s < h->max_systems; s++) {
-        SlotState& st = h->hs[s];
-        if (!st.active || st.status != SMR_ST_RUNNING) continue;
-        if (st.dt < 0) { st.dt = p->dt0; st.alpha = p->alpha0; st.npos = 0; st.steps = 0; fresh.push_back(s); }
-        ids.push_back(s);
+        const SlotState& st = h->hs[s];
+        if (st.active && st.status == SMR_ST_RUNNING) ids.push_back(s);
     }
-    int r = upload_slots(h, fresh);
-    if (r) return r;
+    int r = 0;
     h->last_launches = 0;
     cudaStream_t s = h->stream;
     KernelArgs a = base_args(h);

@@ -417,9 +417,11 @@ __device__ void run_system(const KernelArgs& a, const Smem& S, int w, int rank) 
     const SlotState st = a.slots[slot];
     const TopoDev tp = a.topos[st.topo];
     const int N = st.natoms;
+    // a slot with dt < 0 has not started FIRE yet: zero velocities, dt0, alpha0
+    const bool fresh = !EVAL && st.dt < 0.0;
     for (int i = rank; i < N; i += T) {
         S.P[i] = a.pos[st.atom_off + i];
-        S.V[i] = EVAL ? make_float4(0.f, 0.f, 0.f, 0.f) : a.vel[st.atom_off + i];
+        S.V[i] = (EVAL || fresh) ? make_float4(0.f, 0.f, 0.f, 0.f) : a.vel[st.atom_off + i];
         const float4 q = __ldg(a.req + tp.atom_off + i);
         S.Q[i] = q;
         S.Ng[i] = a.neigh[tp.atom_off + i];
@@ -444,8 +446,8 @@ __device__ void run_system(const KernelArgs& a, const Smem& S, int w, int rank) 
         return;
     }
 
-    double dt = st.dt, alpha = st.alpha;
-    int npos = st.npos, steps = st.steps, status = st.status;
+    double dt = fresh ? a.fire.dt0 : st.dt, alpha = fresh ? a.fire.alpha0 : st.alpha;
+    int npos = fresh ? 0 : st.npos, steps = fresh ? 0 : st.steps, status = st.status;
     float fmax = st.fmax;
     int nsteps = a.max_steps;
     if (a.step_budget > 0) nsteps = min(nsteps, a.step_budget - steps);
