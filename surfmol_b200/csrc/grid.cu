@@ -359,7 +359,8 @@ int build_grid_device(const GridBuildArgs& A, float4* out, cudaStream_t s, char*
     DevBuf buf;
     // host copy of ions for layer grouping and the geometry checks
     std::vector<double> hion(4 * (size_t)A.nions);
-    GB_CHECK(cudaMemcpy(hion.data(), A.ions, hion.size() * 8, cudaMemcpyDeviceToHost));
+    GB_CHECK(cudaMemcpyAsync(hion.data(), A.ions, hion.size() * 8, cudaMemcpyDeviceToHost, s));
+    GB_CHECK(cudaStreamSynchronize(s));
     double ztop = -1e300, qsum = 0.0, qz = 0.0;
     for (int i = 0; i < A.nions; i++) { ztop = std::max(ztop, hion[4 * i + 2]); qsum += hion[4 * i + 3]; qz += hion[4 * i + 3] * hion[4 * i + 2]; }
     const double dmin = A.p0[2] - ztop;
@@ -397,7 +398,9 @@ int build_grid_device(const GridBuildArgs& A, float4* out, cudaStream_t s, char*
         structure_factor_kernel<<<(w * nk + 127) / 128, 128, 0, s>>>(A.nions, A.ions, ddz, X, Y, H, K, g1, g2, S);
         GB_CHECK(cudaGetLastError());
         std::vector<double2> hS((size_t)w * nk);
-        GB_CHECK(cudaMemcpy(hS.data(), S, hS.size() * sizeof(double2), cudaMemcpyDeviceToHost));
+        // the handle's stream does not synchronise with the legacy default stream: copy on it and wait
+        GB_CHECK(cudaMemcpyAsync(hS.data(), S, hS.size() * sizeof(double2), cudaMemcpyDeviceToHost, s));
+        GB_CHECK(cudaStreamSynchronize(s));
         // amplitudes at the grid bottom and their pruning threshold
         std::vector<double2> amp;
         std::vector<int> hcol, rowptr(1, 0), krow;

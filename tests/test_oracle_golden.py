@@ -110,3 +110,14 @@ def test_ewald_matches_direct_image_sum(oracle):
     pe = oracle.ewald_points(pts, slab.ions, slab.Lx, slab.Ly, gcut=40.0)
     pb = oracle.brute_coulomb_points(pts, slab.ions, slab.Lx, slab.Ly, nrep=60)
     assert np.allclose(pe, pb, atol=2e-3)
+
+
+def test_separable_grid_build_matches_direct(oracle):
+    """orc_build_grid_fast (separable Ewald, used for full-size grids) equals the direct per-point build."""
+    from surfmol_b200 import synth
+    slab = synth.rocksalt_slab(2, 3)
+    args = (slab.ions, slab.req(), slab.Lx, slab.Ly, 10, 10, 8, (0.0, 0.0, 1.0), (slab.Lx / 10, slab.Ly / 10, 0.3))
+    a = oracle.build_grid(*args, gcut=40.0)
+    b = oracle.build_grid_fast(*args)
+    for c in range(3):
+        assert np.abs(a[..., c] - b[..., c]).max() < 1e-9 * np.abs(a[..., c]).max()
