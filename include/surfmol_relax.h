@@ -126,6 +126,29 @@ int smr_get_grid(smr_handle* h, void* coef_out, int* dtype, float scale[4], int 
 int smr_build_grid(smr_handle* h, int nions, const double* ions, const double* ion_re, double Lx, double Ly,
                    int nx, int ny, int nz, const double p0[3], const double step[3],
                    const smr_grid_build_params* p);
+/* Allocation-free grid build.  No counterpart in the reference.  For callers that cannot call
+ * cudaMalloc (a host that owns all device memory through its own pool and forbids allocation
+ * after start-up, or code issuing work during stream capture): builds the same float32 grid as
+ * smr_build_grid, without a handle, into coef_out (a DEVICE buffer of nx*ny*nz*4 floats the
+ * caller owns), on the caller's stream (void* cudaStream_t; 0 = default stream), asynchronously.
+ * ions / ion_re are host arrays as for smr_build_grid.  Scratch is one 8 MiB static device array
+ * per GPU (held until exit): three FP64 channels (24 B per voxel) plus the Ewald tables must fit,
+ * i.e. at most ~340,000 voxels (less for large cells or many ions), 4 <= nx, ny, nz <= 512.
+ * Larger requests fail with SMR_ERR_CAPACITY and a message in err.  The first call on a device looks up the array's address (make it before any
+ * stream capture); calls whose GPU work overlaps share the array and race.  Returns SMR_OK or a
+ * negative SMR_ERR_* code; never allocates device memory. */
+typedef struct {
+    double alpha_morse;
+    int    npbc;
+    double ewald_tol;
+    int    dtype;              /* must be SMR_GRID_F32 */
+    double morse_rcut;
+} smr_grid_build_params_static;
+int smr_build_grid_static(int nions, const double* ions, const double* ion_re, double Lx, double Ly,
+                          int nx, int ny, int nz, const double p0[3], const double step[3],
+                          const smr_grid_build_params_static* p, float* coef_out, void* stream,
+                          char* err, int errlen);
+
 /* Re-encode the current grid to another storage dtype with per-channel scales (max|c| mapping). */
 int smr_convert_grid(smr_handle* h, int dtype);
 

@@ -39,6 +39,11 @@ class SmrGridBuildParams(C.Structure):
                 ("morse_rcut", C.c_double), ("reserved", C.c_int * 4)]
 
 
+class SmrGridBuildParamsStatic(C.Structure):
+    _fields_ = [("alpha_morse", C.c_double), ("npbc", C.c_int), ("ewald_tol", C.c_double), ("dtype", C.c_int),
+                ("morse_rcut", C.c_double)]
+
+
 class SmrTopologyDesc(C.Structure):
     _fields_ = [("natoms", C.c_int), ("req", DP), ("neighs", IP), ("bond_kl", DP),
                 ("nang", C.c_int), ("angs", IP), ("angp", DP),
@@ -58,6 +63,8 @@ SIGNATURES = {
     "smr_build_grid": (C.c_int, [VP, C.c_int, DP, DP, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, DP, DP,
                                  C.POINTER(SmrGridBuildParams)]),
     "smr_convert_grid": (C.c_int, [VP, C.c_int]),
+    "smr_build_grid_static": (C.c_int, [C.c_int, DP, DP, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, DP, DP,
+                                        C.POINTER(SmrGridBuildParamsStatic), VP, VP, C.c_char_p, C.c_int]),
     "smr_add_molecule": (C.c_int, [VP, C.c_int, IP, DP, DP, C.c_double, IP]),
     "smr_add_topology": (C.c_int, [VP, C.POINTER(SmrTopologyDesc), IP]),
     "smr_topology_counts": (C.c_int, [VP, C.c_int, IP]),

@@ -27,6 +27,7 @@
 #include <vector>
 
 #include "smr_internal.h"
+#include "../../include/surfmol_relax.h"
 
 namespace smr {
 namespace {
@@ -481,3 +482,184 @@ int build_grid_device(const GridBuildArgs& A, float4* out, cudaStream_t s, char*
 }
 
 }  // namespace smr
+
+// ============================================================================ allocation-free grid build
+//
+// smr_build_grid_static: the same grid as smr_build_grid for small substrates, for callers that
+// cannot call cudaMalloc -- e.g. a host framework that owns all device memory through its own
+// pool and forbids allocation after start-up (the reference's GPU harness forbids allocation in
+// its step path), or code issuing work while a CUDA stream is being captured.  All scratch lives
+// in the file-scope array below: kStaticScratchBytes (8 MiB) held by every GPU that loads the
+// library, until the process exits.  In host code the array's name is only a host-side stand-in,
+// so the entry point looks up its device address with cudaGetSymbolAddress, once per device, on
+// the first call made on that device (that first call should come before any stream capture).
+// Every call shares the array: calls whose GPU work overlaps (different streams or threads) race.
+// Nothing in it has to start at zero: each buffer is written before it is read.  Differences to
+// smr_build_grid: no pruning of negligible reciprocal vectors (all G with |G| <= gmax are summed)
+// and the structure factors are summed directly per ion; both agree to ~1e-12 relative.
+static __device__ __align__(256) unsigned char smr_grid_static_scratch[8u << 20];
+
+namespace smr {
+namespace {
+
+constexpr size_t kStaticScratchBytes = 8u << 20;
+constexpr int kStaticMaxDevices = 64;
+void* g_static_ptr[kStaticMaxDevices] = {nullptr};
+
+__global__ void static_structure_factor(int nions, const double* __restrict__ ions, double z0, int H, int K,
+                                        double g1, double g2, double2* __restrict__ S) {
+    const int w = 2 * H + 1;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= w * (2 * K + 1)) return;
+    const double Gx = (t % w - H) * g1, Gy = (t / w - K) * g2, Gn = sqrt(Gx * Gx + Gy * Gy);
+    double sr = 0.0, si = 0.0;
+    for (int i = 0; i < nions; i++) {
+        double s, c;
+        sincos(-(Gx * ions[4 * i] + Gy * ions[4 * i + 1]), &s, &c);
+        const double q = ions[4 * i + 3] * exp(-Gn * (z0 - ions[4 * i + 2]));
+        sr += q * c; si += q * s;
+    }
+    S[t] = make_double2(sr, si);
+}
+
+// out[(m + half) * n + i] = exp(i m g (p0 + i st)), m in [-half, half]
+__global__ void static_phase(int n, int half, double p0, double st, double g, double2* __restrict__ out) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (2 * half + 1) * n) return;
+    double s, c;
+    sincos((double)(t / n - half) * g * (p0 + (t % n) * st), &s, &c);
+    out[t] = make_double2(c, s);
+}
+
+// B[kk * nx + ix] = sum_h pref(G) S(h, k) exp(-|G| dzp) Ex[h, ix] over 0 < |G| <= gmax
+__global__ void static_stage1(int H, int K, const double2* __restrict__ S, double gmax, double g1, double g2, double area,
+                              double dzp, int nx, const double2* __restrict__ Ex, double2* __restrict__ B) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (2 * K + 1) * nx) return;
+    const int kk = t / nx, ix = t % nx, w = 2 * H + 1;
+    const double Gy = (kk - K) * g2;
+    double br = 0.0, bi = 0.0;
+    for (int hh = 0; hh < w; hh++) {
+        const double Gx = (hh - H) * g1, G = sqrt(Gx * Gx + Gy * Gy);
+        if (G == 0.0 || G > gmax) continue;
+        const double f = 2.0 * kPi / (area * G) * exp(-G * dzp);
+        const double2 a = S[(size_t)kk * w + hh];
+        const double2 c = Ex[(size_t)hh * nx + ix];
+        br += f * (a.x * c.x - a.y * c.y);
+        bi += f * (a.x * c.y + a.y * c.x);
+    }
+    B[t] = make_double2(br, bi);
+}
+
+// Thomas tables on the host stack (n <= kStaticMaxLine)
+constexpr int kStaticMaxLine = 512;
+void thomas_stack(int n, double b0, double bn, double* cp, double* m) {
+    const double a = 1.0 / 6.0, b = 2.0 / 3.0;
+    m[0] = b0; cp[0] = a / m[0];
+    for (int i = 1; i < n; i++) { const double di = (i == n - 1) ? bn : b; m[i] = di - a * cp[i - 1]; cp[i] = a / m[i]; }
+}
+
+}  // namespace
+}  // namespace smr
+
+extern "C" int smr_build_grid_static(int nions, const double* ions, const double* ion_re, double Lx, double Ly,
+                                     int nx, int ny, int nz, const double p0[3], const double step[3],
+                                     const smr_grid_build_params_static* p, float* coef_out, void* stream,
+                                     char* err, int errlen) {
+    using namespace smr;
+    auto fail = [&](int code, const char* msg) { if (err && errlen > 0) std::snprintf(err, errlen, "%s", msg); return code; };
+    if (!ions || !ion_re || !p0 || !step || !p || !coef_out || nions <= 0) return fail(-1, "null argument or no ions");
+    if (p->dtype != GRID_F32) return fail(-5, "only float32 output is supported without allocation");
+    if (nx < 4 || ny < 4 || nz < 4 || nx > kStaticMaxLine || ny > kStaticMaxLine || nz > kStaticMaxLine)
+        return fail(-1, "grid dimensions must be in [4, 512]");
+    if (!(Lx > 0 && Ly > 0)) return fail(-1, "cell must be positive");
+    double ztop = -1e300, qsum = 0.0, qz = 0.0;
+    for (int i = 0; i < nions; i++) { ztop = std::max(ztop, ions[4 * i + 2]); qsum += ions[4 * i + 3]; qz += ions[4 * i + 3] * ions[4 * i + 2]; }
+    const double dmin = p0[2] - ztop;
+    if (!(dmin > 0.05)) return fail(-1, "grid bottom must lie above the top ion");
+    if (std::fabs(qsum) > 1e-6 * std::max(1.0, (double)nions)) return fail(-1, "slab is not neutral");
+    const double g1 = 2.0 * kPi / Lx, g2 = 2.0 * kPi / Ly, area = Lx * Ly;
+    const double tol = p->ewald_tol > 0 ? p->ewald_tol : 1e-12;
+    const double gmax = -std::log(tol) / dmin;
+    const int H = std::max(1, (int)std::floor(gmax / g1)), K = std::max(1, (int)std::floor(gmax / g2));
+    const int w = 2 * H + 1, nk = 2 * K + 1;
+    const size_t N = (size_t)nx * ny * nz;
+    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+    const size_t need = 3 * al(N * 8) + 2 * al((size_t)nions * 32) + al((size_t)w * nk * 16) + al((size_t)w * nx * 16) +
+                        al((size_t)nk * ny * 16) + al((size_t)nk * nx * 16) + 8 * al(kStaticMaxLine * 8);
+    if (need > kStaticScratchBytes) {
+        char msg[200];
+        std::snprintf(msg, sizeof(msg), "needs %zu bytes of scratch, more than the static %zu (reduce the grid, the ions "
+                      "or raise ewald_tol)", need, kStaticScratchBytes);
+        return fail(-3, msg);
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kStaticMaxDevices) return fail(-2, "no current CUDA device");
+    if (!g_static_ptr[dev]) {   // first call on this device: device address of the static array
+        void* ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, smr_grid_static_scratch);
+        if (e != cudaSuccess || !ptr) return fail(-2, cudaGetErrorString(e));
+        g_static_ptr[dev] = ptr;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned char* base = (unsigned char*)g_static_ptr[dev];
+    size_t off = 0;
+    auto take = [&](size_t bytes) { void* q = base + off; off += al(bytes); return q; };
+    double* paul = (double*)take(N * 8);
+    double* lond = (double*)take(N * 8);
+    double* coul = (double*)take(N * 8);
+    double* dions = (double*)take((size_t)nions * 32);
+    double* dre = (double*)take((size_t)nions * 32);
+    double2* S = (double2*)take((size_t)w * nk * 16);
+    double2* Ex = (double2*)take((size_t)w * nx * 16);
+    double2* Ey = (double2*)take((size_t)nk * ny * 16);
+    double2* B = (double2*)take((size_t)nk * nx * 16);
+    double* tab[8];
+    for (int k = 0; k < 8; k++) tab[k] = (double*)take(kStaticMaxLine * 8);
+#define ST_CHECK(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) return fail(-2, cudaGetErrorString(e_)); } while (0)
+    ST_CHECK(cudaMemcpyAsync(dions, ions, (size_t)nions * 32, cudaMemcpyHostToDevice, s));
+    ST_CHECK(cudaMemcpy2DAsync(dre, 32, ion_re, 16, 16, nions, cudaMemcpyHostToDevice, s));
+    const float rc2 = p->morse_rcut > 0 ? (float)(p->morse_rcut * p->morse_rcut) : 3.0e38f;
+    morse_kernel<<<(unsigned)((N + 127) / 128), 128, 0, s>>>(nions, dions, dre, Lx, Ly, p->npbc, nx, ny, nz, p0[0], p0[1], p0[2],
+                                                             step[0], step[1], step[2], (float)p->alpha_morse, rc2, paul, lond);
+    static_structure_factor<<<(w * nk + 127) / 128, 128, 0, s>>>(nions, dions, p0[2], H, K, g1, g2, S);
+    static_phase<<<(w * nx + 255) / 256, 256, 0, s>>>(nx, H, p0[0], step[0], g1, Ex);
+    static_phase<<<(nk * ny + 255) / 256, 256, 0, s>>>(ny, K, p0[1], step[1], g2, Ey);
+    ST_CHECK(cudaGetLastError());
+    for (int iz = 0; iz < nz; iz++) {
+        const double z = p0[2] + iz * step[2];
+        const double phi0 = -(2.0 * kPi / area) * (qsum * z - qz);
+        static_stage1<<<(nk * nx + 127) / 128, 128, 0, s>>>(H, K, S, gmax, g1, g2, area, iz * step[2], nx, Ex, B);
+        ewald_stage2<<<(nx * ny + 127) / 128, 128, 0, s>>>(nk, B, Ey, nx, ny, phi0, iz, nz, coul);
+    }
+    ST_CHECK(cudaGetLastError());
+    // exact B-spline fit: z open, y and x cyclic (tables from the host stack)
+    const double a = 1.0 / 6.0, b = 2.0 / 3.0, gamma = -b;
+    double cp[kStaticMaxLine], m[kStaticMaxLine], u[kStaticMaxLine];
+    thomas_stack(nz, b, b, cp, m);
+    ST_CHECK(cudaMemcpyAsync(tab[0], cp, nz * 8, cudaMemcpyHostToDevice, s));
+    ST_CHECK(cudaMemcpyAsync(tab[1], m, nz * 8, cudaMemcpyHostToDevice, s));
+    double den[2];
+    for (int axis = 0; axis < 2; axis++) {
+        const int n = axis == 0 ? ny : nx;
+        thomas_stack(n, b - gamma, b - a * a / gamma, cp, m);
+        for (int i = 0; i < n; i++) u[i] = 0.0;
+        u[0] = gamma; u[n - 1] = a;
+        u[0] /= m[0];
+        for (int i = 1; i < n; i++) u[i] = (u[i] - a * u[i - 1]) / m[i];
+        for (int i = n - 2; i >= 0; i--) u[i] -= cp[i] * u[i + 1];
+        den[axis] = 1.0 + u[0] + a * u[n - 1] / gamma;
+        ST_CHECK(cudaMemcpyAsync(tab[2 + 3 * axis], cp, n * 8, cudaMemcpyHostToDevice, s));
+        ST_CHECK(cudaMemcpyAsync(tab[3 + 3 * axis], m, n * 8, cudaMemcpyHostToDevice, s));
+        ST_CHECK(cudaMemcpyAsync(tab[4 + 3 * axis], u, n * 8, cudaMemcpyHostToDevice, s));
+    }
+    for (double* ch : {paul, lond, coul}) {
+        fit_z<<<(nx * ny + 127) / 128, 128, 0, s>>>(ch, nx, ny, nz, tab[0], tab[1]);
+        fit_y<<<(nx * nz + 127) / 128, 128, 0, s>>>(ch, nx, ny, nz, tab[2], tab[3], tab[4], gamma, den[0]);
+        fit_x<<<(ny * nz + 127) / 128, 128, 0, s>>>(ch, nx, ny, nz, tab[5], tab[6], tab[7], gamma, den[1]);
+    }
+    pack_kernel<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(N, paul, lond, coul, (float4*)coef_out);
+    ST_CHECK(cudaGetLastError());
+#undef ST_CHECK
+    return 0;
+}
