@@ -212,6 +212,27 @@ int smr_download(smr_handle* h, int nsys, const int* slot_ids, float* pos, float
  * smr_eval_forces call, and the number of kernel launches it made. */
 int smr_last_timing(smr_handle* h, double* ms, long long* launches);
 
+/* Schedule of smr_run_fire (batched and plain alike): every system runs its first switch_step
+ * FIRE steps in the rounds form (warp-sized teams, bonded terms in conflict-free rounds: best
+ * throughput when many systems share the GPU) and later steps in the gather form with
+ * latency_team threads per system (all bonded terms at once into shared memory, then a
+ * per-atom gather: best latency for the slow tail of a batch).  switch_step <= 0 keeps the
+ * rounds form throughout; latency_team 0 picks by size.  The switch depends only on a system's
+ * own step count, so results do not depend on what else runs.  eval_form (0 rounds, 1 gather)
+ * selects the form of smr_eval_forces. */
+int smr_set_schedule(smr_handle* h, int switch_step, int latency_team, int eval_form);
+int smr_get_schedule(smr_handle* h, int* switch_step, int* latency_team, int* eval_form);
+
+/* General schedule: nstages (1..16) stages; stage k covers FIRE steps [starts[k], starts[k+1])
+ * (the last one is open), starts[0] == 0 and strictly increasing.  Stage 0 runs the rounds form
+ * with the topology's team (teams[0] ignored); stage k >= 1 runs the gather form with teams[k]
+ * threads per system (0: pick by size; 32, 64, 128, 256 or 512).  In batched mode every stage
+ * is a separate launch over the systems still running, which also spreads the remaining
+ * systems evenly over the SMs again.  smr_set_schedule(h, s, t, f) equals the two stages
+ * {0, s} / {0, t}.  No counterpart in the reference (its OpenCL harness has one kernel form). */
+int smr_set_stages(smr_handle* h, int nstages, const int* starts, const int* teams, int eval_form);
+int smr_get_stages(smr_handle* h, int* nstages, int* starts, int* teams);
+
 /* Team configuration of the persistent kernel: threads per system team for systems of
  * up to n atoms (0 = library default / autotuned). */
 int smr_set_team_size(smr_handle* h, int max_atoms, int threads);

@@ -86,6 +86,10 @@ SIGNATURES = {
     "smr_download": (C.c_int, [VP, C.c_int, IP, FP, FP, DP, IP, IP]),
     "smr_last_timing": (C.c_int, [VP, DP, LLP]),
     "smr_set_team_size": (C.c_int, [VP, C.c_int, C.c_int]),
+    "smr_set_schedule": (C.c_int, [VP, C.c_int, C.c_int, C.c_int]),
+    "smr_get_schedule": (C.c_int, [VP, IP, IP, IP]),
+    "smr_set_stages": (C.c_int, [VP, C.c_int, IP, IP, C.c_int]),
+    "smr_get_stages": (C.c_int, [VP, IP, IP, IP]),
 }
 
 _lib = None

@@ -63,7 +63,7 @@ struct smr_handle {
     long long max_atoms = 0;
 
     // per-atom system state and per-slot state
-    float4 *pos = nullptr, *vel = nullptr, *force = nullptr, *stage = nullptr;
+    float4 *pos = nullptr, *plo = nullptr, *vel = nullptr, *force = nullptr, *stage = nullptr;
     SlotState* slots = nullptr;
     int* work = nullptr;
     int* counter = nullptr;
@@ -83,8 +83,16 @@ struct smr_handle {
     std::vector<AngRec> hang; std::vector<DihRec> hdih; std::vector<InvRec> hinv;
     DArr<float4> dreq, dbk, dbl; DArr<short4> dneigh;
     DArr<AngRec> dang; DArr<DihRec> ddih; DArr<InvRec> dinv;
-    size_t up_atoms = 0, up_ang = 0, up_dih = 0, up_inv = 0, up_topo = 0;   // uploaded prefixes
+    std::vector<int2> ha2f; std::vector<int> hidx;      // gather form: per atom (start, count), piece indices
+    DArr<int2> da2f; DArr<int> didx;
+    size_t up_atoms = 0, up_ang = 0, up_dih = 0, up_inv = 0, up_topo = 0, up_idx = 0;   // uploaded prefixes
     std::map<int, int> team_override;   // max_atoms -> threads
+    // schedule: stage 0 runs FIRE steps [0, stage_start[1]) in the rounds form with the topology's
+    // team; stage k >= 1 runs steps [stage_start[k], stage_start[k+1]) in the gather form with
+    // stage_team[k] threads per system (0: pick by size).  One stage = the rounds form throughout.
+    std::vector<int> stage_start{0};
+    std::vector<int> stage_team{0};
+    int eval_form = 0;                  // form used by smr_eval_forces
 
     // grid
     void* grid = nullptr;
@@ -139,6 +147,15 @@ void append_topology(smr_handle* h, const HostTopo& T) {
     td.ang_off = (int)h->hang.size(); td.ang_rounds = P.ang_rounds; h->hang.insert(h->hang.end(), P.ang.begin(), P.ang.end());
     td.dih_off = (int)h->hdih.size(); td.dih_rounds = P.dih_rounds; h->hdih.insert(h->hdih.end(), P.dih.begin(), P.dih.end());
     td.inv_off = (int)h->hinv.size(); td.inv_rounds = P.inv_rounds; h->hinv.insert(h->hinv.end(), P.inv.begin(), P.inv.end());
+    FlatTerms F;
+    flat_terms(T, F);
+    td.nang = (int)F.ang.size(); td.ndih = (int)F.dih.size(); td.ninv = (int)F.inv.size(); td.npieces = F.npieces;
+    td.fang_off = (int)h->hang.size(); h->hang.insert(h->hang.end(), F.ang.begin(), F.ang.end());
+    td.fdih_off = (int)h->hdih.size(); h->hdih.insert(h->hdih.end(), F.dih.begin(), F.dih.end());
+    td.finv_off = (int)h->hinv.size(); h->hinv.insert(h->hinv.end(), F.inv.begin(), F.inv.end());
+    td.a2f_off = (int)h->hidx.size();
+    h->ha2f.insert(h->ha2f.end(), F.a2f.begin(), F.a2f.end());
+    h->hidx.insert(h->hidx.end(), F.idx.begin(), F.idx.end());
     h->htd.push_back(td);
 }
 
@@ -160,7 +177,9 @@ int upload_all(smr_handle* h) {
     t = ua; CU(h, sync_arr(h->dneigh, h->hneigh, t, s));
     t = ua; CU(h, sync_arr(h->dbk, h->hbk, t, s));
     t = ua; CU(h, sync_arr(h->dbl, h->hbl, t, s));
+    t = ua; CU(h, sync_arr(h->da2f, h->ha2f, t, s));
     h->up_atoms = h->hreq.size();
+    CU(h, sync_arr(h->didx, h->hidx, h->up_idx, s));
     CU(h, sync_arr(h->dang, h->hang, h->up_ang, s));
     CU(h, sync_arr(h->ddih, h->hdih, h->up_dih, s));
     CU(h, sync_arr(h->dinv, h->hinv, h->up_inv, s));
@@ -171,8 +190,8 @@ int upload_all(smr_handle* h) {
 // repack every topology for the current team mapping (after smr_set_team_size)
 int repack_all(smr_handle* h) {
     h->htd.clear(); h->hreq.clear(); h->hneigh.clear(); h->hbk.clear(); h->hbl.clear();
-    h->hang.clear(); h->hdih.clear(); h->hinv.clear();
-    h->up_atoms = h->up_ang = h->up_dih = h->up_inv = h->up_topo = 0;
+    h->hang.clear(); h->hdih.clear(); h->hinv.clear(); h->ha2f.clear(); h->hidx.clear();
+    h->up_atoms = h->up_ang = h->up_dih = h->up_inv = h->up_topo = h->up_idx = 0;
     for (const HostTopo& T : h->topos) append_topology(h, T);
     return upload_all(h);
 }
@@ -239,7 +258,8 @@ KernelArgs base_args(smr_handle* h) {
     a.topos = h->dtd.d;
     a.req = h->dreq.d; a.neigh = h->dneigh.d; a.bk = h->dbk.d; a.bl = h->dbl.d;
     a.angs = h->dang.d; a.dihs = h->ddih.d; a.invs = h->dinv.d;
-    a.pos = h->pos; a.vel = h->vel; a.force = h->force;
+    a.a2f = h->da2f.d; a.a2f_idx = h->didx.d;
+    a.pos = h->pos; a.plo = h->plo; a.vel = h->vel; a.force = h->force;
     a.has_grid = h->has_grid ? 1 : 0;
     a.grid.data = h->grid;
     a.grid.dtype = h->grid_dtype;
@@ -252,19 +272,61 @@ KernelArgs base_args(smr_handle* h) {
     return a;
 }
 
-// group slots by team size; returns (team, begin, end, nmax) segments of the reordered list
-struct Seg { int team, begin, end, nmax; };
-std::vector<Seg> group_by_team(smr_handle* h, std::vector<int>& ids) {
+// group slots by launch configuration; returns (team, form, begin, end, nmax, nfmax) segments
+struct Seg { int team, form, begin, end, nmax, nfmax; };
+
+int latency_team_for(int requested, int n) {
+    if (requested) return requested;
+    return n <= 64 ? 128 : (n <= 200 ? 256 : 512);
+}
+
+// Launch segments for a list of slots.  The form of every system is decided from the system
+// alone (the gather form when its own shared memory fits, else the rounds form with its
+// topology's team), never from what it is batched with; segments group equal (form, team) and
+// are split wherever the segment's largest system would no longer fit.
+std::vector<Seg> group_by(smr_handle* h, std::vector<int>& ids, int form, int lat_team = 0) {
+    struct Key { int form, team, n, nf; };
+    auto key_of = [&](int s) {
+        const SlotState& st = h->hs[s];
+        const int n = st.natoms, nf = h->htd[st.topo].npieces;
+        if (form == FORM_GATHER) {
+            const int t = latency_team_for(lat_team, n);
+            if (team_smem_bytes(n, nf, t, FORM_GATHER) <= h->smem_optin) return Key{FORM_GATHER, t, n, nf};
+        }
+        return Key{FORM_ROUNDS, h->htd[st.topo].team, n, nf};
+    };
+    std::vector<Key> keys(h->max_systems);
+    for (int s : ids) keys[s] = key_of(s);
     std::stable_sort(ids.begin(), ids.end(), [&](int a, int b) {
-        return h->htd[h->hs[a].topo].team < h->htd[h->hs[b].topo].team;
+        const Key &x = keys[a], &y = keys[b];
+        if (x.form != y.form) return x.form < y.form;
+        if (x.team != y.team) return x.team < y.team;
+        return x.n < y.n;
     });
     std::vector<Seg> segs;
     for (int i = 0; i < (int)ids.size(); i++) {
-        int t = h->htd[h->hs[ids[i]].topo].team, n = h->hs[ids[i]].natoms;
-        if (segs.empty() || segs.back().team != t) segs.push_back({t, i, i + 1, n});
-        else { segs.back().end = i + 1; segs.back().nmax = std::max(segs.back().nmax, n); }
+        const Key& k = keys[ids[i]];
+        if (!segs.empty()) {
+            Seg& g = segs.back();
+            if (g.form == k.form && g.team == k.team &&
+                team_smem_bytes(std::max(g.nmax, k.n), std::max(g.nfmax, k.nf), k.team, k.form) <= h->smem_optin) {
+                g.end = i + 1; g.nmax = std::max(g.nmax, k.n); g.nfmax = std::max(g.nfmax, k.nf);
+                continue;
+            }
+        }
+        segs.push_back({k.team, k.form, i, i + 1, k.n, k.nf});
     }
     return segs;
+}
+
+bool fits(const smr_handle* h, const Seg& g) {
+    return team_smem_bytes(g.nmax, g.nfmax, g.team, g.form) <= h->smem_optin;
+}
+
+int check_smem(smr_handle* h, const Seg& g) {
+    if (fits(h, g)) return 0;
+    return fail(h, SMR_ERR_CAPACITY, "systems of %d atoms need %zu B of shared memory per block (device limit %zu); "
+                "use a larger team or smaller systems", g.nmax, team_smem_bytes(g.nmax, g.nfmax, g.team, g.form), h->smem_optin);
 }
 
 // a batch of slots must be distinct, active and fit the staging buffers
@@ -277,14 +339,6 @@ int check_batch(smr_handle* h, int nsys, const int* ids) {
         if (seen[s]) return fail(h, SMR_ERR_ARG, "slot %d listed twice", s);
         seen[s] = 1;
     }
-    return 0;
-}
-
-int check_smem(smr_handle* h, const Seg& g) {
-    size_t need = team_smem_bytes(g.nmax) * (g.team == 32 ? 4 : 1);
-    if (need > h->smem_optin)
-        return fail(h, SMR_ERR_CAPACITY, "systems of %d atoms need %zu B of shared memory per block (device limit %zu); "
-                    "use a larger team or smaller systems", g.nmax, need, h->smem_optin);
     return 0;
 }
 
@@ -313,13 +367,14 @@ int smr_create(const smr_config* cfg, smr_handle** out) {
     cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device); h->smem_optin = (size_t)v;
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(SMR_ERR_CUDA);
     size_t na = (size_t)cfg->max_atoms, ns = (size_t)cfg->max_systems;
-    if (cudaMalloc(&h->pos, na * 16) || cudaMalloc(&h->vel, na * 16) || cudaMalloc(&h->force, na * 16) ||
+    if (cudaMalloc(&h->pos, na * 16) || cudaMalloc(&h->plo, na * 16) || cudaMalloc(&h->vel, na * 16) || cudaMalloc(&h->force, na * 16) ||
         cudaMalloc(&h->stage, na * 16) || cudaMalloc(&h->slots, ns * sizeof(SlotState)) ||
         cudaMalloc(&h->work, ns * 4) || cudaMalloc(&h->counter, 64) || cudaMalloc(&h->ecomp, ns * 8 * 8) ||
         cudaMalloc(&h->xfer, ns * 3 * 4) || cudaMallocHost(&h->pinned, na * 16))
         return bail(SMR_ERR_CUDA);
     cudaMemset(h->slots, 0, ns * sizeof(SlotState));
     cudaMemset(h->vel, 0, na * 16);
+    cudaMemset(h->plo, 0, na * 16);
     h->hs.assign(ns, SlotState{});
     for (int s = (int)ns - 1; s >= 0; s--) h->free_slots.push_back(s);
     h->free_atoms[0] = (long long)na;
@@ -332,7 +387,7 @@ int smr_create(const smr_config* cfg, smr_handle** out) {
 int smr_destroy(smr_handle* h) {
     if (!h) return SMR_ERR_ARG;
     if (h->stream) cudaStreamSynchronize(h->stream);
-    cudaFree(h->pos); cudaFree(h->vel); cudaFree(h->force); cudaFree(h->stage); cudaFree(h->slots);
+    cudaFree(h->pos); cudaFree(h->plo); cudaFree(h->vel); cudaFree(h->force); cudaFree(h->stage); cudaFree(h->slots);
     cudaFree(h->work); cudaFree(h->counter); cudaFree(h->ecomp); cudaFree(h->xfer);
     if (h->pinned) cudaFreeHost(h->pinned);
     if (h->grid) cudaFree(h->grid);
@@ -548,6 +603,8 @@ int smr_add_systems(smr_handle* h, int nsys, const int* topo_ids, const float* p
     std::copy(src.begin(), src.end(), desc.begin()); std::copy(len.begin(), len.end(), desc.begin() + nsys); std::copy(dst.begin(), dst.end(), desc.begin() + 2 * nsys);
     CU(h, cudaMemcpyAsync(h->xfer, desc.data(), desc.size() * 4, cudaMemcpyHostToDevice, s));
     if (launch_copy_segments(h->xfer, h->xfer + nsys, h->xfer + 2 * nsys, nsys, h->stage, h->pos, s)) return fail(h, SMR_ERR_CUDA, "scatter launch failed");
+    CU(h, cudaMemsetAsync(h->stage, 0, (size_t)p * 16, s));
+    if (launch_copy_segments(h->xfer, h->xfer + nsys, h->xfer + 2 * nsys, nsys, h->stage, h->plo, s)) return fail(h, SMR_ERR_CUDA, "scatter launch failed");
     int r = upload_slots(h, ids);
     if (r) return r;
     r = wait_stream(h, 600.0);
@@ -586,6 +643,9 @@ int smr_set_positions(smr_handle* h, int nsys, const int* slot_ids, const float*
     CU(h, cudaMemcpyAsync(h->stage, h->pinned, p * 16, cudaMemcpyHostToDevice, h->stream));
     CU(h, cudaMemcpyAsync(h->xfer, desc.data(), desc.size() * 4, cudaMemcpyHostToDevice, h->stream));
     if (launch_copy_segments(h->xfer, h->xfer + nsys, h->xfer + 2 * nsys, nsys, h->stage, h->pos, h->stream)) return fail(h, SMR_ERR_CUDA, "scatter launch failed");
+    // new positions carry no accumulated low part
+    CU(h, cudaMemsetAsync(h->stage, 0, (size_t)p * 16, h->stream));
+    if (launch_copy_segments(h->xfer, h->xfer + nsys, h->xfer + 2 * nsys, nsys, h->stage, h->plo, h->stream)) return fail(h, SMR_ERR_CUDA, "scatter launch failed");
     return wait_stream(h, 600.0);
 }
 
@@ -613,27 +673,22 @@ int smr_reset_fire(smr_handle* h, int nsys, const int* slot_ids) {
 int smr_eval_forces(smr_handle* h, int nsys, const int* slot_ids, float* forces, double* energy) {
     if (!h || nsys < 0 || (nsys && !slot_ids)) return SMR_ERR_ARG;
     { int r = check_batch(h, nsys, slot_ids); if (r) return r; }
-    for (int i = 0; i < nsys; i++) if (!valid_slot(h, slot_ids[i])) return fail(h, SMR_ERR_ARG, "slot %d not active", slot_ids[i]);
     if (nsys == 0) return SMR_OK;
-    std::vector<int> ids(slot_ids, slot_ids + nsys);
-    std::vector<int> order(nsys);
-    for (int i = 0; i < nsys; i++) order[i] = i;
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return h->htd[h->hs[ids[a]].topo].team < h->htd[h->hs[ids[b]].topo].team; });
-    std::vector<int> sorted(nsys);
-    for (int i = 0; i < nsys; i++) sorted[i] = ids[order[i]];
-    std::vector<int> tmp = sorted;
-    auto segs = group_by_team(h, tmp);
+    std::vector<int> sorted(slot_ids, slot_ids + nsys);
+    auto segs = group_by(h, sorted, h->eval_form);
     for (auto& g : segs) { int r = check_smem(h, g); if (r) return r; }
+    std::vector<int> pos_in_input(h->max_systems);
+    for (int i = 0; i < nsys; i++) pos_in_input[slot_ids[i]] = i;
     cudaStream_t s = h->stream;
     CU(h, cudaMemcpyAsync(h->work, sorted.data(), nsys * 4, cudaMemcpyHostToDevice, s));
     KernelArgs a = base_args(h);
     h->last_launches = 0;
     cudaEventRecord(h->ev0, s);
     for (auto& g : segs) {
-        a.work = h->work + g.begin; a.nwork = g.end - g.begin; a.nmax = g.nmax;
+        a.work = h->work + g.begin; a.nwork = g.end - g.begin; a.nmax = g.nmax; a.nfmax = g.nfmax;
         a.ecomp = h->ecomp + (size_t)g.begin * 8;
         CU(h, cudaMemsetAsync(h->counter, 0, 4, s));
-        int r = launch_relax(a, g.team, 1, s, h->num_sms, &h->last_launches);
+        int r = launch_relax(a, g.team, g.form, 1, s, h->num_sms, &h->last_launches);
         if (r) return fail(h, SMR_ERR_CUDA, "eval launch: %s", cudaGetErrorString((cudaError_t)r));
     }
     cudaEventRecord(h->ev1, s);
@@ -645,7 +700,7 @@ int smr_eval_forces(smr_handle* h, int nsys, const int* slot_ids, float* forces,
     if (energy) {
         std::vector<double> e((size_t)nsys * 8);
         CU(h, cudaMemcpy(e.data(), h->ecomp, e.size() * 8, cudaMemcpyDeviceToHost));
-        for (int i = 0; i < nsys; i++) std::copy(&e[(size_t)i * 8], &e[(size_t)i * 8 + 8], energy + (size_t)order[i] * 8);
+        for (int i = 0; i < nsys; i++) std::copy(&e[(size_t)i * 8], &e[(size_t)i * 8 + 8], energy + (size_t)pos_in_input[sorted[i]] * 8);
     }
     if (forces) {
         r = smr_download(h, nsys, slot_ids, nullptr, forces, nullptr, nullptr, nullptr);
@@ -654,50 +709,115 @@ int smr_eval_forces(smr_handle* h, int nsys, const int* slot_ids, float* forces,
     return SMR_OK;
 }
 
+static bool team_ok(int t) { return t == 0 || t == 32 || t == 64 || t == 128 || t == 256 || t == 512; }
+
+int smr_set_stages(smr_handle* h, int nstages, const int* starts, const int* teams, int eval_form) {
+    if (!h || nstages < 1 || nstages > 16 || !starts || !teams) return SMR_ERR_ARG;
+    if (starts[0] != 0) return fail(h, SMR_ERR_ARG, "the first stage must start at step 0");
+    for (int k = 1; k < nstages; k++) if (starts[k] <= starts[k - 1]) return fail(h, SMR_ERR_ARG, "stage starts must increase");
+    for (int k = 0; k < nstages; k++) if (!team_ok(teams[k])) return fail(h, SMR_ERR_ARG, "stage team must be 0, 32, 64, 128, 256 or 512");
+    if (eval_form != FORM_ROUNDS && eval_form != FORM_GATHER) return fail(h, SMR_ERR_ARG, "eval form must be 0 (rounds) or 1 (gather)");
+    h->stage_start.assign(starts, starts + nstages);
+    h->stage_team.assign(teams, teams + nstages);
+    h->eval_form = eval_form;
+    return SMR_OK;
+}
+
+int smr_set_schedule(smr_handle* h, int switch_step, int latency_team, int eval_form) {
+    if (!h) return SMR_ERR_ARG;
+    if (switch_step <= 0) { int st = 0, tm = 0; return smr_set_stages(h, 1, &st, &tm, eval_form); }
+    int st[2] = {0, switch_step}, tm[2] = {0, latency_team};
+    return smr_set_stages(h, 2, st, tm, eval_form);
+}
+
+int smr_get_stages(smr_handle* h, int* nstages, int* starts, int* teams) {
+    if (!h || !nstages) return SMR_ERR_ARG;
+    const int n = (int)h->stage_start.size();
+    if (starts && teams) {
+        if (*nstages < n) return fail(h, SMR_ERR_CAPACITY, "schedule has %d stages", n);
+        std::copy(h->stage_start.begin(), h->stage_start.end(), starts);
+        std::copy(h->stage_team.begin(), h->stage_team.end(), teams);
+    }
+    *nstages = n;
+    return SMR_OK;
+}
+
+int smr_get_schedule(smr_handle* h, int* switch_step, int* latency_team, int* eval_form) {
+    if (!h) return SMR_ERR_ARG;
+    if (switch_step) *switch_step = h->stage_start.size() > 1 ? h->stage_start[1] : 0;
+    if (latency_team) *latency_team = h->stage_team.size() > 1 ? h->stage_team[1] : 0;
+    if (eval_form) *eval_form = h->eval_form;
+    return SMR_OK;
+}
+
 int smr_run_fire(smr_handle* h, int max_steps, int step_budget, const smr_fire_params* p, int mode, int* nfinished) {
     if (!h || !p || max_steps < 0) return SMR_ERR_ARG;
     if (mode != SMR_MODE_BATCHED && mode != SMR_MODE_PLAIN) return fail(h, SMR_ERR_ARG, "unknown mode %d", mode);
     if (!(p->dt0 > 0 && p->dt_max > 0 && p->f_dec > 0 && p->f_inc > 0)) return fail(h, SMR_ERR_ARG, "invalid FIRE parameters");
+    // every running slot may advance to min(steps + max_steps, step_budget) in this call
     std::vector<int> ids;
+    std::vector<int> start(h->max_systems, 0);
     for (int s = 0; s < h->max_systems; s++) {
-        const SlotState& st = h->hs[s];
-        if (st.active && st.status == SMR_ST_RUNNING) ids.push_back(s);
+        SlotState& st = h->hs[s];
+        if (!st.active || st.status != SMR_ST_RUNNING) continue;
+        const int cur = st.dt < 0 ? 0 : st.steps;
+        long long tgt = (long long)cur + max_steps;
+        if (step_budget > 0) tgt = std::min<long long>(tgt, step_budget);
+        st.target = (int)std::min<long long>(tgt, 0x7fffffff);
+        start[s] = cur;
+        ids.push_back(s);
     }
-    int r = 0;
+    int r = upload_slots(h, ids);
+    if (r) return r;
     h->last_launches = 0;
     cudaStream_t s = h->stream;
     KernelArgs a = base_args(h);
     a.fire = FireDev{p->dt0, p->dt_max, p->alpha0, p->f_inc, p->f_dec, p->f_alpha, p->fconv, p->flimit, p->n_min};
     a.step_budget = step_budget;
-    auto segs = group_by_team(h, ids);
-    for (auto& g : segs) { r = check_smem(h, g); if (r) return r; }
-    if (!ids.empty()) CU(h, cudaMemcpyAsync(h->work, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice, s));
+    const int nst = (int)h->stage_start.size();
+    auto stage_end = [&](int k) { return k + 1 < nst ? h->stage_start[k + 1] : 0x7fffffff; };
+    // per stage: segments of the running systems in that stage's form and team
+    std::vector<std::vector<int>> sids(nst, ids);
+    std::vector<std::vector<Seg>> ssegs(nst);
+    for (int k = 0; k < nst; k++) ssegs[k] = group_by(h, sids[k], k == 0 ? FORM_ROUNDS : FORM_GATHER, h->stage_team[k]);
+    for (auto& g : ssegs[0]) { r = check_smem(h, g); if (r) return r; }
     cudaEventRecord(h->ev0, s);
+    auto launch = [&](const Seg& g, const int* work_base, int limit, int nwork_override) -> int {
+        a.work = work_base + g.begin; a.nwork = nwork_override > 0 ? nwork_override : g.end - g.begin;
+        a.nmax = g.nmax; a.nfmax = g.nfmax; a.phase_limit = limit;
+        CU(h, cudaMemsetAsync(h->counter, 0, 4, s));
+        int e = launch_relax(a, g.team, g.form, 0, s, h->num_sms, &h->last_launches);
+        if (e) return fail(h, SMR_ERR_CUDA, "relax launch: %s", cudaGetErrorString((cudaError_t)e));
+        return 0;
+    };
     if (mode == SMR_MODE_BATCHED) {
-        a.max_steps = max_steps;
-        for (auto& g : segs) {
-            a.work = h->work + g.begin; a.nwork = g.end - g.begin; a.nmax = g.nmax;
-            CU(h, cudaMemsetAsync(h->counter, 0, 4, s));
-            int e = launch_relax(a, g.team, 0, s, h->num_sms, &h->last_launches);
-            if (e) return fail(h, SMR_ERR_CUDA, "relax launch: %s", cudaGetErrorString((cudaError_t)e));
+        // stages run in order; every launch redistributes the systems still running over the GPU
+        for (int k = 0; k < nst; k++) {
+            if (sids[k].empty()) continue;
+            CU(h, cudaMemcpyAsync(h->work, sids[k].data(), sids[k].size() * 4, cudaMemcpyHostToDevice, s));
+            for (auto& g : ssegs[k]) { r = launch(g, h->work, stage_end(k), 0); if (r) return r; }
         }
     } else {
         // plain form: one launch per system per FIRE step, status read back after each step
-        a.max_steps = 1;
-        for (auto& g : segs) {
-            a.nmax = g.nmax; a.nwork = 1;
-            for (int k = g.begin; k < g.end; k++) {
-                a.work = h->work + k;
-                const int slot = ids[k];
-                for (int step = 0; step < max_steps; step++) {
-                    CU(h, cudaMemsetAsync(h->counter, 0, 4, s));
-                    int e = launch_relax(a, g.team, 0, s, h->num_sms, &h->last_launches);
-                    if (e) return fail(h, SMR_ERR_CUDA, "relax launch: %s", cudaGetErrorString((cudaError_t)e));
-                    int st = 0;
-                    CU(h, cudaMemcpyAsync(&st, &h->slots[slot].status, 4, cudaMemcpyDeviceToHost, s));
-                    CU(h, cudaStreamSynchronize(s));
-                    if (st != SMR_ST_RUNNING) break;
-                }
+        CU(h, cudaMemcpyAsync(h->work, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice, s));
+        for (int kk = 0; kk < (int)ids.size(); kk++) {
+            const int slot = ids[kk];
+            const SlotState& st = h->hs[slot];
+            std::vector<Seg> per_stage(nst);
+            for (int k = 0; k < nst; k++) {
+                std::vector<int> one{slot};
+                per_stage[k] = group_by(h, one, k == 0 ? FORM_ROUNDS : FORM_GATHER, h->stage_team[k])[0];
+                per_stage[k].begin = kk; per_stage[k].end = kk + 1;
+            }
+            for (int steps = start[slot]; steps < st.target; steps++) {
+                int k = 0;
+                while (k + 1 < nst && steps >= h->stage_start[k + 1]) k++;
+                r = launch(per_stage[k], h->work, steps + 1, 1);
+                if (r) return r;
+                int stt = 0;
+                CU(h, cudaMemcpyAsync(&stt, &h->slots[slot].status, 4, cudaMemcpyDeviceToHost, s));
+                CU(h, cudaStreamSynchronize(s));
+                if (stt != SMR_ST_RUNNING) break;
             }
         }
     }

@@ -41,38 +41,37 @@ __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(
 
 __host__ __device__ inline size_t red_bytes(int T) { return T > 32 ? size_t(T / 32) * 4 * sizeof(double) : 0; }
 
-// Shared memory of one team for systems of up to nmax atoms.
-__host__ __device__ inline size_t team_bytes(int nmax, int T) {
+// Shared memory of one team for systems of up to nmax atoms (and nfmax bonded force pieces in
+// the gather form).
+__host__ __device__ inline size_t team_bytes(int nmax, int nfmax, int T, int form) {
     size_t n = (size_t)nmax;
-    return n * 16 * 5 + n * 64 + align16(n * 4) + align16(n * 8) + red_bytes(T);
+    return n * 16 * 6 + n * 64 + align16(n * 4) + align16(n * 8) + red_bytes(T) +
+           (form == FORM_GATHER ? (size_t)nfmax * 16 : 0);
 }
 
+// Shared memory of one team: one base pointer and the capacity; every array's address is
+// computed on use (keeping ten 64-bit pointers live would cost twenty registers).
 struct Smem {
-    float4* P;   // positions (w unused)
-    float4* V;   // velocities
-    float4* F;   // forces, w = per-atom energy (reference fapos.w convention)
-    float4* Q;   // R, sqrt(E), Q, H
-    float4* PL;  // grid prefactors (Pauli, London, Q, 0) times the grid channel scales
-    float4* H;   // hneigh: 4 per atom, (unit bond vector, 1/length)
-    float* Eh;   // bond + NB part of the per-atom energy (counted twice in fapos.w)
-    short4* Ng;  // neighbour slots
-    double* red; // team reduction scratch (T > 32)
+    char* base;
+    int n;
+    __device__ __forceinline__ float4* P() const { return (float4*)base; }                         // positions
+    __device__ __forceinline__ float4* Lo() const { return (float4*)(base + (size_t)n * 16); }      // low parts of positions
+    __device__ __forceinline__ float4* V() const { return (float4*)(base + (size_t)n * 32); }       // velocities
+    __device__ __forceinline__ float4* F() const { return (float4*)(base + (size_t)n * 48); }       // forces, w = per-atom energy
+    __device__ __forceinline__ float4* Q() const { return (float4*)(base + (size_t)n * 64); }       // R, sqrt(E), Q, H
+    __device__ __forceinline__ float4* PL() const { return (float4*)(base + (size_t)n * 80); }      // grid prefactors x channel scales
+    __device__ __forceinline__ float4* H() const { return (float4*)(base + (size_t)n * 96); }       // hneigh: 4 per atom
+    __device__ __forceinline__ float* Eh() const { return (float*)(base + (size_t)n * 160); }        // bond + NB part of E_atom
+    __device__ __forceinline__ short4* Ng() const { return (short4*)(base + (size_t)n * 160 + align16((size_t)n * 4)); }
+    __device__ __forceinline__ double* red() const {
+        return (double*)(base + (size_t)n * 160 + align16((size_t)n * 4) + align16((size_t)n * 8));
+    }
+    __device__ __forceinline__ float4* Pc(int T) const {   // gather form: bonded force pieces
+        return (float4*)((char*)red() + red_bytes(T));
+    }
 };
 
-__device__ inline Smem carve(char* base, int nmax, int T) {
-    Smem s;
-    size_t n = (size_t)nmax;
-    s.P = (float4*)base; base += n * 16;
-    s.V = (float4*)base; base += n * 16;
-    s.F = (float4*)base; base += n * 16;
-    s.Q = (float4*)base; base += n * 16;
-    s.PL = (float4*)base; base += n * 16;
-    s.H = (float4*)base; base += n * 64;
-    s.Eh = (float*)base; base += align16(n * 4);
-    s.Ng = (short4*)base; base += align16(n * 8);
-    s.red = (double*)base;
-    return s;
-}
+__device__ __forceinline__ Smem carve(char* base, int nmax) { Smem s; s.base = base; s.n = nmax; return s; }
 
 template <int T> __device__ __forceinline__ void team_sync() {
     if (T == 32) __syncwarp(); else __syncthreads();
@@ -128,17 +127,29 @@ template <class Rec> __device__ __forceinline__ Rec load_rec(const Rec* p) {
 
 // ---- grid voxel loads
 template <int GDT> __device__ __forceinline__ float4 load_voxel(const void* g, size_t i);
+// Grid voxels are read through the non-coherent path without allocating in L1: the stencil
+// lines are used once per atom-step and would otherwise evict the topology records.
+__device__ __forceinline__ float4 ldg_stream(const float4* p) {
+    float4 v;
+    asm("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ uint2 ldg_stream(const uint2* p) {
+    uint2 v;
+    asm("ld.global.nc.L1::no_allocate.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "l"(p));
+    return v;
+}
 template <> __device__ __forceinline__ float4 load_voxel<GRID_F32>(const void* g, size_t i) {
-    return __ldg(reinterpret_cast<const float4*>(g) + i);
+    return ldg_stream(reinterpret_cast<const float4*>(g) + i);
 }
 template <> __device__ __forceinline__ float4 load_voxel<GRID_F16>(const void* g, size_t i) {
-    uint2 u = __ldg(reinterpret_cast<const uint2*>(g) + i);
+    uint2 u = ldg_stream(reinterpret_cast<const uint2*>(g) + i);
     float2 a = __half22float2(*reinterpret_cast<const __half2*>(&u.x));
     float2 b = __half22float2(*reinterpret_cast<const __half2*>(&u.y));
     return make_float4(a.x, a.y, b.x, b.y);
 }
 template <> __device__ __forceinline__ float4 load_voxel<GRID_BF16>(const void* g, size_t i) {
-    uint2 u = __ldg(reinterpret_cast<const uint2*>(g) + i);
+    uint2 u = ldg_stream(reinterpret_cast<const uint2*>(g) + i);
     float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.x));
     float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.y));
     return make_float4(a.x, a.y, b.x, b.y);
@@ -170,174 +181,258 @@ __device__ __forceinline__ int nb_lanes(int N, int T) {
     return best;
 }
 
+
+// ------------------------------------------------------------------ bonded terms (opencl/UFF.cl:326-795)
+// Each returns the force on every atom of the term and the term energy.
+__device__ __forceinline__ float angle_term(const Smem& S, const AngRec& rec, float3& fpi, float3& fpj, float3& fpk) {
+    const float4 qij = S.H()[rec.sl.x], qkj = S.H()[rec.sl.y];
+    const float hx = qij.x + qkj.x, hy = qij.y + qkj.y, hz = qij.z + qkj.z;
+    float c = 0.5f * (hx * hx + hy * hy + hz * hz - 2.0f);
+    c = fminf(fmaxf(c, -1.0f), 1.0f);
+    const float s = sqrtf(fmaxf(0.0f, 1.0f - c * c) + 1e-14f);
+    const float is = (s > 1e-12f) ? 1.0f / s : 0.0f;
+    const float c2x = c * c - s * s, c2y = c * s + s * c;
+    const float c3x = c2x * c - c2y * s, c3y = c2x * s + c2y * c;
+    const float4 p = rec.p;   // K*(c0, c1, c2, c3); the energy omits the c1 term, the force keeps it
+    const float E = p.x + p.z * c2x + p.w * c3x;
+    const float fm = p.y + p.z * c2y * is * 2.0f + p.w * c3y * is * 3.0f;
+    const float fi = fm * qij.w, fk = fm * qkj.w, fic = fi * c, fkc = fk * c;
+    fpi = make_float3(fic * qij.x - fi * qkj.x, fic * qij.y - fi * qkj.y, fic * qij.z - fi * qkj.z);
+    fpk = make_float3(-fk * qij.x + fkc * qkj.x, -fk * qij.y + fkc * qkj.y, -fk * qij.z + fkc * qkj.z);
+    fpj = make_float3((fk - fic) * qij.x + (fi - fkc) * qkj.x, (fk - fic) * qij.y + (fi - fkc) * qkj.y,
+                      (fk - fic) * qij.z + (fi - fkc) * qkj.z);
+    return E;
+}
+
+__device__ __forceinline__ float dihedral_term(const Smem& S, const DihRec& rec, float3& f1, float3& f2, float3& f3, float3& f4) {
+    const float4 q12 = S.H()[rec.sl.x], q32 = S.H()[rec.sl.y], q43 = S.H()[rec.sl.z];
+    const float3 n123 = make_float3(q12.y * q32.z - q12.z * q32.y, q12.z * q32.x - q12.x * q32.z, q12.x * q32.y - q12.y * q32.x);
+    const float3 n234 = make_float3(q43.y * q32.z - q43.z * q32.y, q43.z * q32.x - q43.x * q32.z, q43.x * q32.y - q43.y * q32.x);
+    const float a2 = n123.x * n123.x + n123.y * n123.y + n123.z * n123.z;
+    const float b2 = n234.x * n234.x + n234.y * n234.y + n234.z * n234.z;
+    f1 = f2 = f3 = f4 = make_float3(0.f, 0.f, 0.f);
+    if (a2 < 1e-30f || b2 < 1e-30f) return 0.f;
+    const float il2a = 1.0f / a2, il2b = 1.0f / b2, inv = sqrtf(il2a * il2b);
+    const float cx = (n123.x * n234.x + n123.y * n234.y + n123.z * n234.z) * inv;
+    const float cy = -(n123.x * q43.x + n123.y * q43.y + n123.z * q43.z) * inv;
+    float nx = cx, ny = cy;
+    const int nn = (int)rec.p.z;
+    for (int k = 1; k < nn; k++) { const float t = nx * cx - ny * cy; ny = nx * cy + ny * cx; nx = t; }
+    const float E = rec.p.x * (1.0f + rec.p.y * nx);
+    const float f = -rec.p.x * rec.p.y * rec.p.z * ny;
+    const float s1 = -f * il2a * q12.w, s4 = f * il2b * q43.w;
+    f1 = make_float3(n123.x * s1, n123.y * s1, n123.z * s1);
+    f4 = make_float3(n234.x * s4, n234.y * s4, n234.z * s4);
+    const float c123 = (q32.x * q12.x + q32.y * q12.y + q32.z * q12.z) * (q32.w / q12.w);
+    const float c432 = (q32.x * q43.x + q32.y * q43.y + q32.z * q43.z) * (q32.w / q43.w);
+    f3 = make_float3(-c123 * f1.x + (-c432 - 1.0f) * f4.x, -c123 * f1.y + (-c432 - 1.0f) * f4.y, -c123 * f1.z + (-c432 - 1.0f) * f4.z);
+    f2 = make_float3((c123 - 1.0f) * f1.x + c432 * f4.x, (c123 - 1.0f) * f1.y + c432 * f4.y, (c123 - 1.0f) * f1.z + c432 * f4.z);
+    return E;
+}
+
+__device__ __forceinline__ float inversion_term(const Smem& S, const InvRec& rec, float3& f1, float3& f2, float3& f3, float3& f4) {
+    const float4 q21 = S.H()[rec.sl.x], q31 = S.H()[rec.sl.y], q41 = S.H()[rec.sl.z];
+    float3 n = make_float3(q21.y * q31.z - q21.z * q31.y, q21.z * q31.x - q21.x * q31.z, q21.x * q31.y - q21.y * q31.x);
+    const float nn = n.x * n.x + n.y * n.y + n.z * n.z;
+    float il = 0.0f;
+    if (nn > 1e-16f) { il = rsqrtf(nn); n.x *= il; n.y *= il; n.z *= il; }
+    else n = make_float3(0.f, 0.f, 0.f);
+    float sw = -(n.x * q41.x + n.y * q41.y + n.z * q41.z);
+    sw = fminf(fmaxf(sw, -1.0f), 1.0f);
+    const float cw = sqrtf(1.0f - sw * sw);
+    const float4 p = rec.p;   // K, c0, c1, c2
+    const float E = p.x * (p.y + p.z * cw + p.w * (2.0f * cw * cw - 1.0f));
+    const float dEdw = -p.x * (p.z * sw + 2.0f * p.w * (2.0f * sw * cw));
+    const float ft = (cw > 1e-7f) ? dEdw / cw : 0.0f;
+    const float fq41 = ft * q41.w, fi123 = ft * il;
+    const float3 tq = make_float3(sw * fi123 * n.x + fi123 * q41.x, sw * fi123 * n.y + fi123 * q41.y, sw * fi123 * n.z + fi123 * q41.z);
+    f4 = make_float3(fq41 * n.x + sw * fq41 * q41.x, fq41 * n.y + sw * fq41 * q41.y, fq41 * n.z + sw * fq41 * q41.z);
+    f2 = make_float3((q31.y * tq.z - q31.z * tq.y) * q21.w, (q31.z * tq.x - q31.x * tq.z) * q21.w, (q31.x * tq.y - q31.y * tq.x) * q21.w);
+    f3 = make_float3((tq.y * q21.z - tq.z * q21.y) * q31.w, (tq.z * q21.x - tq.x * q21.z) * q31.w, (tq.x * q21.y - tq.y * q21.x) * q31.w);
+    f1 = make_float3(-(f2.x + f3.x + f4.x), -(f2.y + f3.y + f4.y), -(f2.z + f3.z + f4.z));
+    return E;
+}
+
+__device__ __forceinline__ void addf(float4& a, const float3& f, float e) { a.x += f.x; a.y += f.y; a.z += f.z; a.w += e; }
+
+// Energy accumulators of the evaluation-only launch (bond, angle, dihedral, inversion, NB, grid).
+template <bool EVAL> struct EAcc { __device__ void add(int, double) {} };
+template <> struct EAcc<true> {
+    double e[6] = {0, 0, 0, 0, 0, 0};
+    __device__ void add(int k, double v) { e[k] += v; }
+};
+
 // ------------------------------------------------------------------ force evaluation
-template <int T, int GDT, bool EVAL>
-__device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev& tp, int N, int rank, double* eacc) {
-    // A: bonds and hneigh, one atom per rank
+template <int T, int GDT, bool EVAL, int FORM>
+__device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* __restrict__ tpp, int N, int rank, EAcc<EVAL>& acc) {
+#define TP(f) __ldg(&tpp->f)
+    // A: bonds and hneigh, one atom per rank (opencl/UFF.cl:141-322)
     for (int i = rank; i < N; i += T) {
-        const float4 pi = S.P[i];
-        const short4 ng = S.Ng[i];
-        const float4 bk = __ldg(a.bk + tp.atom_off + i), bl = __ldg(a.bl + tp.atom_off + i);
+        const float4 pi = S.P()[i], li = S.Lo()[i];
+        const short4 ng = S.Ng()[i];
+        const float4 bk = __ldg(a.bk + TP(atom_off) + i), bl = __ldg(a.bl + TP(atom_off) + i);
         float fx = 0.f, fy = 0.f, fz = 0.f, E = 0.f;
 #pragma unroll
         for (int s = 0; s < 4; s++) {
             const int g = comp(ng, s);
-            if (g < 0) { S.H[4 * i + s] = make_float4(0.f, 0.f, 0.f, 1e6f); continue; }
-            const float4 pj = S.P[g];
-            const float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
+            if (g < 0) { S.H()[4 * i + s] = make_float4(0.f, 0.f, 0.f, 1e6f); continue; }
+            const float4 pj = S.P()[g], lj = S.Lo()[g];
+            // difference of the compensated positions: its error is relative to the bond length,
+            // not to the absolute coordinate (float positions alone would put ~1e-6 A of rounding
+            // into every stiff bond and make the force field rough at the 1e-4 eV/A level)
+            const float dx = (pj.x - pi.x) + (lj.x - li.x), dy = (pj.y - pi.y) + (lj.y - li.y), dz = (pj.z - pi.z) + (lj.z - li.z);
             const float l2 = fmaxf(dx * dx + dy * dy + dz * dz, 1e-16f);
             const float l = sqrtf(l2), il = 1.0f / l;
             const float hx = dx * il, hy = dy * il, hz = dz * il;
-            S.H[4 * i + s] = make_float4(hx, hy, hz, il);
+            S.H()[4 * i + s] = make_float4(hx, hy, hz, il);
             const float k = comp(bk, s), dl = l - comp(bl, s), fr = 2.0f * k * dl;
             fx += hx * fr; fy += hy * fr; fz += hz * fr;
             E += k * dl * dl;
         }
-        S.F[i] = make_float4(fx, fy, fz, E);
-        S.Eh[i] = E;
-        if (EVAL) eacc[0] += 0.5 * (double)E;
+        S.F()[i] = make_float4(fx, fy, fz, E);
+        S.Eh()[i] = E;
+        acc.add(0, 0.5 * (double)E);
     }
     team_sync<T>();
 
-    // B1: angles (Fourier form via complex powers)
-    for (int r = 0; r < tp.ang_rounds; r++) {
-        const AngRec rec = load_rec(a.angs + tp.ang_off + (size_t)r * T + rank);
-        const bool ok = rec.at.x >= 0;
-        float3 fpi = {0, 0, 0}, fpj = {0, 0, 0}, fpk = {0, 0, 0};
-        float E = 0.f;
-        if (ok) {
-            const float4 qij = S.H[rec.sl.x], qkj = S.H[rec.sl.y];
-            const float hx = qij.x + qkj.x, hy = qij.y + qkj.y, hz = qij.z + qkj.z;
-            float c = 0.5f * (hx * hx + hy * hy + hz * hz - 2.0f);
-            c = fminf(fmaxf(c, -1.0f), 1.0f);
-            const float s = sqrtf(fmaxf(0.0f, 1.0f - c * c) + 1e-14f);
-            const float is = (s > 1e-12f) ? 1.0f / s : 0.0f;
-            const float c2x = c * c - s * s, c2y = c * s + s * c;
-            const float c3x = c2x * c - c2y * s, c3y = c2x * s + c2y * c;
-            const float4 p = rec.p;   // K*(c0, c1, c2, c3)
-            E = p.x + p.z * c2x + p.w * c3x;
-            const float fm = p.y + p.z * c2y * is * 2.0f + p.w * c3y * is * 3.0f;
-            const float fi = fm * qij.w, fk = fm * qkj.w, fic = fi * c, fkc = fk * c;
-            fpi = make_float3(fic * qij.x - fi * qkj.x, fic * qij.y - fi * qkj.y, fic * qij.z - fi * qkj.z);
-            fpk = make_float3(-fk * qij.x + fkc * qkj.x, -fk * qij.y + fkc * qkj.y, -fk * qij.z + fkc * qkj.z);
-            fpj = make_float3((fk - fic) * qij.x + (fi - fkc) * qkj.x, (fk - fic) * qij.y + (fi - fkc) * qkj.y,
-                              (fk - fic) * qij.z + (fi - fkc) * qkj.z);
-            if (EVAL) eacc[1] += (double)E;
+    if (FORM == FORM_ROUNDS) {
+        // B (rounds): in one round the atoms of each role are distinct, so each role's pieces
+        // are added with plain read-modify-writes separated by team syncs
+        for (int r = 0; r < TP(ang_rounds); r++) {
+            const AngRec rec = load_rec(a.angs + TP(ang_off) + (size_t)r * T + rank);
+            const bool ok = rec.at.x >= 0;
+            float3 f1, f2, f3;
+            float E = 0.f;
+            if (ok) { E = angle_term(S, rec, f1, f2, f3); acc.add(1, (double)E); }
+            const float e3 = E / 3.0f;
+            if (ok) addf(S.F()[rec.at.x], f1, e3);
+            team_sync<T>();
+            if (ok) addf(S.F()[rec.at.y], f2, e3);
+            team_sync<T>();
+            if (ok) addf(S.F()[rec.at.z], f3, e3);
+            team_sync<T>();
         }
-        const float e3 = E / 3.0f;
-        if (ok) add4(S.F[rec.at.x], fpi.x, fpi.y, fpi.z, e3);
-        team_sync<T>();
-        if (ok) add4(S.F[rec.at.y], fpj.x, fpj.y, fpj.z, e3);
-        team_sync<T>();
-        if (ok) add4(S.F[rec.at.z], fpk.x, fpk.y, fpk.z, e3);
-        team_sync<T>();
-    }
-
-    // B2: dihedrals
-    for (int r = 0; r < tp.dih_rounds; r++) {
-        const DihRec rec = load_rec(a.dihs + tp.dih_off + (size_t)r * T + rank);
-        const bool ok = rec.at.x >= 0;
-        float3 f1 = {0, 0, 0}, f2 = {0, 0, 0}, f3 = {0, 0, 0}, f4 = {0, 0, 0};
-        float E = 0.f;
-        if (ok) {
-            const float4 q12 = S.H[rec.sl.x], q32 = S.H[rec.sl.y], q43 = S.H[rec.sl.z];
-            const float3 n123 = make_float3(q12.y * q32.z - q12.z * q32.y, q12.z * q32.x - q12.x * q32.z, q12.x * q32.y - q12.y * q32.x);
-            const float3 n234 = make_float3(q43.y * q32.z - q43.z * q32.y, q43.z * q32.x - q43.x * q32.z, q43.x * q32.y - q43.y * q32.x);
-            const float a2 = n123.x * n123.x + n123.y * n123.y + n123.z * n123.z;
-            const float b2 = n234.x * n234.x + n234.y * n234.y + n234.z * n234.z;
-            if (!(a2 < 1e-30f || b2 < 1e-30f)) {
-                const float il2a = 1.0f / a2, il2b = 1.0f / b2, inv = sqrtf(il2a * il2b);
-                const float cx = (n123.x * n234.x + n123.y * n234.y + n123.z * n234.z) * inv;
-                const float cy = -(n123.x * q43.x + n123.y * q43.y + n123.z * q43.z) * inv;
-                float nx = cx, ny = cy;
-                const int nn = (int)rec.p.z;
-                for (int k = 1; k < nn; k++) { const float t = nx * cx - ny * cy; ny = nx * cy + ny * cx; nx = t; }
-                E = rec.p.x * (1.0f + rec.p.y * nx);
-                const float f = -rec.p.x * rec.p.y * rec.p.z * ny;
-                const float s1 = -f * il2a * q12.w, s4 = f * il2b * q43.w;
-                f1 = make_float3(n123.x * s1, n123.y * s1, n123.z * s1);
-                f4 = make_float3(n234.x * s4, n234.y * s4, n234.z * s4);
-                const float c123 = (q32.x * q12.x + q32.y * q12.y + q32.z * q12.z) * (q32.w / q12.w);
-                const float c432 = (q32.x * q43.x + q32.y * q43.y + q32.z * q43.z) * (q32.w / q43.w);
-                f3 = make_float3(-c123 * f1.x + (-c432 - 1.0f) * f4.x, -c123 * f1.y + (-c432 - 1.0f) * f4.y, -c123 * f1.z + (-c432 - 1.0f) * f4.z);
-                f2 = make_float3((c123 - 1.0f) * f1.x + c432 * f4.x, (c123 - 1.0f) * f1.y + c432 * f4.y, (c123 - 1.0f) * f1.z + c432 * f4.z);
+        for (int r = 0; r < TP(dih_rounds); r++) {
+            const DihRec rec = load_rec(a.dihs + TP(dih_off) + (size_t)r * T + rank);
+            const bool ok = rec.at.x >= 0;
+            float3 f1, f2, f3, f4;
+            float E = 0.f;
+            if (ok) { E = dihedral_term(S, rec, f1, f2, f3, f4); acc.add(2, (double)E); }
+            const float e4 = 0.25f * E;
+            if (ok) addf(S.F()[rec.at.x], f1, e4);
+            team_sync<T>();
+            if (ok) addf(S.F()[rec.at.y], f2, e4);
+            team_sync<T>();
+            if (ok) addf(S.F()[rec.at.z], f3, e4);
+            team_sync<T>();
+            if (ok) addf(S.F()[rec.at.w], f4, e4);
+            team_sync<T>();
+        }
+        for (int r = 0; r < TP(inv_rounds); r++) {
+            const InvRec rec = load_rec(a.invs + TP(inv_off) + (size_t)r * T + rank);
+            const bool ok = rec.at.x >= 0;
+            float3 f1, f2, f3, f4;
+            float E = 0.f;
+            if (ok) { E = inversion_term(S, rec, f1, f2, f3, f4); acc.add(3, (double)E); }
+            const float e4 = 0.25f * E;
+            if (ok) addf(S.F()[rec.at.x], f1, e4);
+            team_sync<T>();
+            if (ok) addf(S.F()[rec.at.y], f2, e4);
+            team_sync<T>();
+            if (ok) addf(S.F()[rec.at.z], f3, e4);
+            team_sync<T>();
+            if (ok) addf(S.F()[rec.at.w], f4, e4);
+            team_sync<T>();
+        }
+    } else {
+        // B (gather): all terms at once, each writing its pieces to its own slots (the reference's
+        // fint array, opencl/UFF.cl:801-880), then every atom sums its pieces in a fixed order
+        const int na = TP(nang), nd = TP(ndih), ni = TP(ninv);
+        for (int t = rank; t < na + nd + ni; t += T) {
+            float3 f1, f2, f3, f4;
+            if (t < na) {
+                const AngRec rec = load_rec(a.angs + TP(fang_off) + t);
+                const float E = angle_term(S, rec, f1, f2, f3);
+                acc.add(1, (double)E);
+                const float e3 = E / 3.0f;
+                float4* P = S.Pc(T) + 3 * t;
+                P[0] = make_float4(f1.x, f1.y, f1.z, e3); P[1] = make_float4(f2.x, f2.y, f2.z, e3); P[2] = make_float4(f3.x, f3.y, f3.z, e3);
+            } else if (t < na + nd) {
+                const int u = t - na;
+                const DihRec rec = load_rec(a.dihs + TP(fdih_off) + u);
+                const float E = dihedral_term(S, rec, f1, f2, f3, f4);
+                acc.add(2, (double)E);
+                const float e4 = 0.25f * E;
+                float4* P = S.Pc(T) + 3 * na + 4 * u;
+                P[0] = make_float4(f1.x, f1.y, f1.z, e4); P[1] = make_float4(f2.x, f2.y, f2.z, e4);
+                P[2] = make_float4(f3.x, f3.y, f3.z, e4); P[3] = make_float4(f4.x, f4.y, f4.z, e4);
+            } else {
+                const int u = t - na - nd;
+                const InvRec rec = load_rec(a.invs + TP(finv_off) + u);
+                const float E = inversion_term(S, rec, f1, f2, f3, f4);
+                acc.add(3, (double)E);
+                const float e4 = 0.25f * E;
+                float4* P = S.Pc(T) + 3 * na + 4 * nd + 4 * u;
+                P[0] = make_float4(f1.x, f1.y, f1.z, e4); P[1] = make_float4(f2.x, f2.y, f2.z, e4);
+                P[2] = make_float4(f3.x, f3.y, f3.z, e4); P[3] = make_float4(f4.x, f4.y, f4.z, e4);
             }
-            if (EVAL) eacc[2] += (double)E;
         }
-        const float e4 = 0.25f * E;
-        if (ok) add4(S.F[rec.at.x], f1.x, f1.y, f1.z, e4);
         team_sync<T>();
-        if (ok) add4(S.F[rec.at.y], f2.x, f2.y, f2.z, e4);
-        team_sync<T>();
-        if (ok) add4(S.F[rec.at.z], f3.x, f3.y, f3.z, e4);
-        team_sync<T>();
-        if (ok) add4(S.F[rec.at.w], f4.x, f4.y, f4.z, e4);
+        const int c = rank & 3;
+        for (int i0 = 0; i0 < N; i0 += T / 4) {
+            const int i = i0 + (rank >> 2);
+            float4 s4 = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (i < N) {
+                const int2 se = __ldg(a.a2f + TP(atom_off) + i);
+                for (int k = c; k < se.y; k += 4) {
+                    const float4 v = S.Pc(T)[__ldg(a.a2f_idx + TP(a2f_off) + se.x + k)];
+                    s4.x += v.x; s4.y += v.y; s4.z += v.z; s4.w += v.w;
+                }
+            }
+            for (int o = 1; o < 4; o <<= 1) {
+                s4.x += __shfl_xor_sync(FULL, s4.x, o); s4.y += __shfl_xor_sync(FULL, s4.y, o);
+                s4.z += __shfl_xor_sync(FULL, s4.z, o); s4.w += __shfl_xor_sync(FULL, s4.w, o);
+            }
+            if (c == 0 && i < N) add4(S.F()[i], s4.x, s4.y, s4.z, s4.w);
+        }
         team_sync<T>();
     }
 
-    // B3: inversions
-    for (int r = 0; r < tp.inv_rounds; r++) {
-        const InvRec rec = load_rec(a.invs + tp.inv_off + (size_t)r * T + rank);
-        const bool ok = rec.at.x >= 0;
-        float3 f1 = {0, 0, 0}, f2 = {0, 0, 0}, f3 = {0, 0, 0}, f4 = {0, 0, 0};
-        float E = 0.f;
-        if (ok) {
-            const float4 q21 = S.H[rec.sl.x], q31 = S.H[rec.sl.y], q41 = S.H[rec.sl.z];
-            float3 n = make_float3(q21.y * q31.z - q21.z * q31.y, q21.z * q31.x - q21.x * q31.z, q21.x * q31.y - q21.y * q31.x);
-            const float nn = n.x * n.x + n.y * n.y + n.z * n.z;
-            float il = 0.0f;
-            if (nn > 1e-16f) { il = rsqrtf(nn); n.x *= il; n.y *= il; n.z *= il; }
-            else n = make_float3(0.f, 0.f, 0.f);
-            float sw = -(n.x * q41.x + n.y * q41.y + n.z * q41.z);
-            sw = fminf(fmaxf(sw, -1.0f), 1.0f);
-            const float cw = sqrtf(1.0f - sw * sw);
-            const float4 p = rec.p;   // K, c0, c1, c2
-            E = p.x * (p.y + p.z * cw + p.w * (2.0f * cw * cw - 1.0f));
-            const float dEdw = -p.x * (p.z * sw + 2.0f * p.w * (2.0f * sw * cw));
-            const float ft = (cw > 1e-7f) ? dEdw / cw : 0.0f;
-            const float fq41 = ft * q41.w, fi123 = ft * il;
-            const float3 tq = make_float3(sw * fi123 * n.x + fi123 * q41.x, sw * fi123 * n.y + fi123 * q41.y, sw * fi123 * n.z + fi123 * q41.z);
-            f4 = make_float3(fq41 * n.x + sw * fq41 * q41.x, fq41 * n.y + sw * fq41 * q41.y, fq41 * n.z + sw * fq41 * q41.z);
-            f2 = make_float3((q31.y * tq.z - q31.z * tq.y) * q21.w, (q31.z * tq.x - q31.x * tq.z) * q21.w, (q31.x * tq.y - q31.y * tq.x) * q21.w);
-            f3 = make_float3((tq.y * q21.z - tq.z * q21.y) * q31.w, (tq.z * q21.x - tq.x * q21.z) * q31.w, (tq.x * q21.y - tq.y * q21.x) * q31.w);
-            f1 = make_float3(-(f2.x + f3.x + f4.x), -(f2.y + f3.y + f4.y), -(f2.z + f3.z + f4.z));
-            if (EVAL) eacc[3] += (double)E;
-        }
-        const float e4 = 0.25f * E;
-        if (ok) add4(S.F[rec.at.x], f1.x, f1.y, f1.z, e4);
-        team_sync<T>();
-        if (ok) add4(S.F[rec.at.y], f2.x, f2.y, f2.z, e4);
-        team_sync<T>();
-        if (ok) add4(S.F[rec.at.z], f3.x, f3.y, f3.z, e4);
-        team_sync<T>();
-        if (ok) add4(S.F[rec.at.w], f4.x, f4.y, f4.z, e4);
-        team_sync<T>();
-    }
-
-    // C: intramolecular LJ + damped Coulomb, all pairs except bonded (1-2) neighbours
+    // C: intramolecular LJ + damped Coulomb over all pairs except bonded (1-2) neighbours
+    // (opencl/UFF.cl:57-95, 1595-1665).  Excluded pairs are evaluated at r2 = 1 and masked out,
+    // so the partner loop has no branch and independent pairs overlap.
     {
         const int L = nb_lanes(N, T), G = T / L;
         const int c = rank & (L - 1);
+        const bool small = N <= 64;
         for (int i0 = 0; i0 < N; i0 += G) {
             const int i = i0 + rank / L;
             float fx = 0.f, fy = 0.f, fz = 0.f, E = 0.f;
             if (i < N) {
-                const float4 pi = S.P[i], qi = S.Q[i];
-                const short4 ng = S.Ng[i];
+                const float4 pi = S.P()[i], qi = S.Q()[i], li = S.Lo()[i];
+                const short4 ng = S.Ng()[i];
+                unsigned long long ex = 1ull << (i & 63);
+                if (ng.x >= 0) ex |= 1ull << (ng.x & 63);
+                if (ng.y >= 0) ex |= 1ull << (ng.y & 63);
+                if (ng.z >= 0) ex |= 1ull << (ng.z & 63);
+                if (ng.w >= 0) ex |= 1ull << (ng.w & 63);
+#pragma unroll 4
                 for (int j = c; j < N; j += L) {
-                    if (j == i || j == ng.x || j == ng.y || j == ng.z || j == ng.w) continue;
-                    const float4 pj = S.P[j];
-                    const float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
-                    const float r2 = dx * dx + dy * dy + dz * dz;
-                    if (r2 > a.rc2) continue;
-                    const float4 qj = S.Q[j];
+                    const float4 pj = S.P()[j], lj = S.Lo()[j];
+                    const float4 qj = S.Q()[j];
+                    const float dx = (pj.x - pi.x) + (lj.x - li.x), dy = (pj.y - pi.y) + (lj.y - li.y), dz = (pj.z - pi.z) + (lj.z - li.z);
+                    float r2 = dx * dx + dy * dy + dz * dz;
+                    const bool skip = (small ? (bool)((ex >> j) & 1ull)
+                                             : (j == i || j == ng.x || j == ng.y || j == ng.z || j == ng.w)) || r2 > a.rc2;
+                    r2 = skip ? 1.0f : r2;
                     const float R0 = qi.x + qj.x, E0 = qi.y * qj.y, Q = qi.z * qj.z;
                     const float rs = rsqrtf(r2 + a.R2damp);          // 1/sqrt(r^2 + Rdamp^2)
                     const float Ec = kCoulomb * Q * rs;
                     const float ir2 = 1.0f / r2;
                     const float u2 = R0 * R0 * ir2, u6 = u2 * u2 * u2, vdW = u6 * E0;
-                    E += (u6 - 2.0f) * vdW + Ec;
-                    const float fr = -12.0f * (u6 - 1.0f) * vdW * ir2 - Ec * (rs * rs);
+                    const float w = skip ? 0.0f : 1.0f;
+                    E += w * ((u6 - 2.0f) * vdW + Ec);
+                    const float fr = w * (-12.0f * (u6 - 1.0f) * vdW * ir2 - Ec * (rs * rs));
                     fx += dx * fr; fy += dy * fr; fz += dz * fr;
                 }
             }
@@ -346,9 +441,9 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev& t
                 fz += __shfl_xor_sync(FULL, fz, o); E += __shfl_xor_sync(FULL, E, o);
             }
             if (c == 0 && i < N) {
-                add4(S.F[i], fx, fy, fz, E);
-                S.Eh[i] += E;
-                if (EVAL) eacc[4] += 0.5 * (double)E;
+                add4(S.F()[i], fx, fy, fz, E);
+                S.Eh()[i] += E;
+                acc.add(4, 0.5 * (double)E);
             }
         }
     }
@@ -362,10 +457,10 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev& t
             const int i = i0 + (rank >> 2);
             float e = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
             if (i < N) {
-                const float4 p = S.P[i];
-                const float ux = (p.x - g.p0[0]) * g.inv_step[0];
-                const float uy = (p.y - g.p0[1]) * g.inv_step[1];
-                const float uz = (p.z - g.p0[2]) * g.inv_step[2];
+                const float4 p = S.P()[i], lp = S.Lo()[i];
+                const float ux = ((p.x - g.p0[0]) + lp.x) * g.inv_step[0];
+                const float uy = ((p.y - g.p0[1]) + lp.y) * g.inv_step[1];
+                const float uz = ((p.z - g.p0[2]) + lp.z) * g.inv_step[2];
                 int ix = (int)ux, iy = (int)uy;
                 const int iz = (int)uz;
                 if (ux < 0) ix--;
@@ -374,7 +469,7 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev& t
                     const float tx = ux - ix, ty = uy - iy, tz = uz - iz;
                     float bx[4], dxw[4], by[4], dyw[4], bz[4], dzw[4];
                     bspline(tx, bx, dxw); bspline(ty, by, dyw); bspline(tz, bz, dzw);
-                    const float4 PL = S.PL[i];
+                    const float4 PL = S.PL()[i];
                     const int xg = imod(ix - 1 + xa, g.nx);
                     const int y0 = imod(iy - 1, g.ny);
                     float sE = 0.f, sDy = 0.f, sDz = 0.f;
@@ -402,83 +497,92 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev& t
             e += __shfl_xor_sync(FULL, e, 2); gx += __shfl_xor_sync(FULL, gx, 2);
             gy += __shfl_xor_sync(FULL, gy, 2); gz += __shfl_xor_sync(FULL, gz, 2);
             if (xa == 0 && i < N) {
-                add4(S.F[i], -gx * g.inv_step[0], -gy * g.inv_step[1], -gz * g.inv_step[2], e);
-                if (EVAL) eacc[5] += (double)e;
+                add4(S.F()[i], -gx * g.inv_step[0], -gy * g.inv_step[1], -gz * g.inv_step[2], e);
+                acc.add(5, (double)e);
             }
         }
     }
     team_sync<T>();
 }
+#undef TP
 
 // ------------------------------------------------------------------ one system
-template <int T, int GDT, bool EVAL>
+template <int T, int GDT, bool EVAL, int FORM>
 __device__ void run_system(const KernelArgs& a, const Smem& S, int w, int rank) {
     const int slot = a.work[w];
     const SlotState st = a.slots[slot];
-    const TopoDev tp = a.topos[st.topo];
-    const int N = st.natoms;
     // a slot with dt < 0 has not started FIRE yet: zero velocities, dt0, alpha0
     const bool fresh = !EVAL && st.dt < 0.0;
+    int steps = fresh ? 0 : st.steps;
+    int nsteps = 0;
+    if (!EVAL) {
+        nsteps = min(st.target, a.phase_limit) - steps;
+        if (a.step_budget > 0) nsteps = min(nsteps, a.step_budget - steps);
+        if (st.status != 0 || nsteps <= 0) return;          // nothing to do in this launch
+    }
+    const TopoDev* tpp = a.topos + st.topo;
+    const int tp_atom_off = __ldg(&tpp->atom_off);
+    const int N = st.natoms;
     for (int i = rank; i < N; i += T) {
-        S.P[i] = a.pos[st.atom_off + i];
-        S.V[i] = (EVAL || fresh) ? make_float4(0.f, 0.f, 0.f, 0.f) : a.vel[st.atom_off + i];
-        const float4 q = __ldg(a.req + tp.atom_off + i);
-        S.Q[i] = q;
-        S.Ng[i] = a.neigh[tp.atom_off + i];
+        S.P()[i] = a.pos[st.atom_off + i];
+        S.Lo()[i] = (EVAL || fresh) ? make_float4(0.f, 0.f, 0.f, 0.f) : a.plo[st.atom_off + i];
+        S.V()[i] = (EVAL || fresh) ? make_float4(0.f, 0.f, 0.f, 0.f) : a.vel[st.atom_off + i];
+        const float4 q = __ldg(a.req + tp_atom_off + i);
+        S.Q()[i] = q;
+        S.Ng()[i] = a.neigh[tp_atom_off + i];
         const float ej = expf(a.alpha_morse * q.x);
-        S.PL[i] = make_float4(ej * ej * q.y * a.grid.scale[0], ej * q.y * a.grid.scale[1], q.z * a.grid.scale[2], 0.f);
+        S.PL()[i] = make_float4(ej * ej * q.y * a.grid.scale[0], ej * q.y * a.grid.scale[1], q.z * a.grid.scale[2], 0.f);
     }
     team_sync<T>();
 
-    double eacc[6] = {0, 0, 0, 0, 0, 0};
+    EAcc<EVAL> acc;
     if (EVAL) {
-        eval_forces<T, GDT, true>(a, S, tp, N, rank, eacc);
-        for (int i = rank; i < N; i += T) a.force[st.atom_off + i] = S.F[i];
-        double tot = 0;
-        for (int k = 0; k < 6; k++) { eacc[k] = team_sum<T>(eacc[k], S.red, rank); tot += eacc[k]; }
-        if (rank == 0) {
-            double* out = a.ecomp + (size_t)w * 8;
-            out[0] = tot;
-            for (int k = 0; k < 6; k++) out[1 + k] = eacc[k];
-            out[7] = 0.0;
+        eval_forces<T, GDT, EVAL, FORM>(a, S, tpp, N, rank, acc);
+        for (int i = rank; i < N; i += T) a.force[st.atom_off + i] = S.F()[i];
+        if constexpr (EVAL) {
+            double tot = 0, e[6];
+            for (int k = 0; k < 6; k++) { e[k] = team_sum<T>(acc.e[k], S.red(), rank); tot += e[k]; }
+            if (rank == 0) {
+                double* out = a.ecomp + (size_t)w * 8;
+                out[0] = tot;
+                for (int k = 0; k < 6; k++) out[1 + k] = e[k];
+                out[7] = 0.0;
+            }
         }
         team_sync<T>();
         return;
     }
 
     double dt = fresh ? a.fire.dt0 : st.dt, alpha = fresh ? a.fire.alpha0 : st.alpha;
-    int npos = fresh ? 0 : st.npos, steps = fresh ? 0 : st.steps, status = st.status;
+    int npos = fresh ? 0 : st.npos, status = st.status;
     float fmax = st.fmax;
-    int nsteps = a.max_steps;
-    if (a.step_budget > 0) nsteps = min(nsteps, a.step_budget - steps);
-    if (status != 0) nsteps = 0;
     const float flim = (float)a.fire.flimit, flim2 = flim * flim;
     int ran = 0;
     for (int it = 0; it < nsteps; it++) {
-        eval_forces<T, GDT, false>(a, S, tp, N, rank, eacc);
+        eval_forces<T, GDT, EVAL, FORM>(a, S, tpp, N, rank, acc);
         ran = 1;
         const double dt_old = dt;
         const float dtf = (float)dt_old;
         double vf = 0.0, vv = 0.0, ff = 0.0;
         float f2m = 0.f;
         for (int i = rank; i < N; i += T) {
-            float4 f = S.F[i];
+            float4 f = S.F()[i];
             float f2 = f.x * f.x + f.y * f.y + f.z * f.z;
             if (flim > 0.f && f2 > flim2) {
                 const float s = flim / sqrtf(f2);
                 f.x *= s; f.y *= s; f.z *= s;
-                S.F[i] = f;
+                S.F()[i] = f;
                 f2 = f.x * f.x + f.y * f.y + f.z * f.z;
             }
             f2m = fmaxf(f2m, f2);
             ff += (double)f2;
-            float4 v = S.V[i];
+            float4 v = S.V()[i];
             v.x += f.x * dtf; v.y += f.y * dtf; v.z += f.z * dtf;
-            S.V[i] = v;
+            S.V()[i] = v;
             vf += (double)(v.x * f.x + v.y * f.y + v.z * f.z);
             vv += (double)(v.x * v.x + v.y * v.y + v.z * v.z);
         }
-        team_reduce4<T>(vf, vv, ff, f2m, S.red, rank);
+        team_reduce4<T>(vf, vv, ff, f2m, S.red(), rank);
         const bool mix = vf > 0.0 && ff > 1e-30 && vv > 1e-30;
         float cv = 0.f, cf = 0.f;
         if (mix) {
@@ -490,17 +594,23 @@ __device__ void run_system(const KernelArgs& a, const Smem& S, int w, int rank) 
             npos = 0; dt *= a.fire.f_dec; alpha = a.fire.alpha0;
         }
         for (int i = rank; i < N; i += T) {
-            float4 v = S.V[i];
+            float4 v = S.V()[i];
             if (mix) {
-                const float4 f = S.F[i];
+                const float4 f = S.F()[i];
                 v.x = v.x * cv + f.x * cf; v.y = v.y * cv + f.y * cf; v.z = v.z * cv + f.z * cf;
             } else {
                 v = make_float4(0.f, 0.f, 0.f, 0.f);
             }
-            S.V[i] = v;
-            float4 p = S.P[i];
-            p.x += v.x * dtf; p.y += v.y * dtf; p.z += v.z * dtf;
-            S.P[i] = p;
+            S.V()[i] = v;
+            // x += v dt with the rounding error of every move carried in Lo (Fast2Sum): late FIRE
+            // moves are ~1e-6 A, the size of one float ulp at 20 A, and would otherwise be lost
+            float4 p = S.P()[i], lo = S.Lo()[i];
+            float y, t;
+            y = v.x * dtf + lo.x; t = p.x + y; lo.x = y - (t - p.x); p.x = t;
+            y = v.y * dtf + lo.y; t = p.y + y; lo.y = y - (t - p.y); p.y = t;
+            y = v.z * dtf + lo.z; t = p.z + y; lo.z = y - (t - p.z); p.z = t;
+            S.P()[i] = p;
+            S.Lo()[i] = lo;
         }
         steps++;
         fmax = sqrtf(f2m);
@@ -512,13 +622,14 @@ __device__ void run_system(const KernelArgs& a, const Smem& S, int w, int rank) 
     double energy = st.energy;
     if (ran) {
         double e = 0.0;
-        for (int i = rank; i < N; i += T) e += (double)S.F[i].w - 0.5 * (double)S.Eh[i];
-        energy = team_sum<T>(e, S.red, rank);
+        for (int i = rank; i < N; i += T) e += (double)S.F()[i].w - 0.5 * (double)S.Eh()[i];
+        energy = team_sum<T>(e, S.red(), rank);
     }
     for (int i = rank; i < N; i += T) {
-        a.pos[st.atom_off + i] = S.P[i];
-        a.vel[st.atom_off + i] = S.V[i];
-        if (ran) a.force[st.atom_off + i] = S.F[i];
+        a.pos[st.atom_off + i] = S.P()[i];
+        a.plo[st.atom_off + i] = S.Lo()[i];
+        a.vel[st.atom_off + i] = S.V()[i];
+        if (ran) a.force[st.atom_off + i] = S.F()[i];
     }
     if (rank == 0) {
         SlotState& o = a.slots[slot];
@@ -528,13 +639,13 @@ __device__ void run_system(const KernelArgs& a, const Smem& S, int w, int rank) 
     team_sync<T>();
 }
 
-template <int T, int GDT, bool EVAL>
-__global__ void __launch_bounds__(T == 32 ? 128 : T)
+template <int T, int GDT, bool EVAL, int FORM>
+__global__ void __launch_bounds__(T == 32 ? 128 : T, T == 32 ? 7 : 1)
 relax_kernel(const KernelArgs a) {
     extern __shared__ __align__(16) char smem[];
     const int team = (T == 32) ? (threadIdx.x >> 5) : 0;
     const int rank = (T == 32) ? (threadIdx.x & 31) : threadIdx.x;
-    const Smem S = carve(smem + (size_t)team * team_bytes(a.nmax, T), a.nmax, T);
+    const Smem S = carve(smem + (size_t)team * team_bytes(a.nmax, a.nfmax, T, FORM), a.nmax);
     __shared__ int s_w;
     for (;;) {
         int w;
@@ -548,16 +659,16 @@ relax_kernel(const KernelArgs a) {
             __syncthreads();
         }
         if (w >= a.nwork) break;
-        run_system<T, GDT, EVAL>(a, S, w, rank);
+        run_system<T, GDT, EVAL, FORM>(a, S, w, rank);
     }
 }
 
-template <int T, int GDT, bool EVAL>
+template <int T, int GDT, bool EVAL, int FORM>
 int launch_t(const KernelArgs& a, cudaStream_t s, int num_sms) {
     const int tpb = (T == 32) ? 4 : 1;           // teams per block
     const int block = T * tpb;
-    const size_t smem = (size_t)tpb * team_bytes(a.nmax, T);
-    auto kern = relax_kernel<T, GDT, EVAL>;
+    const size_t smem = (size_t)tpb * team_bytes(a.nmax, a.nfmax, T, FORM);
+    auto kern = relax_kernel<T, GDT, EVAL, FORM>;
     static std::map<size_t, int> occ_cache;
     int occ;
     auto it = occ_cache.find(smem);
@@ -581,21 +692,31 @@ int launch_t(const KernelArgs& a, cudaStream_t s, int num_sms) {
     return (int)cudaGetLastError();
 }
 
-template <int GDT, bool EVAL>
-int launch_gdt(const KernelArgs& a, int team, cudaStream_t s, int num_sms) {
+template <int GDT, bool EVAL, int FORM>
+int launch_team(const KernelArgs& a, int team, cudaStream_t s, int num_sms) {
     switch (team) {
-        case 32: return launch_t<32, GDT, EVAL>(a, s, num_sms);
-        case 64: return launch_t<64, GDT, EVAL>(a, s, num_sms);
-        case 128: return launch_t<128, GDT, EVAL>(a, s, num_sms);
-        case 256: return launch_t<256, GDT, EVAL>(a, s, num_sms);
-        case 512: return launch_t<512, GDT, EVAL>(a, s, num_sms);
+        case 32: return launch_t<32, GDT, EVAL, FORM>(a, s, num_sms);
+        case 64: return launch_t<64, GDT, EVAL, FORM>(a, s, num_sms);
+        case 128: return launch_t<128, GDT, EVAL, FORM>(a, s, num_sms);
+        case 256: return launch_t<256, GDT, EVAL, FORM>(a, s, num_sms);
+        case 512: return launch_t<512, GDT, EVAL, FORM>(a, s, num_sms);
     }
     return (int)cudaErrorInvalidValue;
 }
 
+template <bool EVAL, int FORM>
+int launch_dtype(const KernelArgs& a, int team, cudaStream_t s, int num_sms) {
+    const int gdt = a.has_grid ? a.grid.dtype : GRID_F32;
+    if (gdt == GRID_F16) return launch_team<GRID_F16, EVAL, FORM>(a, team, s, num_sms);
+    if (gdt == GRID_BF16) return launch_team<GRID_BF16, EVAL, FORM>(a, team, s, num_sms);
+    return launch_team<GRID_F32, EVAL, FORM>(a, team, s, num_sms);
+}
+
 }  // namespace
 
-size_t team_smem_bytes(int nmax) { return team_bytes(nmax, 512); }
+size_t team_smem_bytes(int nmax, int nfmax, int team, int form) {
+    return team_bytes(nmax, nfmax, team, form) * (team == 32 ? 4 : 1);
+}
 
 namespace {
 // copy n segments of float4: dst[dst_off[s] + i] = src[src_off[s] + i], i < len[s]; one block per segment
@@ -614,19 +735,11 @@ int launch_copy_segments(const int* d_src_off, const int* d_len, const int* d_ds
     return (int)cudaGetLastError();
 }
 
-int launch_relax(const KernelArgs& a, int team, int eval_only, cudaStream_t s, int num_sms, long long* launches) {
+int launch_relax(const KernelArgs& a, int team, int form, int eval_only, cudaStream_t s, int num_sms, long long* launches) {
     if (a.nwork <= 0) return 0;
     int r;
-    const int gdt = a.has_grid ? a.grid.dtype : GRID_F32;
-    if (eval_only) {
-        r = gdt == GRID_F16 ? launch_gdt<GRID_F16, true>(a, team, s, num_sms)
-          : gdt == GRID_BF16 ? launch_gdt<GRID_BF16, true>(a, team, s, num_sms)
-          : launch_gdt<GRID_F32, true>(a, team, s, num_sms);
-    } else {
-        r = gdt == GRID_F16 ? launch_gdt<GRID_F16, false>(a, team, s, num_sms)
-          : gdt == GRID_BF16 ? launch_gdt<GRID_BF16, false>(a, team, s, num_sms)
-          : launch_gdt<GRID_F32, false>(a, team, s, num_sms);
-    }
+    if (eval_only) r = form == FORM_GATHER ? launch_dtype<true, FORM_GATHER>(a, team, s, num_sms) : launch_dtype<true, FORM_ROUNDS>(a, team, s, num_sms);
+    else r = form == FORM_GATHER ? launch_dtype<false, FORM_GATHER>(a, team, s, num_sms) : launch_dtype<false, FORM_ROUNDS>(a, team, s, num_sms);
     if (launches && r == 0) (*launches)++;
     return r;
 }

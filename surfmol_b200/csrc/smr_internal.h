@@ -10,7 +10,7 @@
 //     role are pairwise distinct, so a team adds the round's force pieces to its
 //     shared-memory force array without atomics and in a fixed order.
 //   per atom of a system (state arena, indexed by SlotState::atom_off + local atom):
-//     float4 pos, vel, force (force.w = per-atom energy)
+//     float4 pos, plo (low parts of the positions), vel, force (force.w = per-atom energy)
 //   per system: SlotState (FIRE state, status, energy)
 //   grid: z-fastest i = iz + nz*(iy + ny*ix), float4 or 4 x 16-bit per voxel.
 #pragma once
@@ -28,12 +28,19 @@ static_assert(sizeof(AngRec) == 32 && sizeof(DihRec) == 32 && sizeof(InvRec) == 
 
 struct TopoDev {
     int natoms;
-    int atom_off;                 // into req / neigh / bk / bl
+    int atom_off;                 // into req / neigh / bk / bl / a2f
     int ang_off, ang_rounds;      // into the AngRec arena; ang_rounds * team records
     int dih_off, dih_rounds;
     int inv_off, inv_rounds;
     int team;                     // team size the rounds were packed for
-    int pad[3];
+    // gather form: unpadded term records (canonical orientation), piece buffer and per-atom
+    // lists of piece indices (angles 3 pieces, dihedrals and inversions 4; the pieces of term
+    // kind k start at 0, 3*nang, 3*nang + 4*ndih)
+    int fang_off, fdih_off, finv_off;
+    int nang, ndih, ninv;
+    int npieces;
+    int a2f_off;                  // into the piece-index arena; per atom (start, count) at atom_off
+    int pad[2];
 };
 
 struct SlotState {
@@ -44,7 +51,7 @@ struct SlotState {
     int steps;                    // FIRE steps done
     int npos;                     // FIRE consecutive uphill-free steps
     int active;                   // slot in use
-    int pad0;
+    int target;                   // absolute step count this smr_run_fire call may reach
     double dt, alpha;             // FIRE adaptive state
     double energy;                // total physical energy at the last force evaluation
     float fmax;                   // max |F| at the last force evaluation
@@ -73,14 +80,17 @@ struct KernelArgs {
     const TopoDev* topos;
     const float4* req; const short4* neigh; const float4* bk; const float4* bl;
     const AngRec* angs; const DihRec* dihs; const InvRec* invs;
-    float4* pos; float4* vel; float4* force;
+    float4* pos; float4* plo; float4* vel; float4* force;
     GridView grid; int has_grid;
     float R2damp, alpha_morse, rc2;
     FireDev fire;
-    int max_steps;                // steps this launch
-    int step_budget;              // cap on SlotState::steps (<=0: none)
+    int phase_limit;              // this launch runs a system until SlotState::steps reaches min(target, phase_limit)
+    int step_budget;              // a system reaching this many steps gets SMR_ST_MAXSTEPS (<=0: none)
     double* ecomp;                // eval mode: per work item x 8 energy components
     int nmax;                     // max atoms of a system in this launch (shared-memory sizing)
+    int nfmax;                    // gather form: max pieces of a system in this launch
+    const int2* a2f;              // gather form: per atom (first piece-index entry, count)
+    const int* a2f_idx;           // gather form: piece indices
 };
 
 // ---- host topology (topology.cpp)
@@ -90,6 +100,7 @@ struct HostTopo {
     std::vector<int> bonds; std::vector<double> bparams;
     std::vector<int> angs, ang_ngs; std::vector<double> angp;   // 3, 2, 5 per angle
     std::vector<int> dihs, dih_ngs; std::vector<double> dihp;   // 4, 3, 3
+    std::vector<int> dih_kj;                          // slot of j in k's neighbour list (reversed dihedral)
     std::vector<int> invs, inv_ngs; std::vector<double> invp;   // 4, 3, 4
     std::vector<double> req;                          // 4n
     std::vector<double> bond_kl;                      // 8n: (k, l0) per neighbour slot
@@ -101,6 +112,13 @@ struct PackedTerms {
     int ang_rounds = 0, dih_rounds = 0, inv_rounds = 0;
 };
 
+struct FlatTerms {                 // gather form of one topology
+    std::vector<AngRec> ang; std::vector<DihRec> dih; std::vector<InvRec> inv;
+    std::vector<int2> a2f;         // per atom (start into idx, count)
+    std::vector<int> idx;          // piece indices grouped by atom, in term order
+    int npieces = 0;
+};
+
 // topology.cpp
 int build_molecule_topology(int n, const int* Z, const double* pos, const double* q, double bond_cut, HostTopo& T,
                             char* err, int errlen);
@@ -108,11 +126,13 @@ int build_desc_topology(int natoms, const double* req, const int* neighs, const 
                         int nang, const int* angs, const double* angp, int ndih, const int* dihs, const double* dihp,
                         int ninv, const int* invs, const double* invp, HostTopo& T, char* err, int errlen);
 void pack_rounds(const HostTopo& T, int team, PackedTerms& out);
+void flat_terms(const HostTopo& T, FlatTerms& out);
 const char* type_name(int id);
 
 // relax.cu
-int launch_relax(const KernelArgs& a, int team, int eval_only, cudaStream_t s, int num_sms, long long* launches);
-size_t team_smem_bytes(int nmax);
+enum KernelForm { FORM_ROUNDS = 0, FORM_GATHER = 1 };
+int launch_relax(const KernelArgs& a, int team, int form, int eval_only, cudaStream_t s, int num_sms, long long* launches);
+size_t team_smem_bytes(int nmax, int nfmax, int team, int form);
 
 // grid.cu
 struct GridBuildArgs {

@@ -180,10 +180,11 @@ void enumerate_terms(HostTopo& T) {
             }
     std::sort(d.begin(), d.end());
     d.erase(std::unique(d.begin(), d.end()), d.end());
-    T.dihs.clear(); T.dih_ngs.clear();
+    T.dihs.clear(); T.dih_ngs.clear(); T.dih_kj.clear();
     for (auto& q : d) {
         T.dihs.insert(T.dihs.end(), q.begin(), q.end());
         T.dih_ngs.insert(T.dih_ngs.end(), {slot_of(T, q[1], q[0], 4), slot_of(T, q[1], q[2], 4), slot_of(T, q[2], q[3], 4)});
+        T.dih_kj.push_back(slot_of(T, q[2], q[1], 4));
     }
     T.invs.clear(); T.inv_ngs.clear();
     for (int i = 0; i < n; i++) {
@@ -384,6 +385,7 @@ int build_desc_topology(int natoms, const double* req, const int* neighs, const 
         const int* q = dihs + 4 * t;
         T.dihs.insert(T.dihs.end(), q, q + 4);
         T.dih_ngs.insert(T.dih_ngs.end(), {slot_of(T, q[1], q[0], 4), slot_of(T, q[1], q[2], 4), slot_of(T, q[2], q[3], 4)});
+        T.dih_kj.push_back(slot_of(T, q[2], q[1], 4));
         T.dihp.insert(T.dihp.end(), dihp + 3 * t, dihp + 3 * t + 3);
     }
     for (int t = 0; t < ninv; t++) {
@@ -397,58 +399,149 @@ int build_desc_topology(int natoms, const double* req, const int* neighs, const 
     return 0;
 }
 
-// Greedy packing of terms into rounds of `team` records such that within a round the
-// atoms in each role are pairwise distinct.  Empty records have at.x = -1.
+// Packing of terms into rounds of `team` records such that within a round the atoms in
+// each role are pairwise distinct (empty records have at.x = -1).  Greedy first-fit over a
+// term order, where each term may be placed in either of its two equivalent orientations
+// (an angle i-j-k as k-j-i, a dihedral i-j-k-l as l-k-j-i); the best of several seeded
+// random orders is kept, so the result is deterministic.
 namespace {
-template <int R, class Rec, class Fill>
-int pack_one(int n, int nterms, const int* atoms, int team, std::vector<Rec>& out, Fill fill) {
-    std::vector<std::vector<unsigned char>> used;   // [round][role * n + atom]
-    std::vector<int> count;
-    std::vector<int> round_of(nterms), pos_of(nterms);
-    for (int t = 0; t < nterms; t++) {
-        const int* a = atoms + R * t;
-        int r = 0;
-        for (;; r++) {
-            if (r == (int)used.size()) { used.emplace_back((size_t)R * n, 0); count.push_back(0); }
-            if (count[r] >= team) continue;
-            bool ok = true;
-            for (int k = 0; k < R && ok; k++) if (used[r][(size_t)k * n + a[k]]) ok = false;
-            if (ok) break;
+struct Xorshift {
+    unsigned long long s;
+    unsigned long long next() { s ^= s << 13; s ^= s >> 7; s ^= s << 17; return s; }
+};
+
+// atoms[t*R*2 + o*R + k]: atom of role k in orientation o (o = 1 may equal o = 0)
+template <int R>
+int pack_assign(int n, int nterms, const std::vector<int>& atoms, int team, std::vector<int>& round_of,
+                std::vector<int>& pos_of, std::vector<int>& orient_of) {
+    if (nterms == 0) { round_of.clear(); pos_of.clear(); orient_of.clear(); return 0; }
+    const int tries = std::max(1, std::min(64, 400000 / (nterms * R + 1)));
+    Xorshift rng{0x9E3779B97F4A7C15ull ^ (unsigned long long)nterms};
+    std::vector<int> order(nterms), r_of(nterms), p_of(nterms), o_of(nterms);
+    int best = 1 << 30;
+    for (int tr = 0; tr < tries; tr++) {
+        for (int t = 0; t < nterms; t++) order[t] = t;
+        if (tr > 0) for (int t = nterms - 1; t > 0; t--) std::swap(order[t], order[rng.next() % (unsigned long long)(t + 1)]);
+        std::vector<std::vector<unsigned char>> used;
+        std::vector<int> count;
+        for (int t : order) {
+            int br = -1, bo = 0;
+            for (int o = 0; o < 2; o++) {
+                const int* at = &atoms[((size_t)t * 2 + o) * R];
+                if (o == 1 && std::equal(at, at + R, &atoms[(size_t)t * 2 * R])) break;
+                for (int r = 0; r < (br < 0 ? (int)used.size() : br); r++) {
+                    if (count[r] >= team) continue;
+                    bool ok = true;
+                    for (int k = 0; k < R && ok; k++) if (used[r][(size_t)k * n + at[k]]) ok = false;
+                    if (ok) { br = r; bo = o; break; }
+                }
+            }
+            if (br < 0) { br = (int)used.size(); bo = 0; used.emplace_back((size_t)R * n, 0); count.push_back(0); }
+            const int* at = &atoms[((size_t)t * 2 + bo) * R];
+            for (int k = 0; k < R; k++) used[br][(size_t)k * n + at[k]] = 1;
+            r_of[t] = br; p_of[t] = count[br]++; o_of[t] = bo;
+            if ((int)used.size() >= best) break;
         }
-        for (int k = 0; k < R; k++) used[r][(size_t)k * n + a[k]] = 1;
-        round_of[t] = r; pos_of[t] = count[r]++;
+        if ((int)used.size() < best) { best = (int)used.size(); round_of = r_of; pos_of = p_of; orient_of = o_of; }
     }
-    int nr = (int)used.size();
+    return best;
+}
+
+template <class Rec, class Fill>
+void emit(int rounds, int team, int nterms, const std::vector<int>& round_of, const std::vector<int>& pos_of,
+          const std::vector<int>& orient_of, std::vector<Rec>& out, Fill fill) {
     Rec empty;
     std::memset(&empty, 0, sizeof(Rec));
     empty.at = make_short4(-1, -1, -1, -1);
-    empty.sl = make_short4(0, 0, 0, 0);
-    out.assign((size_t)nr * team, empty);
-    for (int t = 0; t < nterms; t++) fill(out[(size_t)round_of[t] * team + pos_of[t]], t);
-    return nr;
+    out.assign((size_t)rounds * team, empty);
+    for (int t = 0; t < nterms; t++) fill(out[(size_t)round_of[t] * team + pos_of[t]], t, orient_of[t]);
 }
 }  // namespace
 
-void pack_rounds(const HostTopo& T, int team, PackedTerms& P) {
-    int na = (int)T.angs.size() / 3, nd = (int)T.dihs.size() / 4, ni = (int)T.invs.size() / 4;
-    P.ang_rounds = pack_one<3>(T.n, na, T.angs.data(), team, P.ang, [&](AngRec& r, int t) {
+// Gather form: every term once in canonical orientation, pieces laid out as angles (3 each),
+// dihedrals (4), inversions (4), and for each atom the list of its pieces in that order.
+void flat_terms(const HostTopo& T, FlatTerms& F) {
+    const int na = (int)T.angs.size() / 3, nd = (int)T.dihs.size() / 4, ni = (int)T.invs.size() / 4;
+    F.ang.resize(na); F.dih.resize(nd); F.inv.resize(ni);
+    std::vector<std::vector<int>> per(T.n);
+    for (int t = 0; t < na; t++) {
         const int* a = &T.angs[3 * t]; const int* s = &T.ang_ngs[2 * t]; const double* p = &T.angp[5 * t];
+        AngRec& r = F.ang[t];
         r.at = make_short4((short)a[0], (short)a[1], (short)a[2], 0);
         r.sl = make_short4((short)s[0], (short)s[1], 0, 0);
         r.p = make_float4((float)(p[0] * p[1]), (float)(p[0] * p[2]), (float)(p[0] * p[3]), (float)(p[0] * p[4]));
-    });
-    P.dih_rounds = pack_one<4>(T.n, nd, T.dihs.data(), team, P.dih, [&](DihRec& r, int t) {
+        for (int k = 0; k < 3; k++) per[a[k]].push_back(3 * t + k);
+    }
+    for (int t = 0; t < nd; t++) {
         const int* a = &T.dihs[4 * t]; const int* s = &T.dih_ngs[3 * t]; const double* p = &T.dihp[3 * t];
+        DihRec& r = F.dih[t];
         r.at = make_short4((short)a[0], (short)a[1], (short)a[2], (short)a[3]);
         r.sl = make_short4((short)s[0], (short)s[1], (short)s[2], 0);
         r.p = make_float4((float)p[0], (float)p[1], (float)p[2], 0.f);
-    });
-    P.inv_rounds = pack_one<4>(T.n, ni, T.invs.data(), team, P.inv, [&](InvRec& r, int t) {
+        for (int k = 0; k < 4; k++) per[a[k]].push_back(3 * na + 4 * t + k);
+    }
+    for (int t = 0; t < ni; t++) {
         const int* a = &T.invs[4 * t]; const int* s = &T.inv_ngs[3 * t]; const double* p = &T.invp[4 * t];
+        InvRec& r = F.inv[t];
         r.at = make_short4((short)a[0], (short)a[1], (short)a[2], (short)a[3]);
         r.sl = make_short4((short)s[0], (short)s[1], (short)s[2], 0);
         r.p = make_float4((float)p[0], (float)p[1], (float)p[2], (float)p[3]);
-    });
+        for (int k = 0; k < 4; k++) per[a[k]].push_back(3 * na + 4 * nd + 4 * t + k);
+    }
+    F.npieces = 3 * na + 4 * nd + 4 * ni;
+    F.a2f.resize(T.n);
+    F.idx.clear();
+    for (int a = 0; a < T.n; a++) {
+        F.a2f[a] = make_int2((int)F.idx.size(), (int)per[a].size());
+        F.idx.insert(F.idx.end(), per[a].begin(), per[a].end());
+    }
+}
+
+void pack_rounds(const HostTopo& T, int team, PackedTerms& P) {
+    const int na = (int)T.angs.size() / 3, nd = (int)T.dihs.size() / 4, ni = (int)T.invs.size() / 4;
+    std::vector<int> ro, po, oo;
+    {   // angles: (i, j, k) or (k, j, i)
+        std::vector<int> at(6 * (size_t)na);
+        for (int t = 0; t < na; t++) {
+            const int* a = &T.angs[3 * t];
+            int* d = &at[6 * (size_t)t];
+            d[0] = a[0]; d[1] = a[1]; d[2] = a[2]; d[3] = a[2]; d[4] = a[1]; d[5] = a[0];
+        }
+        P.ang_rounds = pack_assign<3>(T.n, na, at, team, ro, po, oo);
+        emit(P.ang_rounds, team, na, ro, po, oo, P.ang, [&](AngRec& r, int t, int o) {
+            const int* a = &T.angs[3 * t]; const int* s = &T.ang_ngs[2 * t]; const double* p = &T.angp[5 * t];
+            if (o == 0) { r.at = make_short4((short)a[0], (short)a[1], (short)a[2], 0); r.sl = make_short4((short)s[0], (short)s[1], 0, 0); }
+            else { r.at = make_short4((short)a[2], (short)a[1], (short)a[0], 0); r.sl = make_short4((short)s[1], (short)s[0], 0, 0); }
+            r.p = make_float4((float)(p[0] * p[1]), (float)(p[0] * p[2]), (float)(p[0] * p[3]), (float)(p[0] * p[4]));
+        });
+    }
+    {   // dihedrals: (i, j, k, l) or (l, k, j, i); the reversed form needs the slot of j in k's list
+        std::vector<int> at(8 * (size_t)nd);
+        for (int t = 0; t < nd; t++) {
+            const int* a = &T.dihs[4 * t];
+            int* d = &at[8 * (size_t)t];
+            for (int k = 0; k < 4; k++) { d[k] = a[k]; d[4 + k] = a[3 - k]; }
+            if (T.dih_kj.empty() || T.dih_kj[t] < 0) for (int k = 0; k < 4; k++) d[4 + k] = a[k];   // no reversed form
+        }
+        P.dih_rounds = pack_assign<4>(T.n, nd, at, team, ro, po, oo);
+        emit(P.dih_rounds, team, nd, ro, po, oo, P.dih, [&](DihRec& r, int t, int o) {
+            const int* a = &T.dihs[4 * t]; const int* s = &T.dih_ngs[3 * t]; const double* p = &T.dihp[3 * t];
+            if (o == 0) { r.at = make_short4((short)a[0], (short)a[1], (short)a[2], (short)a[3]); r.sl = make_short4((short)s[0], (short)s[1], (short)s[2], 0); }
+            else { r.at = make_short4((short)a[3], (short)a[2], (short)a[1], (short)a[0]); r.sl = make_short4((short)s[2], (short)T.dih_kj[t], (short)s[0], 0); }
+            r.p = make_float4((float)p[0], (float)p[1], (float)p[2], 0.f);
+        });
+    }
+    {   // inversions: the centre must stay first; one orientation
+        std::vector<int> at(8 * (size_t)ni);
+        for (int t = 0; t < ni; t++) for (int k = 0; k < 4; k++) at[8 * (size_t)t + k] = at[8 * (size_t)t + 4 + k] = T.invs[4 * t + k];
+        P.inv_rounds = pack_assign<4>(T.n, ni, at, team, ro, po, oo);
+        emit(P.inv_rounds, team, ni, ro, po, oo, P.inv, [&](InvRec& r, int t, int) {
+            const int* a = &T.invs[4 * t]; const int* s = &T.inv_ngs[3 * t]; const double* p = &T.invp[4 * t];
+            r.at = make_short4((short)a[0], (short)a[1], (short)a[2], (short)a[3]);
+            r.sl = make_short4((short)s[0], (short)s[1], (short)s[2], 0);
+            r.p = make_float4((float)p[0], (float)p[1], (float)p[2], (float)p[3]);
+        });
+    }
 }
 
 }  // namespace smr

@@ -190,6 +190,29 @@ class RelaxMulti:
     def convert_grid(self, dtype):
         self._chk(self.L.smr_convert_grid(self.h, dtype), "smr_convert_grid")
 
+    def set_schedule(self, switch_step=0, latency_team=0, eval_form=0):
+        self._chk(self.L.smr_set_schedule(self.h, switch_step, latency_team, eval_form), "smr_set_schedule")
+
+    def get_schedule(self):
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        self._chk(self.L.smr_get_schedule(self.h, C.byref(a), C.byref(b), C.byref(c)), "smr_get_schedule")
+        return a.value, b.value, c.value
+
+    def set_stages(self, starts, teams, eval_form=0):
+        """Multi-stage schedule: stage k runs FIRE steps [starts[k], starts[k+1]); stage 0 in the
+        rounds form, later stages in the gather form with teams[k] threads (0: by size)."""
+        st, tm = _i(starts), _i(teams)
+        if len(st) != len(tm):
+            raise ValueError("starts and teams differ in length")
+        self._chk(self.L.smr_set_stages(self.h, len(st), _p(st, N.IP), _p(tm, N.IP), eval_form), "smr_set_stages")
+
+    def get_stages(self):
+        n = C.c_int(16)
+        st = np.zeros(16, np.int32)
+        tm = np.zeros(16, np.int32)
+        self._chk(self.L.smr_get_stages(self.h, C.byref(n), _p(st, N.IP), _p(tm, N.IP)), "smr_get_stages")
+        return st[:n.value].tolist(), tm[:n.value].tolist()
+
     def set_team_size(self, max_atoms, threads):
         self._chk(self.L.smr_set_team_size(self.h, max_atoms, threads), "smr_set_team_size")
 

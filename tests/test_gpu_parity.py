@@ -69,10 +69,13 @@ def test_pentacene_bonded(R, oracle):
     R.set_nb()
 
 
-@pytest.mark.parametrize("n,team", [(40, 32), (40, 64), (21, 32), (90, 64), (90, 128), (250, 128), (250, 256), (600, 512)])
-def test_forces_energies_match_oracle(R, oracle, slab_grid, n, team):
+@pytest.mark.parametrize("n,team,form", [(40, 32, 0), (40, 64, 0), (21, 32, 0), (90, 64, 0), (90, 128, 0), (250, 128, 0),
+                                         (250, 256, 0), (600, 512, 0), (40, 128, 1), (40, 32, 1), (90, 256, 1), (250, 512, 1)])
+def test_forces_energies_match_oracle(R, oracle, slab_grid, n, team, form):
+    """Rounds form (bonded terms in conflict-free rounds) and gather form (pieces + per-atom sums)."""
     slab, g = slab_grid
     R.set_team_size(1 << 20, team)
+    R.set_schedule(0, team, form)
     rng = np.random.default_rng(n * 31 + team)
     Z, P, q = molecule_on_slab(rng, n, slab)
     tid = R.add_molecule(Z, P, q)
@@ -90,6 +93,7 @@ def test_forces_energies_match_oracle(R, oracle, slab_grid, n, team):
     assert abs(E[0, 0] - Eco[0]) < 2e-6 * max(1.0, np.abs(Eco[1:7]).sum())
     R.remove_systems(s)
     R.set_team_size(1 << 20, 0)
+    R.set_schedule(0, 0, 0)
 
 
 @pytest.mark.parametrize("ncell,nlayers,nxy,nz", [(1, 2, 16, 20), (2, 3, 24, 16)])
@@ -169,6 +173,50 @@ def test_batched_plain_alone_mix_bitwise(R, oracle, slab_grid):
     assert mix["steps"][2] == alone["steps"][0] == plain["steps"][0] == 150
 
 
+@pytest.mark.parametrize("starts,teams", [([0, 60], [0, 128]), ([0, 1], [0, 256]), ([0, 60], [0, 32]),
+                                          ([0, 30, 80], [0, 64, 256])])
+def test_staged_schedule_bitwise(R, oracle, slab_grid, starts, teams):
+    """Rounds form until starts[1] steps, gather form stages after: batched, plain and chunked-alone runs
+    agree bit for bit (chunk ends fall inside and on stage boundaries), and the relaxed structure is an
+    oracle minimum."""
+    slab, g = slab_grid
+    if len(starts) == 2:
+        R.set_schedule(starts[1], teams[1], 0)
+        assert R.get_schedule() == (starts[1], teams[1], 0)
+    else:
+        R.set_stages(starts, teams)
+    assert R.get_stages() == (starts, teams)
+    rng = np.random.default_rng(21 + starts[1])
+    mols = [molecule_on_slab(rng, n, slab) for n in (40, 30, 120)]
+    tids = [R.add_molecule(Z, P, q) for Z, P, q in mols]
+    a = R.add_systems(tids, [m[1] for m in mols])
+    R.run_fire(140, step_budget=140, fconv=1e-6)
+    mix = R.download(a)
+    R.remove_systems(a)
+    b = R.add_systems([tids[0]], [mols[0][1]])
+    for _ in range(4):
+        R.run_fire(35, step_budget=140, fconv=1e-6)
+    alone = R.download(b)
+    R.remove_systems(b)
+    c = R.add_systems([tids[0]], [mols[0][1]])
+    R.run_fire(140, step_budget=140, fconv=1e-6, mode=1)
+    plain = R.download(c)
+    R.remove_systems(c)
+    assert np.array_equal(mix["pos"][0], alone["pos"][0]) and np.array_equal(mix["pos"][0], plain["pos"][0])
+    assert mix["steps"][0] == alone["steps"][0] == plain["steps"][0] == 140
+    d = R.add_systems([tids[1]], [mols[1][1]])
+    R.run_fire(3000, step_budget=3000, fconv=1e-3)
+    out = R.download(d)
+    assert out["status"][0] in (1, 2)
+    S = oracle.System.from_molecule(*mols[1])
+    Fo, _, _ = S.eval(out["pos"][0].astype(np.float64), oracle.Grid(g["coef"], g["p0"], g["step"]))
+    assert force_err(out["forces"][0], Fo) < 1e-3          # forces of the last step were taken 1 move earlier
+    if out["status"][0] == 1:
+        assert np.sqrt((Fo ** 2).sum(1)).max() < 1e-3 + 3e-4
+    R.remove_systems(d)
+    R.set_schedule(0, 0, 0)
+
+
 def test_nonfinite_system_is_isolated(R, oracle, slab_grid):
     slab, g = slab_grid
     rng = np.random.default_rng(13)
@@ -185,3 +233,18 @@ def test_nonfinite_system_is_isolated(R, oracle, slab_grid):
     assert np.array_equal(out["pos"][0], out2["pos"][0]) and np.array_equal(out["pos"][2], out2["pos"][1])
     R.remove_systems(s)
     R.remove_systems(ref)
+
+
+def test_full_config_grid_matches_oracle(R, oracle):
+    """The 226x226x121 grid of the benchmark workload (2-layer 4x4-cell slab) against the FP64 builder."""
+    slab = synth.rocksalt_slab(4, 2)
+    g = synth.grid_for(slab, nz=121)
+    R.build_grid(slab.ions, slab.req()[:, :2], slab.Lx, slab.Ly, g.nx, g.ny, g.nz, g.p0, g.step)
+    cg = R.get_grid()["coef"].astype(np.float64)
+    co = oracle.build_grid_fast(slab.ions, slab.req(), slab.Lx, slab.Ly, g.nx, g.ny, g.nz, g.p0, g.step)
+    # Morse node values are sums of FP32 terms (as make_MorseFF computes them) and the exact
+    # B-spline fit amplifies node errors by up to 3 per axis: 1e-5 for P, L; FP64 Ewald: 2e-6
+    for c, tol in zip(range(3), (1e-5, 1e-5, 2e-6)):
+        scale = np.abs(co[..., c]).max()
+        assert scale > 0
+        assert np.abs(cg[..., c] - co[..., c]).max() < tol * scale, c
