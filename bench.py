@@ -34,6 +34,21 @@ METRIC = "relaxed systems/sec at ≤1e-4 eV/Å force error; p50/p99 relax latenc
 FIRE = dict(dt0=0.001, dt_max=0.05, fconv=1e-3)
 MAX_STEPS = 2000
 SEED = 20261203
+# FIRE steps [0, 1100) in the rounds form (a warp per system: throughput), the rest in the gather
+# form with 128 threads per system (latency of the slow tail)
+STAGES = "0:rounds:0,1100:gather:128"
+FORMS = {"rounds": 0, "gather": 1, "owner": 2}
+
+
+def parse_stages(txt):
+    """'start:form:team,...' -> (starts, forms, teams)"""
+    st, fm, tm = [], [], []
+    for part in txt.split(","):
+        a, f, t = part.split(":")
+        st.append(int(a))
+        fm.append(FORMS[f])
+        tm.append(int(t))
+    return st, fm, tm
 
 
 def peaks():
@@ -213,6 +228,7 @@ def run_ours(args, ws, rank, local):
     tgrid = time.perf_counter() - t0
     tid = R.add_molecule(w.Z[0], w.pos[0], w.q[0])
     slots = R.add_systems([tid] * args.nsys, w.pos)
+    R.set_stages(*parse_stages(args.stages))
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MB > 126 MB L2
 
     def reset():
@@ -287,7 +303,7 @@ def run_ours(args, ws, rank, local):
                        "converged_fraction": conv / (args.nsys * args.steps),
                        "fire_steps_p50": float(np.percentile(steps_all, 50)),
                        "fire_steps_p99": float(np.percentile(steps_all, 99)),
-                       "mode": "batched persistent kernel (one launch per team class)"},
+                       "mode": "batched persistent kernel, one launch per schedule stage", "stages": args.stages},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "traffic": traffic, "peak_source": peak_kind,
                          "algorithmic_bytes": "1024 B per atom-step (64 float4 grid voxels), state resident in shared memory"},
@@ -316,6 +332,7 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--max-steps", type=int, default=MAX_STEPS, help="FIRE step cap per system (profiling runs)")
+    ap.add_argument("--stages", default=STAGES, help="schedule: start:form:team,... (form rounds / gather / owner; team 0 = by size)")
     ap.add_argument("--profile", action="store_true", help="timed steps only: no e2e leg, no CPU baseline")
     args = ap.parse_args()
     if args.impl == "reference":

@@ -207,31 +207,46 @@ int smr_reset_fire(smr_handle* h, int nsys, const int* slot_ids);
  * the last force evaluation); steps: FIRE steps done; status: SMR_ST_*. */
 int smr_download(smr_handle* h, int nsys, const int* slot_ids, float* pos, float* forces, double* energy,
                  int* steps, int* status);
+/* Positions at full precision: the kernels carry each coordinate as a float plus the float
+ * rounding error of its FIRE moves; this returns their sum as sum(natoms) x 3 doubles.  No
+ * counterpart in the reference (its state is float only). */
+int smr_download_pos64(smr_handle* h, int nsys, const int* slot_ids, double* pos);
 
 /* Device time (ms, CUDA events on the handle's stream) of the last smr_run_fire /
  * smr_eval_forces call, and the number of kernel launches it made. */
 int smr_last_timing(smr_handle* h, double* ms, long long* launches);
 
-/* Schedule of smr_run_fire (batched and plain alike): every system runs its first switch_step
- * FIRE steps in the rounds form (warp-sized teams, bonded terms in conflict-free rounds: best
- * throughput when many systems share the GPU) and later steps in the gather form with
- * latency_team threads per system (all bonded terms at once into shared memory, then a
- * per-atom gather: best latency for the slow tail of a batch).  switch_step <= 0 keeps the
- * rounds form throughout; latency_team 0 picks by size.  The switch depends only on a system's
- * own step count, so results do not depend on what else runs.  eval_form (0 rounds, 1 gather)
- * selects the form of smr_eval_forces. */
+/* Force-evaluation forms of the kernels (results agree to rounding; each is deterministic):
+ *  SMR_FORM_ROUNDS  bonded terms in host-packed conflict-free rounds added straight into the
+ *                   shared-memory force array (one team size per topology): best throughput
+ *                   when many small systems share the GPU
+ *  SMR_FORM_GATHER  all bonded terms at once into a piece buffer, then a per-atom gather
+ *                   (opencl/UFF.cl:801-880): most parallel per system, best latency
+ *  SMR_FORM_OWNER   every term evaluated by the atom that owns it (angle apex, inversion centre,
+ *                   both central atoms of a dihedral) with its neighbours' pieces kept in
+ *                   registers and gathered over the bond back-slots: no team syncs between terms */
+#define SMR_FORM_ROUNDS 0
+#define SMR_FORM_GATHER 1
+#define SMR_FORM_OWNER 2
+
+/* Schedule of smr_run_fire (batched and plain alike): nstages (1..16) stages; stage k covers
+ * FIRE steps [starts[k], starts[k+1]) of each system (the last one is open), starts[0] == 0 and
+ * strictly increasing, and runs forms[k] with teams[k] threads per system (0: the form's default
+ * for the system's size; else 32, 64, 128, 256 or 512).  A system whose topology or shared memory
+ * does not allow the requested form runs the rounds form instead.  Which form a system runs
+ * depends only on the system and its own step count, so results do not depend on what else runs.
+ * In batched mode each stage is a separate launch over the systems still running (which also
+ * spreads them evenly over the SMs again).  eval_form is the form of smr_eval_forces (team by
+ * size).  Default: one stage, SMR_FORM_ROUNDS.  No counterpart in the reference (one OpenCL
+ * kernel form). */
+int smr_set_stages(smr_handle* h, int nstages, const int* starts, const int* forms, const int* teams, int eval_form);
+/* *nstages: capacity of the arrays in, stage count out (arrays may be null to query the count). */
+int smr_get_stages(smr_handle* h, int* nstages, int* starts, int* forms, int* teams);
+/* Two-stage shortcut: rounds form until switch_step FIRE steps, then the gather form with
+ * latency_team threads (0: by size); switch_step <= 0 keeps the rounds form throughout.
+ * smr_eval_forces then runs eval_form with latency_team threads. */
 int smr_set_schedule(smr_handle* h, int switch_step, int latency_team, int eval_form);
 int smr_get_schedule(smr_handle* h, int* switch_step, int* latency_team, int* eval_form);
-
-/* General schedule: nstages (1..16) stages; stage k covers FIRE steps [starts[k], starts[k+1])
- * (the last one is open), starts[0] == 0 and strictly increasing.  Stage 0 runs the rounds form
- * with the topology's team (teams[0] ignored); stage k >= 1 runs the gather form with teams[k]
- * threads per system (0: pick by size; 32, 64, 128, 256 or 512).  In batched mode every stage
- * is a separate launch over the systems still running, which also spreads the remaining
- * systems evenly over the SMs again.  smr_set_schedule(h, s, t, f) equals the two stages
- * {0, s} / {0, t}.  No counterpart in the reference (its OpenCL harness has one kernel form). */
-int smr_set_stages(smr_handle* h, int nstages, const int* starts, const int* teams, int eval_form);
-int smr_get_stages(smr_handle* h, int* nstages, int* starts, int* teams);
 
 /* Team configuration of the persistent kernel: threads per system team for systems of
  * up to n atoms (0 = library default / autotuned). */

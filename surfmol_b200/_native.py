@@ -84,12 +84,13 @@ SIGNATURES = {
     "smr_run_fire": (C.c_int, [VP, C.c_int, C.c_int, C.POINTER(SmrFireParams), C.c_int, IP]),
     "smr_reset_fire": (C.c_int, [VP, C.c_int, IP]),
     "smr_download": (C.c_int, [VP, C.c_int, IP, FP, FP, DP, IP, IP]),
+    "smr_download_pos64": (C.c_int, [VP, C.c_int, IP, DP]),
     "smr_last_timing": (C.c_int, [VP, DP, LLP]),
     "smr_set_team_size": (C.c_int, [VP, C.c_int, C.c_int]),
     "smr_set_schedule": (C.c_int, [VP, C.c_int, C.c_int, C.c_int]),
     "smr_get_schedule": (C.c_int, [VP, IP, IP, IP]),
-    "smr_set_stages": (C.c_int, [VP, C.c_int, IP, IP, C.c_int]),
-    "smr_get_stages": (C.c_int, [VP, IP, IP, IP]),
+    "smr_set_stages": (C.c_int, [VP, C.c_int, IP, IP, IP, C.c_int]),
+    "smr_get_stages": (C.c_int, [VP, IP, IP, IP, IP]),
 }
 
 _lib = None

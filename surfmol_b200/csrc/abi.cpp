@@ -29,13 +29,19 @@ struct DArr {   // growable device array with a host mirror of the uploaded pref
     T* d = nullptr;
     size_t cap = 0;
     ~DArr() { if (d) cudaFree(d); }
-    cudaError_t reserve(size_t n, size_t keep) {
+    // grow to at least n elements keeping the first `keep`; the copy is ordered after earlier
+    // uploads on stream s and completes before the old buffer is freed
+    cudaError_t reserve(size_t n, size_t keep, cudaStream_t s) {
         if (n <= cap) return cudaSuccess;
         size_t nc = std::max(n, cap * 2 + 1024);
         T* nd = nullptr;
         cudaError_t e = cudaMalloc(&nd, nc * sizeof(T));
         if (e != cudaSuccess) return e;
-        if (d && keep) { e = cudaMemcpy(nd, d, keep * sizeof(T), cudaMemcpyDeviceToDevice); if (e != cudaSuccess) { cudaFree(nd); return e; } }
+        if (d && keep) {
+            e = cudaMemcpyAsync(nd, d, keep * sizeof(T), cudaMemcpyDeviceToDevice, s);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            if (e != cudaSuccess) { cudaFree(nd); return e; }
+        }
         if (d) cudaFree(d);
         d = nd; cap = nc;
         return cudaSuccess;
@@ -85,14 +91,17 @@ struct smr_handle {
     DArr<AngRec> dang; DArr<DihRec> ddih; DArr<InvRec> dinv;
     std::vector<int2> ha2f; std::vector<int> hidx;      // gather form: per atom (start, count), piece indices
     DArr<int2> da2f; DArr<int> didx;
-    size_t up_atoms = 0, up_ang = 0, up_dih = 0, up_inv = 0, up_topo = 0, up_idx = 0;   // uploaded prefixes
+    std::vector<short4> hown_geo; std::vector<float4> hown_par; std::vector<int> hown_meta;   // owner form
+    DArr<short4> down_geo; DArr<float4> down_par; DArr<int> down_meta;
+    size_t up_atoms = 0, up_ang = 0, up_dih = 0, up_inv = 0, up_topo = 0, up_idx = 0, up_own = 0;   // uploaded prefixes
     std::map<int, int> team_override;   // max_atoms -> threads
-    // schedule: stage 0 runs FIRE steps [0, stage_start[1]) in the rounds form with the topology's
-    // team; stage k >= 1 runs steps [stage_start[k], stage_start[k+1]) in the gather form with
-    // stage_team[k] threads per system (0: pick by size).  One stage = the rounds form throughout.
+    // schedule: stage k runs FIRE steps [stage_start[k], stage_start[k+1]) in stage_form[k] with
+    // stage_team[k] threads per system (0: the form's default for the system's size)
     std::vector<int> stage_start{0};
     std::vector<int> stage_team{0};
-    int eval_form = 0;                  // form used by smr_eval_forces
+    std::vector<int> stage_form{FORM_ROUNDS};
+    int eval_form = FORM_ROUNDS;        // form and team (0: by size) of smr_eval_forces
+    int eval_team = 0;
 
     // grid
     void* grid = nullptr;
@@ -156,13 +165,25 @@ void append_topology(smr_handle* h, const HostTopo& T) {
     td.a2f_off = (int)h->hidx.size();
     h->ha2f.insert(h->ha2f.end(), F.a2f.begin(), F.a2f.end());
     h->hidx.insert(h->hidx.end(), F.idx.begin(), F.idx.end());
+    OwnerTerms O;
+    td.own_ok = owner_terms(T, O) ? 1 : 0;
+    if (td.own_ok) {
+        td.own_a_off = (int)h->hown_geo.size();
+        td.own_i_off = td.own_a_off + O.rows_a * T.n;
+        td.own_d_off = td.own_i_off + O.rows_i * T.n;
+        h->hown_geo.insert(h->hown_geo.end(), O.geo.begin(), O.geo.end());
+        h->hown_par.insert(h->hown_par.end(), O.par.begin(), O.par.end());
+        h->hown_meta.insert(h->hown_meta.end(), O.meta.begin(), O.meta.end());
+    } else {
+        h->hown_meta.insert(h->hown_meta.end(), T.n, 0);
+    }
     h->htd.push_back(td);
 }
 
 template <class T>
 cudaError_t sync_arr(DArr<T>& d, const std::vector<T>& hv, size_t& up, cudaStream_t s) {
     if (hv.size() == up) return cudaSuccess;
-    cudaError_t e = d.reserve(hv.size(), up);
+    cudaError_t e = d.reserve(hv.size(), up, s);
     if (e != cudaSuccess) return e;
     e = cudaMemcpyAsync(d.d + up, hv.data() + up, (hv.size() - up) * sizeof(T), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) up = hv.size();
@@ -178,7 +199,11 @@ int upload_all(smr_handle* h) {
     t = ua; CU(h, sync_arr(h->dbk, h->hbk, t, s));
     t = ua; CU(h, sync_arr(h->dbl, h->hbl, t, s));
     t = ua; CU(h, sync_arr(h->da2f, h->ha2f, t, s));
+    t = ua; CU(h, sync_arr(h->down_meta, h->hown_meta, t, s));
     h->up_atoms = h->hreq.size();
+    t = h->up_own; CU(h, sync_arr(h->down_geo, h->hown_geo, t, s));
+    t = h->up_own; CU(h, sync_arr(h->down_par, h->hown_par, t, s));
+    h->up_own = h->hown_geo.size();
     CU(h, sync_arr(h->didx, h->hidx, h->up_idx, s));
     CU(h, sync_arr(h->dang, h->hang, h->up_ang, s));
     CU(h, sync_arr(h->ddih, h->hdih, h->up_dih, s));
@@ -191,7 +216,8 @@ int upload_all(smr_handle* h) {
 int repack_all(smr_handle* h) {
     h->htd.clear(); h->hreq.clear(); h->hneigh.clear(); h->hbk.clear(); h->hbl.clear();
     h->hang.clear(); h->hdih.clear(); h->hinv.clear(); h->ha2f.clear(); h->hidx.clear();
-    h->up_atoms = h->up_ang = h->up_dih = h->up_inv = h->up_topo = h->up_idx = 0;
+    h->hown_geo.clear(); h->hown_par.clear(); h->hown_meta.clear();
+    h->up_atoms = h->up_ang = h->up_dih = h->up_inv = h->up_topo = h->up_idx = h->up_own = 0;
     for (const HostTopo& T : h->topos) append_topology(h, T);
     return upload_all(h);
 }
@@ -259,6 +285,7 @@ KernelArgs base_args(smr_handle* h) {
     a.req = h->dreq.d; a.neigh = h->dneigh.d; a.bk = h->dbk.d; a.bl = h->dbl.d;
     a.angs = h->dang.d; a.dihs = h->ddih.d; a.invs = h->dinv.d;
     a.a2f = h->da2f.d; a.a2f_idx = h->didx.d;
+    a.own_geo = h->down_geo.d; a.own_par = h->down_par.d; a.own_meta = h->down_meta.d;
     a.pos = h->pos; a.plo = h->plo; a.vel = h->vel; a.force = h->force;
     a.has_grid = h->has_grid ? 1 : 0;
     a.grid.data = h->grid;
@@ -281,19 +308,23 @@ int latency_team_for(int requested, int n) {
 }
 
 // Launch segments for a list of slots.  The form of every system is decided from the system
-// alone (the gather form when its own shared memory fits, else the rounds form with its
-// topology's team), never from what it is batched with; segments group equal (form, team) and
-// are split wherever the segment's largest system would no longer fit.
-std::vector<Seg> group_by(smr_handle* h, std::vector<int>& ids, int form, int lat_team = 0) {
+// alone (the requested form when the topology supports it and its own shared memory fits, else
+// the rounds form with its topology's team), never from what it is batched with; segments group
+// equal (form, team) and are split wherever the segment's largest system would no longer fit.
+std::vector<Seg> group_by(smr_handle* h, std::vector<int>& ids, int form, int req_team = 0) {
     struct Key { int form, team, n, nf; };
     auto key_of = [&](int s) {
         const SlotState& st = h->hs[s];
-        const int n = st.natoms, nf = h->htd[st.topo].npieces;
+        const TopoDev& td = h->htd[st.topo];
+        const int n = st.natoms, nf = td.npieces;
         if (form == FORM_GATHER) {
-            const int t = latency_team_for(lat_team, n);
+            const int t = latency_team_for(req_team, n);
             if (team_smem_bytes(n, nf, t, FORM_GATHER) <= h->smem_optin) return Key{FORM_GATHER, t, n, nf};
+        } else if (form == FORM_OWNER && td.own_ok) {
+            const int t = req_team ? req_team : td.team;
+            if (team_smem_bytes(n, nf, t, FORM_OWNER) <= h->smem_optin) return Key{FORM_OWNER, t, n, nf};
         }
-        return Key{FORM_ROUNDS, h->htd[st.topo].team, n, nf};
+        return Key{FORM_ROUNDS, td.team, n, nf};
     };
     std::vector<Key> keys(h->max_systems);
     for (int s : ids) keys[s] = key_of(s);
@@ -372,9 +403,10 @@ int smr_create(const smr_config* cfg, smr_handle** out) {
         cudaMalloc(&h->work, ns * 4) || cudaMalloc(&h->counter, 64) || cudaMalloc(&h->ecomp, ns * 8 * 8) ||
         cudaMalloc(&h->xfer, ns * 3 * 4) || cudaMallocHost(&h->pinned, na * 16))
         return bail(SMR_ERR_CUDA);
-    cudaMemset(h->slots, 0, ns * sizeof(SlotState));
-    cudaMemset(h->vel, 0, na * 16);
-    cudaMemset(h->plo, 0, na * 16);
+    // zeroed on the handle's stream (a legacy-stream memset is not ordered with it)
+    if (cudaMemsetAsync(h->slots, 0, ns * sizeof(SlotState), h->stream) || cudaMemsetAsync(h->vel, 0, na * 16, h->stream) ||
+        cudaMemsetAsync(h->plo, 0, na * 16, h->stream) || cudaStreamSynchronize(h->stream))
+        return bail(SMR_ERR_CUDA);
     h->hs.assign(ns, SlotState{});
     for (int s = (int)ns - 1; s >= 0; s--) h->free_slots.push_back(s);
     h->free_atoms[0] = (long long)na;
@@ -425,7 +457,8 @@ int smr_set_grid(smr_handle* h, const void* coef, int dtype, const float scale[4
     size_t nv = (size_t)nx * ny * nz, bytes = nv * voxel_bytes(dtype);
     void* d = nullptr;
     CU(h, cudaMalloc(&d, bytes));
-    cudaError_t e = cudaMemcpy(d, coef, bytes, cudaMemcpyHostToDevice);
+    cudaError_t e = cudaMemcpyAsync(d, coef, bytes, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) { cudaFree(d); return fail(h, SMR_ERR_CUDA, "grid upload: %s", cudaGetErrorString(e)); }
     if (h->grid) cudaFree(h->grid);
     h->grid = d; h->grid_dtype = dtype; h->has_grid = true;
@@ -445,7 +478,8 @@ int smr_get_grid(smr_handle* h, void* coef_out, int* dtype, float scale[4], int 
     if (step) for (int k = 0; k < 3; k++) step[k] = h->gstep[k];
     if (coef_out) {
         size_t bytes = (size_t)h->gdim[0] * h->gdim[1] * h->gdim[2] * voxel_bytes(h->grid_dtype);
-        CU(h, cudaMemcpy(coef_out, h->grid, bytes, cudaMemcpyDeviceToHost));
+        CU(h, cudaMemcpyAsync(coef_out, h->grid, bytes, cudaMemcpyDeviceToHost, h->stream));
+        CU(h, cudaStreamSynchronize(h->stream));
     }
     return SMR_OK;
 }
@@ -489,11 +523,12 @@ int smr_build_grid(smr_handle* h, int nions, const double* ions, const double* i
     CU(h, cudaMalloc(&dions, (size_t)nions * 32));
     cudaError_t e = cudaMalloc(&dre, (size_t)nions * 32);
     if (e == cudaSuccess) e = cudaMalloc(&out, nv * 16);
-    if (e == cudaSuccess) e = cudaMemcpy(dions, ions, (size_t)nions * 32, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dions, ions, (size_t)nions * 32, cudaMemcpyHostToDevice, h->stream);
     if (e == cudaSuccess) {
         std::vector<double> re4(4 * (size_t)nions, 0.0);
         for (int i = 0; i < nions; i++) { re4[4 * i] = ion_re[2 * i]; re4[4 * i + 1] = ion_re[2 * i + 1]; }
-        e = cudaMemcpy(dre, re4.data(), re4.size() * 8, cudaMemcpyHostToDevice);
+        e = cudaMemcpyAsync(dre, re4.data(), re4.size() * 8, cudaMemcpyHostToDevice, h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);   // re4 is freed on return
     }
     if (e != cudaSuccess) { cudaFree(dions); cudaFree(dre); cudaFree(out); return fail(h, SMR_ERR_CUDA, "grid build alloc: %s", cudaGetErrorString(e)); }
     GridBuildArgs A{};
@@ -675,7 +710,7 @@ int smr_eval_forces(smr_handle* h, int nsys, const int* slot_ids, float* forces,
     { int r = check_batch(h, nsys, slot_ids); if (r) return r; }
     if (nsys == 0) return SMR_OK;
     std::vector<int> sorted(slot_ids, slot_ids + nsys);
-    auto segs = group_by(h, sorted, h->eval_form);
+    auto segs = group_by(h, sorted, h->eval_form, h->eval_team);
     for (auto& g : segs) { int r = check_smem(h, g); if (r) return r; }
     std::vector<int> pos_in_input(h->max_systems);
     for (int i = 0; i < nsys; i++) pos_in_input[slot_ids[i]] = i;
@@ -699,7 +734,8 @@ int smr_eval_forces(smr_handle* h, int nsys, const int* slot_ids, float* forces,
     h->last_ms = ms;
     if (energy) {
         std::vector<double> e((size_t)nsys * 8);
-        CU(h, cudaMemcpy(e.data(), h->ecomp, e.size() * 8, cudaMemcpyDeviceToHost));
+        CU(h, cudaMemcpyAsync(e.data(), h->ecomp, e.size() * 8, cudaMemcpyDeviceToHost, h->stream));
+        CU(h, cudaStreamSynchronize(h->stream));
         for (int i = 0; i < nsys; i++) std::copy(&e[(size_t)i * 8], &e[(size_t)i * 8 + 8], energy + (size_t)pos_in_input[sorted[i]] * 8);
     }
     if (forces) {
@@ -710,42 +746,55 @@ int smr_eval_forces(smr_handle* h, int nsys, const int* slot_ids, float* forces,
 }
 
 static bool team_ok(int t) { return t == 0 || t == 32 || t == 64 || t == 128 || t == 256 || t == 512; }
+static bool form_ok(int f) { return f == FORM_ROUNDS || f == FORM_GATHER || f == FORM_OWNER; }
 
-int smr_set_stages(smr_handle* h, int nstages, const int* starts, const int* teams, int eval_form) {
-    if (!h || nstages < 1 || nstages > 16 || !starts || !teams) return SMR_ERR_ARG;
+int smr_set_stages(smr_handle* h, int nstages, const int* starts, const int* forms, const int* teams, int eval_form) {
+    if (!h || nstages < 1 || nstages > 16 || !starts || !forms || !teams) return SMR_ERR_ARG;
     if (starts[0] != 0) return fail(h, SMR_ERR_ARG, "the first stage must start at step 0");
     for (int k = 1; k < nstages; k++) if (starts[k] <= starts[k - 1]) return fail(h, SMR_ERR_ARG, "stage starts must increase");
-    for (int k = 0; k < nstages; k++) if (!team_ok(teams[k])) return fail(h, SMR_ERR_ARG, "stage team must be 0, 32, 64, 128, 256 or 512");
-    if (eval_form != FORM_ROUNDS && eval_form != FORM_GATHER) return fail(h, SMR_ERR_ARG, "eval form must be 0 (rounds) or 1 (gather)");
+    for (int k = 0; k < nstages; k++) {
+        if (!team_ok(teams[k])) return fail(h, SMR_ERR_ARG, "stage team must be 0, 32, 64, 128, 256 or 512");
+        if (!form_ok(forms[k])) return fail(h, SMR_ERR_ARG, "stage form must be 0 (rounds), 1 (gather) or 2 (owner)");
+    }
+    if (!form_ok(eval_form)) return fail(h, SMR_ERR_ARG, "eval form must be 0 (rounds), 1 (gather) or 2 (owner)");
     h->stage_start.assign(starts, starts + nstages);
+    h->stage_form.assign(forms, forms + nstages);
     h->stage_team.assign(teams, teams + nstages);
     h->eval_form = eval_form;
+    h->eval_team = 0;
     return SMR_OK;
 }
 
-int smr_set_schedule(smr_handle* h, int switch_step, int latency_team, int eval_form) {
-    if (!h) return SMR_ERR_ARG;
-    if (switch_step <= 0) { int st = 0, tm = 0; return smr_set_stages(h, 1, &st, &tm, eval_form); }
-    int st[2] = {0, switch_step}, tm[2] = {0, latency_team};
-    return smr_set_stages(h, 2, st, tm, eval_form);
-}
-
-int smr_get_stages(smr_handle* h, int* nstages, int* starts, int* teams) {
+int smr_get_stages(smr_handle* h, int* nstages, int* starts, int* forms, int* teams) {
     if (!h || !nstages) return SMR_ERR_ARG;
     const int n = (int)h->stage_start.size();
-    if (starts && teams) {
+    if (starts && forms && teams) {
         if (*nstages < n) return fail(h, SMR_ERR_CAPACITY, "schedule has %d stages", n);
         std::copy(h->stage_start.begin(), h->stage_start.end(), starts);
+        std::copy(h->stage_form.begin(), h->stage_form.end(), forms);
         std::copy(h->stage_team.begin(), h->stage_team.end(), teams);
     }
     *nstages = n;
     return SMR_OK;
 }
 
+int smr_set_schedule(smr_handle* h, int switch_step, int latency_team, int eval_form) {
+    if (!h) return SMR_ERR_ARG;
+    if (!team_ok(latency_team)) return fail(h, SMR_ERR_ARG, "latency team must be 0, 32, 64, 128, 256 or 512");
+    int r;
+    if (switch_step <= 0) { int st = 0, fm = FORM_ROUNDS, tm = 0; r = smr_set_stages(h, 1, &st, &fm, &tm, eval_form); }
+    else {
+        int st[2] = {0, switch_step}, fm[2] = {FORM_ROUNDS, FORM_GATHER}, tm[2] = {0, latency_team};
+        r = smr_set_stages(h, 2, st, fm, tm, eval_form);
+    }
+    if (r == SMR_OK) h->eval_team = latency_team;
+    return r;
+}
+
 int smr_get_schedule(smr_handle* h, int* switch_step, int* latency_team, int* eval_form) {
     if (!h) return SMR_ERR_ARG;
     if (switch_step) *switch_step = h->stage_start.size() > 1 ? h->stage_start[1] : 0;
-    if (latency_team) *latency_team = h->stage_team.size() > 1 ? h->stage_team[1] : 0;
+    if (latency_team) *latency_team = h->stage_team.size() > 1 ? h->stage_team[1] : h->eval_team;
     if (eval_form) *eval_form = h->eval_form;
     return SMR_OK;
 }
@@ -779,8 +828,8 @@ int smr_run_fire(smr_handle* h, int max_steps, int step_budget, const smr_fire_p
     // per stage: segments of the running systems in that stage's form and team
     std::vector<std::vector<int>> sids(nst, ids);
     std::vector<std::vector<Seg>> ssegs(nst);
-    for (int k = 0; k < nst; k++) ssegs[k] = group_by(h, sids[k], k == 0 ? FORM_ROUNDS : FORM_GATHER, h->stage_team[k]);
-    for (auto& g : ssegs[0]) { r = check_smem(h, g); if (r) return r; }
+    for (int k = 0; k < nst; k++) ssegs[k] = group_by(h, sids[k], h->stage_form[k], h->stage_team[k]);
+    for (auto& sg : ssegs) for (auto& g : sg) { r = check_smem(h, g); if (r) return r; }
     cudaEventRecord(h->ev0, s);
     auto launch = [&](const Seg& g, const int* work_base, int limit, int nwork_override) -> int {
         a.work = work_base + g.begin; a.nwork = nwork_override > 0 ? nwork_override : g.end - g.begin;
@@ -806,7 +855,7 @@ int smr_run_fire(smr_handle* h, int max_steps, int step_budget, const smr_fire_p
             std::vector<Seg> per_stage(nst);
             for (int k = 0; k < nst; k++) {
                 std::vector<int> one{slot};
-                per_stage[k] = group_by(h, one, k == 0 ? FORM_ROUNDS : FORM_GATHER, h->stage_team[k])[0];
+                per_stage[k] = group_by(h, one, h->stage_form[k], h->stage_team[k])[0];
                 per_stage[k].begin = kk; per_stage[k].end = kk + 1;
             }
             for (int steps = start[slot]; steps < st.target; steps++) {
@@ -868,6 +917,37 @@ int smr_download(smr_handle* h, int nsys, const int* slot_ids, float* pos, float
         if (r) return r;
         if (which == 0) for (long long a = 0; a < p; a++) { out[3 * a] = h->pinned[a].x; out[3 * a + 1] = h->pinned[a].y; out[3 * a + 2] = h->pinned[a].z; }
         else std::memcpy(out, h->pinned, p * 16);
+    }
+    return SMR_OK;
+}
+
+int smr_download_pos64(smr_handle* h, int nsys, const int* slot_ids, double* pos) {
+    if (!h || nsys < 0 || (nsys && (!slot_ids || !pos))) return SMR_ERR_ARG;
+    { int r = check_batch(h, nsys, slot_ids); if (r) return r; }
+    for (int i = 0; i < nsys; i++) if (!valid_slot(h, slot_ids[i])) return fail(h, SMR_ERR_ARG, "slot %d not active", slot_ids[i]);
+    if (!nsys) return SMR_OK;
+    std::vector<int> desc(3 * nsys);
+    long long p = 0;
+    for (int i = 0; i < nsys; i++) {
+        const SlotState& st = h->hs[slot_ids[i]];
+        desc[i] = st.atom_off; desc[nsys + i] = st.natoms; desc[2 * nsys + i] = (int)p;
+        p += st.natoms;
+    }
+    cudaStream_t s = h->stream;
+    CU(h, cudaMemcpyAsync(h->xfer, desc.data(), desc.size() * 4, cudaMemcpyHostToDevice, s));
+    std::vector<float4> hi((size_t)p);
+    for (int which = 0; which < 2; which++) {
+        if (launch_copy_segments(h->xfer, h->xfer + nsys, h->xfer + 2 * nsys, nsys, which == 0 ? h->pos : h->plo, h->stage, s))
+            return fail(h, SMR_ERR_CUDA, "gather launch failed");
+        CU(h, cudaMemcpyAsync(h->pinned, h->stage, p * 16, cudaMemcpyDeviceToHost, s));
+        int r = wait_stream(h, 600.0);
+        if (r) return r;
+        if (which == 0) std::memcpy(hi.data(), h->pinned, p * 16);
+    }
+    for (long long a = 0; a < p; a++) {
+        pos[3 * a] = (double)hi[a].x + (double)h->pinned[a].x;
+        pos[3 * a + 1] = (double)hi[a].y + (double)h->pinned[a].y;
+        pos[3 * a + 2] = (double)hi[a].z + (double)h->pinned[a].z;
     }
     return SMR_OK;
 }

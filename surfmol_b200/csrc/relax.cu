@@ -8,14 +8,20 @@
 // dynamically.  Per FIRE step a team runs:
 //
 //   A  bonds + hneigh per atom ............ opencl/UFF.cl:141-322 (evalBondsAndHNeigh_UFF)
-//   B  angle / dihedral / inversion rounds  opencl/UFF.cl:326-795 with the assembly of
-//      801-880 replaced by shared-memory adds: the host packs terms into rounds in which
-//      the atoms of each role are distinct, so the adds need no atomics and run in a
-//      fixed order (bitwise reproducible, independent of co-resident systems)
+//   B  angles / dihedrals / inversions ..... opencl/UFF.cl:326-795, assembled (801-880) in
+//      one of three forms, all without atomics and in a fixed order (bitwise reproducible,
+//      independent of co-resident systems):
+//        rounds - host-packed rounds in which the atoms of each role are distinct, added
+//                 straight into the force array between team syncs
+//        gather - all terms at once into a piece buffer, then a per-atom CSR gather
+//        owner  - each atom evaluates the terms it owns (angle apex, inversion centre, both
+//                 central atoms of a dihedral), keeps its neighbours' pieces in registers and
+//                 stores them by bond slot; each atom then gathers over its bond back-slots
 //   C  intramolecular LJ + Coulomb ......... opencl/UFF.cl:57-95, 1595-1665 (1-2 exclusion)
 //      with L lanes per atom splitting the partner loop, combined by shuffles
 //   D  tricubic B-spline grid sample ....... opencl/UFF.cl:1384-1511, 1671-1711, four lanes
-//      per atom, each fetching one x-slice (16 voxels) through the read-only path
+//      per atom, lane k fetching the voxels at z offset k of the 16 (x, y) columns, so the
+//      four lanes of an atom read each 4-voxel column as one contiguous 64 B run
 //   E  FIRE ................................ crates/apps/molengine/src/main.rs:237-277, with
 //      the power / norm sums in FP64 and reduced inside the team
 //
@@ -45,8 +51,8 @@ __host__ __device__ inline size_t red_bytes(int T) { return T > 32 ? size_t(T / 
 // the gather form).
 __host__ __device__ inline size_t team_bytes(int nmax, int nfmax, int T, int form) {
     size_t n = (size_t)nmax;
-    return n * 16 * 6 + n * 64 + align16(n * 4) + align16(n * 8) + red_bytes(T) +
-           (form == FORM_GATHER ? (size_t)nfmax * 16 : 0);
+    return n * 16 * 5 + n * 64 + align16(n * 4) + align16(n * 8) + red_bytes(T) +
+           (form == FORM_GATHER ? (size_t)nfmax * 16 : 0) + (form == FORM_OWNER ? n * 64 : 0);
 }
 
 // Shared memory of one team: one base pointer and the capacity; every array's address is
@@ -59,16 +65,20 @@ struct Smem {
     __device__ __forceinline__ float4* V() const { return (float4*)(base + (size_t)n * 32); }       // velocities
     __device__ __forceinline__ float4* F() const { return (float4*)(base + (size_t)n * 48); }       // forces, w = per-atom energy
     __device__ __forceinline__ float4* Q() const { return (float4*)(base + (size_t)n * 64); }       // R, sqrt(E), Q, H
-    __device__ __forceinline__ float4* PL() const { return (float4*)(base + (size_t)n * 80); }      // grid prefactors x channel scales
-    __device__ __forceinline__ float4* H() const { return (float4*)(base + (size_t)n * 96); }       // hneigh: 4 per atom
-    __device__ __forceinline__ float* Eh() const { return (float*)(base + (size_t)n * 160); }        // bond + NB part of E_atom
-    __device__ __forceinline__ short4* Ng() const { return (short4*)(base + (size_t)n * 160 + align16((size_t)n * 4)); }
+    // hneigh (unit bond vector, 1/length) of bond slot s of atom i at H()[s * n + i]: slot-major,
+    // so lanes handling consecutive atoms touch consecutive words
+    __device__ __forceinline__ float4* H() const { return (float4*)(base + (size_t)n * 80); }
+    __device__ __forceinline__ float4 hget(int h) const { return H()[(h & 3) * n + (h >> 2)]; }   // h = 4 * atom + slot
+    __device__ __forceinline__ float* Eh() const { return (float*)(base + (size_t)n * 144); }        // bond + NB part of E_atom
+    __device__ __forceinline__ short4* Ng() const { return (short4*)(base + (size_t)n * 144 + align16((size_t)n * 4)); }
     __device__ __forceinline__ double* red() const {
-        return (double*)(base + (size_t)n * 160 + align16((size_t)n * 4) + align16((size_t)n * 8));
+        return (double*)(base + (size_t)n * 144 + align16((size_t)n * 4) + align16((size_t)n * 8));
     }
     __device__ __forceinline__ float4* Pc(int T) const {   // gather form: bonded force pieces
         return (float4*)((char*)red() + red_bytes(T));
     }
+    // owner form: piece of the terms owned by atom o on its neighbour in slot s, at Fs()[s * n + o]
+    __device__ __forceinline__ float4* Fs(int T) const { return (float4*)((char*)red() + red_bytes(T)); }
 };
 
 __device__ __forceinline__ Smem carve(char* base, int nmax) { Smem s; s.base = base; s.n = nmax; return s; }
@@ -184,8 +194,8 @@ __device__ __forceinline__ int nb_lanes(int N, int T) {
 
 // ------------------------------------------------------------------ bonded terms (opencl/UFF.cl:326-795)
 // Each returns the force on every atom of the term and the term energy.
-__device__ __forceinline__ float angle_term(const Smem& S, const AngRec& rec, float3& fpi, float3& fpj, float3& fpk) {
-    const float4 qij = S.H()[rec.sl.x], qkj = S.H()[rec.sl.y];
+__device__ __forceinline__ float angle_term(const Smem& S, short4 sl, float4 p, float3& fpi, float3& fpj, float3& fpk) {
+    const float4 qij = S.hget(sl.x), qkj = S.hget(sl.y);
     const float hx = qij.x + qkj.x, hy = qij.y + qkj.y, hz = qij.z + qkj.z;
     float c = 0.5f * (hx * hx + hy * hy + hz * hz - 2.0f);
     c = fminf(fmaxf(c, -1.0f), 1.0f);
@@ -193,7 +203,7 @@ __device__ __forceinline__ float angle_term(const Smem& S, const AngRec& rec, fl
     const float is = (s > 1e-12f) ? 1.0f / s : 0.0f;
     const float c2x = c * c - s * s, c2y = c * s + s * c;
     const float c3x = c2x * c - c2y * s, c3y = c2x * s + c2y * c;
-    const float4 p = rec.p;   // K*(c0, c1, c2, c3); the energy omits the c1 term, the force keeps it
+    // p = K*(c0, c1, c2, c3); the energy omits the c1 term, the force keeps it
     const float E = p.x + p.z * c2x + p.w * c3x;
     const float fm = p.y + p.z * c2y * is * 2.0f + p.w * c3y * is * 3.0f;
     const float fi = fm * qij.w, fk = fm * qkj.w, fic = fi * c, fkc = fk * c;
@@ -204,8 +214,8 @@ __device__ __forceinline__ float angle_term(const Smem& S, const AngRec& rec, fl
     return E;
 }
 
-__device__ __forceinline__ float dihedral_term(const Smem& S, const DihRec& rec, float3& f1, float3& f2, float3& f3, float3& f4) {
-    const float4 q12 = S.H()[rec.sl.x], q32 = S.H()[rec.sl.y], q43 = S.H()[rec.sl.z];
+__device__ __forceinline__ float dihedral_term(const Smem& S, short4 sl, float4 p, float3& f1, float3& f2, float3& f3, float3& f4) {
+    const float4 q12 = S.hget(sl.x), q32 = S.hget(sl.y), q43 = S.hget(sl.z);
     const float3 n123 = make_float3(q12.y * q32.z - q12.z * q32.y, q12.z * q32.x - q12.x * q32.z, q12.x * q32.y - q12.y * q32.x);
     const float3 n234 = make_float3(q43.y * q32.z - q43.z * q32.y, q43.z * q32.x - q43.x * q32.z, q43.x * q32.y - q43.y * q32.x);
     const float a2 = n123.x * n123.x + n123.y * n123.y + n123.z * n123.z;
@@ -216,10 +226,10 @@ __device__ __forceinline__ float dihedral_term(const Smem& S, const DihRec& rec,
     const float cx = (n123.x * n234.x + n123.y * n234.y + n123.z * n234.z) * inv;
     const float cy = -(n123.x * q43.x + n123.y * q43.y + n123.z * q43.z) * inv;
     float nx = cx, ny = cy;
-    const int nn = (int)rec.p.z;
+    const int nn = (int)p.z;
     for (int k = 1; k < nn; k++) { const float t = nx * cx - ny * cy; ny = nx * cy + ny * cx; nx = t; }
-    const float E = rec.p.x * (1.0f + rec.p.y * nx);
-    const float f = -rec.p.x * rec.p.y * rec.p.z * ny;
+    const float E = p.x * (1.0f + p.y * nx);
+    const float f = -p.x * p.y * p.z * ny;
     const float s1 = -f * il2a * q12.w, s4 = f * il2b * q43.w;
     f1 = make_float3(n123.x * s1, n123.y * s1, n123.z * s1);
     f4 = make_float3(n234.x * s4, n234.y * s4, n234.z * s4);
@@ -230,8 +240,8 @@ __device__ __forceinline__ float dihedral_term(const Smem& S, const DihRec& rec,
     return E;
 }
 
-__device__ __forceinline__ float inversion_term(const Smem& S, const InvRec& rec, float3& f1, float3& f2, float3& f3, float3& f4) {
-    const float4 q21 = S.H()[rec.sl.x], q31 = S.H()[rec.sl.y], q41 = S.H()[rec.sl.z];
+__device__ __forceinline__ float inversion_term(const Smem& S, short4 sl, float4 p, float3& f1, float3& f2, float3& f3, float3& f4) {
+    const float4 q21 = S.hget(sl.x), q31 = S.hget(sl.y), q41 = S.hget(sl.z);
     float3 n = make_float3(q21.y * q31.z - q21.z * q31.y, q21.z * q31.x - q21.x * q31.z, q21.x * q31.y - q21.y * q31.x);
     const float nn = n.x * n.x + n.y * n.y + n.z * n.z;
     float il = 0.0f;
@@ -240,7 +250,7 @@ __device__ __forceinline__ float inversion_term(const Smem& S, const InvRec& rec
     float sw = -(n.x * q41.x + n.y * q41.y + n.z * q41.z);
     sw = fminf(fmaxf(sw, -1.0f), 1.0f);
     const float cw = sqrtf(1.0f - sw * sw);
-    const float4 p = rec.p;   // K, c0, c1, c2
+    // p = (K, c0, c1, c2)
     const float E = p.x * (p.y + p.z * cw + p.w * (2.0f * cw * cw - 1.0f));
     const float dEdw = -p.x * (p.z * sw + 2.0f * p.w * (2.0f * sw * cw));
     const float ft = (cw > 1e-7f) ? dEdw / cw : 0.0f;
@@ -254,6 +264,14 @@ __device__ __forceinline__ float inversion_term(const Smem& S, const InvRec& rec
 }
 
 __device__ __forceinline__ void addf(float4& a, const float3& f, float e) { a.x += f.x; a.y += f.y; a.z += f.z; a.w += e; }
+
+// owner form: add a piece to the accumulator of bond slot s (a select chain, no local memory)
+__device__ __forceinline__ void slot_add(float4& s0, float4& s1, float4& s2, float4& s3, int s, const float3& f, float e) {
+    if (s == 0) addf(s0, f, e);
+    else if (s == 1) addf(s1, f, e);
+    else if (s == 2) addf(s2, f, e);
+    else addf(s3, f, e);
+}
 
 // Energy accumulators of the evaluation-only launch (bond, angle, dihedral, inversion, NB, grid).
 template <bool EVAL> struct EAcc { __device__ void add(int, double) {} };
@@ -275,7 +293,7 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
 #pragma unroll
         for (int s = 0; s < 4; s++) {
             const int g = comp(ng, s);
-            if (g < 0) { S.H()[4 * i + s] = make_float4(0.f, 0.f, 0.f, 1e6f); continue; }
+            if (g < 0) { S.H()[s * S.n + i] = make_float4(0.f, 0.f, 0.f, 1e6f); continue; }
             const float4 pj = S.P()[g], lj = S.Lo()[g];
             // difference of the compensated positions: its error is relative to the bond length,
             // not to the absolute coordinate (float positions alone would put ~1e-6 A of rounding
@@ -284,7 +302,7 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
             const float l2 = fmaxf(dx * dx + dy * dy + dz * dz, 1e-16f);
             const float l = sqrtf(l2), il = 1.0f / l;
             const float hx = dx * il, hy = dy * il, hz = dz * il;
-            S.H()[4 * i + s] = make_float4(hx, hy, hz, il);
+            S.H()[s * S.n + i] = make_float4(hx, hy, hz, il);
             const float k = comp(bk, s), dl = l - comp(bl, s), fr = 2.0f * k * dl;
             fx += hx * fr; fy += hy * fr; fz += hz * fr;
             E += k * dl * dl;
@@ -303,7 +321,7 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
             const bool ok = rec.at.x >= 0;
             float3 f1, f2, f3;
             float E = 0.f;
-            if (ok) { E = angle_term(S, rec, f1, f2, f3); acc.add(1, (double)E); }
+            if (ok) { E = angle_term(S, rec.sl, rec.p, f1, f2, f3); acc.add(1, (double)E); }
             const float e3 = E / 3.0f;
             if (ok) addf(S.F()[rec.at.x], f1, e3);
             team_sync<T>();
@@ -317,7 +335,7 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
             const bool ok = rec.at.x >= 0;
             float3 f1, f2, f3, f4;
             float E = 0.f;
-            if (ok) { E = dihedral_term(S, rec, f1, f2, f3, f4); acc.add(2, (double)E); }
+            if (ok) { E = dihedral_term(S, rec.sl, rec.p, f1, f2, f3, f4); acc.add(2, (double)E); }
             const float e4 = 0.25f * E;
             if (ok) addf(S.F()[rec.at.x], f1, e4);
             team_sync<T>();
@@ -333,7 +351,7 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
             const bool ok = rec.at.x >= 0;
             float3 f1, f2, f3, f4;
             float E = 0.f;
-            if (ok) { E = inversion_term(S, rec, f1, f2, f3, f4); acc.add(3, (double)E); }
+            if (ok) { E = inversion_term(S, rec.sl, rec.p, f1, f2, f3, f4); acc.add(3, (double)E); }
             const float e4 = 0.25f * E;
             if (ok) addf(S.F()[rec.at.x], f1, e4);
             team_sync<T>();
@@ -344,6 +362,93 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
             if (ok) addf(S.F()[rec.at.w], f4, e4);
             team_sync<T>();
         }
+    } else if (FORM == FORM_OWNER) {
+        // B (owner): lane o evaluates the terms atom o owns and keeps every piece in registers: its
+        // own, and those of its neighbours by bond slot (angles: apex j, pieces on i and k;
+        // inversions: centre i, pieces on j, k, l; a dihedral i-j-k-l once at j, keeping the
+        // pieces of j and i, and once at k, keeping those of k and l).  Records of one kind are
+        // read row by row, a warp's lanes reading consecutive records.
+        const int abase = TP(atom_off);
+        for (int o0 = 0; o0 < N; o0 += T) {
+            const int o = o0 + rank;
+            const int meta = o < N ? __ldg(a.own_meta + abase + o) : 0;
+            float4 fo = make_float4(0.f, 0.f, 0.f, 0.f), s0 = fo, s1 = fo, s2 = fo, s3 = fo;
+            {
+                const int cnt = meta & 255, m = __reduce_max_sync(FULL, cnt);
+                const int off = TP(own_a_off) + o;
+                for (int r = 0; r < m; r++) {
+                    if (r < cnt) {
+                        const short4 g = __ldg(a.own_geo + off + r * N);
+                        const float4 p = __ldg(a.own_par + off + r * N);
+                        float3 f1, f2, f3;
+                        const float E = angle_term(S, g, p, f1, f2, f3);
+                        acc.add(1, (double)E);
+                        const float e3 = E / 3.0f;
+                        addf(fo, f2, e3);
+                        slot_add(s0, s1, s2, s3, g.x & 3, f1, e3);
+                        slot_add(s0, s1, s2, s3, g.y & 3, f3, e3);
+                    }
+                }
+            }
+            {
+                const int cnt = (meta >> 8) & 255, m = __reduce_max_sync(FULL, cnt);
+                const int off = TP(own_i_off) + o;
+                for (int r = 0; r < m; r++) {
+                    if (r < cnt) {
+                        const short4 g = __ldg(a.own_geo + off + r * N);
+                        const float4 p = __ldg(a.own_par + off + r * N);
+                        float3 f1, f2, f3, f4;
+                        const float E = inversion_term(S, g, p, f1, f2, f3, f4);
+                        acc.add(3, (double)E);
+                        const float e4 = 0.25f * E;
+                        addf(fo, f1, e4);
+                        slot_add(s0, s1, s2, s3, g.x & 3, f2, e4);
+                        slot_add(s0, s1, s2, s3, g.y & 3, f3, e4);
+                        slot_add(s0, s1, s2, s3, g.z & 3, f4, e4);
+                    }
+                }
+            }
+            {
+                const int cnt = (meta >> 16) & 255, m = __reduce_max_sync(FULL, cnt);
+                const int off = TP(own_d_off) + o;
+                for (int r = 0; r < m; r++) {
+                    if (r < cnt) {
+                        const short4 g = __ldg(a.own_geo + off + r * N);
+                        const float4 p = __ldg(a.own_par + off + r * N);
+                        float3 f1, f2, f3, f4;
+                        const float E = dihedral_term(S, g, p, f1, f2, f3, f4);
+                        acc.add(2, 0.5 * (double)E);
+                        const float e4 = 0.25f * E;
+                        const bool at_k = g.w != 0;          // this record is the k half
+                        addf(fo, at_k ? f3 : f2, e4);
+                        slot_add(s0, s1, s2, s3, at_k ? (g.z & 3) : (g.x & 3), at_k ? f4 : f1, e4);
+                    }
+                }
+            }
+            if (o < N) {
+                add4(S.F()[o], fo.x, fo.y, fo.z, fo.w);
+                float4* Fs = S.Fs(T);
+                Fs[o] = s0; Fs[S.n + o] = s1; Fs[2 * S.n + o] = s2; Fs[3 * S.n + o] = s3;
+            }
+        }
+        team_sync<T>();
+        // assembly: atom i adds the piece each neighbour g holds for it, in slot order
+        for (int i = rank; i < N; i += T) {
+            const short4 ng = S.Ng()[i];
+            const int meta = __ldg(a.own_meta + abase + i);
+            float4 f = S.F()[i];
+#pragma unroll
+            for (int s = 0; s < 4; s++) {
+                const int g = comp(ng, s);
+                if (g >= 0) {
+                    const int b = (meta >> (24 + 2 * s)) & 3;
+                    const float4 v = S.Fs(T)[b * S.n + g];
+                    f.x += v.x; f.y += v.y; f.z += v.z; f.w += v.w;
+                }
+            }
+            S.F()[i] = f;
+        }
+        team_sync<T>();
     } else {
         // B (gather): all terms at once, each writing its pieces to its own slots (the reference's
         // fint array, opencl/UFF.cl:801-880), then every atom sums its pieces in a fixed order
@@ -352,7 +457,7 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
             float3 f1, f2, f3, f4;
             if (t < na) {
                 const AngRec rec = load_rec(a.angs + TP(fang_off) + t);
-                const float E = angle_term(S, rec, f1, f2, f3);
+                const float E = angle_term(S, rec.sl, rec.p, f1, f2, f3);
                 acc.add(1, (double)E);
                 const float e3 = E / 3.0f;
                 float4* P = S.Pc(T) + 3 * t;
@@ -360,7 +465,7 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
             } else if (t < na + nd) {
                 const int u = t - na;
                 const DihRec rec = load_rec(a.dihs + TP(fdih_off) + u);
-                const float E = dihedral_term(S, rec, f1, f2, f3, f4);
+                const float E = dihedral_term(S, rec.sl, rec.p, f1, f2, f3, f4);
                 acc.add(2, (double)E);
                 const float e4 = 0.25f * E;
                 float4* P = S.Pc(T) + 3 * na + 4 * u;
@@ -369,7 +474,7 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
             } else {
                 const int u = t - na - nd;
                 const InvRec rec = load_rec(a.invs + TP(finv_off) + u);
-                const float E = inversion_term(S, rec, f1, f2, f3, f4);
+                const float E = inversion_term(S, rec.sl, rec.p, f1, f2, f3, f4);
                 acc.add(3, (double)E);
                 const float e4 = 0.25f * E;
                 float4* P = S.Pc(T) + 3 * na + 4 * nd + 4 * u;
@@ -449,10 +554,11 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
     }
     team_sync<T>();
 
-    // D: substrate grid, 4 lanes per atom (one x-slice of the 4x4x4 stencil each)
+    // D: substrate grid, 4 lanes per atom; lane kz reads the voxels at z offset kz of the 16 (x, y)
+    // columns of the stencil, so the 4 lanes of an atom read each column as one 64 B run
     if (a.has_grid) {
         const GridView& g = a.grid;
-        const int xa = rank & 3;
+        const int kz = rank & 3;
         for (int i0 = 0; i0 < N; i0 += T / 4) {
             const int i = i0 + (rank >> 2);
             float e = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
@@ -469,34 +575,38 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
                     const float tx = ux - ix, ty = uy - iy, tz = uz - iz;
                     float bx[4], dxw[4], by[4], dyw[4], bz[4], dzw[4];
                     bspline(tx, bx, dxw); bspline(ty, by, dyw); bspline(tz, bz, dzw);
-                    const float4 PL = S.PL()[i];
-                    const int xg = imod(ix - 1 + xa, g.nx);
-                    const int y0 = imod(iy - 1, g.ny);
-                    float sE = 0.f, sDy = 0.f, sDz = 0.f;
+                    // atom prefactors (opencl/UFF.cl:1681-1687) times the stored channel scales
+                    const float4 q = S.Q()[i];
+                    const float ej = expf(a.alpha_morse * q.x);
+                    const float PLx = ej * ej * q.y * g.scale[0], PLy = ej * q.y * g.scale[1], PLz = q.z * g.scale[2];
+                    const int x0 = imod(ix - 1, g.nx), y0 = imod(iy - 1, g.ny);
+                    const size_t zoff = (size_t)(iz - 1 + kz);
+                    float sE = 0.f, sX = 0.f, sY = 0.f;
 #pragma unroll
-                    for (int b = 0; b < 4; b++) {
-                        int yg = y0 + b;
-                        if (yg >= g.ny) yg -= g.ny;
-                        const size_t base = (size_t)(iz - 1) + (size_t)g.nz * ((size_t)yg + (size_t)g.ny * (size_t)xg);
-                        float pz = 0.f, dz = 0.f;
+                    for (int ax = 0; ax < 4; ax++) {
+                        int xg = x0 + ax;
+                        if (xg >= g.nx) xg -= g.nx;
+                        float pE = 0.f, pY = 0.f;
 #pragma unroll
-                        for (int k = 0; k < 4; k++) {
-                            const float4 v = load_voxel<GDT>(g.data, base + k);
-                            const float cs = PL.x * v.x + PL.y * v.y + PL.z * v.z + PL.w * v.w;
-                            pz += bz[k] * cs; dz += dzw[k] * cs;
+                        for (int b = 0; b < 4; b++) {
+                            int yg = y0 + b;
+                            if (yg >= g.ny) yg -= g.ny;
+                            const float4 v = load_voxel<GDT>(g.data, zoff + (size_t)g.nz * ((size_t)yg + (size_t)g.ny * (size_t)xg));
+                            const float cs = PLx * v.x + PLy * v.y + PLz * v.z;
+                            pE += by[b] * cs; pY += dyw[b] * cs;
                         }
-                        sE += by[b] * pz; sDy += dyw[b] * pz; sDz += by[b] * dz;
+                        sE += bx[ax] * pE; sX += dxw[ax] * pE; sY += bx[ax] * pY;
                     }
-                    const float bxa = comp(make_float4(bx[0], bx[1], bx[2], bx[3]), xa);
-                    const float dxa = comp(make_float4(dxw[0], dxw[1], dxw[2], dxw[3]), xa);
-                    e = bxa * sE; gx = dxa * sE; gy = bxa * sDy; gz = bxa * sDz;
+                    const float bzk = comp(make_float4(bz[0], bz[1], bz[2], bz[3]), kz);
+                    const float dzk = comp(make_float4(dzw[0], dzw[1], dzw[2], dzw[3]), kz);
+                    e = bzk * sE; gx = bzk * sX; gy = bzk * sY; gz = dzk * sE;
                 }
             }
             e += __shfl_xor_sync(FULL, e, 1); gx += __shfl_xor_sync(FULL, gx, 1);
             gy += __shfl_xor_sync(FULL, gy, 1); gz += __shfl_xor_sync(FULL, gz, 1);
             e += __shfl_xor_sync(FULL, e, 2); gx += __shfl_xor_sync(FULL, gx, 2);
             gy += __shfl_xor_sync(FULL, gy, 2); gz += __shfl_xor_sync(FULL, gz, 2);
-            if (xa == 0 && i < N) {
+            if (kz == 0 && i < N) {
                 add4(S.F()[i], -gx * g.inv_step[0], -gy * g.inv_step[1], -gz * g.inv_step[2], e);
                 acc.add(5, (double)e);
             }
@@ -525,13 +635,11 @@ __device__ void run_system(const KernelArgs& a, const Smem& S, int w, int rank) 
     const int N = st.natoms;
     for (int i = rank; i < N; i += T) {
         S.P()[i] = a.pos[st.atom_off + i];
-        S.Lo()[i] = (EVAL || fresh) ? make_float4(0.f, 0.f, 0.f, 0.f) : a.plo[st.atom_off + i];
+        S.Lo()[i] = a.plo[st.atom_off + i];     // zeroed whenever positions are set
         S.V()[i] = (EVAL || fresh) ? make_float4(0.f, 0.f, 0.f, 0.f) : a.vel[st.atom_off + i];
         const float4 q = __ldg(a.req + tp_atom_off + i);
         S.Q()[i] = q;
         S.Ng()[i] = a.neigh[tp_atom_off + i];
-        const float ej = expf(a.alpha_morse * q.x);
-        S.PL()[i] = make_float4(ej * ej * q.y * a.grid.scale[0], ej * q.y * a.grid.scale[1], q.z * a.grid.scale[2], 0.f);
     }
     team_sync<T>();
 
@@ -640,7 +748,9 @@ __device__ void run_system(const KernelArgs& a, const Smem& S, int w, int rank) 
 }
 
 template <int T, int GDT, bool EVAL, int FORM>
-__global__ void __launch_bounds__(T == 32 ? 128 : T, T == 32 ? 7 : 1)
+// warp teams: 4 per block; a 40-atom system's shared memory allows 7 blocks per SM in the rounds
+// and gather forms and 6 in the owner form (slot pieces), which leaves it 85 registers
+__global__ void __launch_bounds__(T == 32 ? 128 : T, T == 32 ? (FORM == FORM_OWNER ? 6 : 7) : 1)
 relax_kernel(const KernelArgs a) {
     extern __shared__ __align__(16) char smem[];
     const int team = (T == 32) ? (threadIdx.x >> 5) : 0;
@@ -738,8 +848,12 @@ int launch_copy_segments(const int* d_src_off, const int* d_len, const int* d_ds
 int launch_relax(const KernelArgs& a, int team, int form, int eval_only, cudaStream_t s, int num_sms, long long* launches) {
     if (a.nwork <= 0) return 0;
     int r;
-    if (eval_only) r = form == FORM_GATHER ? launch_dtype<true, FORM_GATHER>(a, team, s, num_sms) : launch_dtype<true, FORM_ROUNDS>(a, team, s, num_sms);
-    else r = form == FORM_GATHER ? launch_dtype<false, FORM_GATHER>(a, team, s, num_sms) : launch_dtype<false, FORM_ROUNDS>(a, team, s, num_sms);
+    if (eval_only) r = form == FORM_GATHER ? launch_dtype<true, FORM_GATHER>(a, team, s, num_sms)
+                     : form == FORM_OWNER ? launch_dtype<true, FORM_OWNER>(a, team, s, num_sms)
+                                          : launch_dtype<true, FORM_ROUNDS>(a, team, s, num_sms);
+    else r = form == FORM_GATHER ? launch_dtype<false, FORM_GATHER>(a, team, s, num_sms)
+           : form == FORM_OWNER ? launch_dtype<false, FORM_OWNER>(a, team, s, num_sms)
+                                : launch_dtype<false, FORM_ROUNDS>(a, team, s, num_sms);
     if (launches && r == 0) (*launches)++;
     return r;
 }

@@ -40,8 +40,15 @@ struct TopoDev {
     int nang, ndih, ninv;
     int npieces;
     int a2f_off;                  // into the piece-index arena; per atom (start, count) at atom_off
-    int pad[2];
+    // owner form: every term is evaluated by an atom whose neighbour slots cover the term's
+    // other atoms (angles by the apex, inversions by the centre, each dihedral twice: by j for
+    // (i, j) and by k for (k, l)).  Records of one kind are stored by row: row r of owner o at
+    // off + r * natoms + o, so a warp's lanes read consecutive records.
+    int own_a_off, own_i_off, own_d_off;   // into the owner record arenas (geo + par)
+    int own_ok;                   // 0: the topology cannot run the owner form (rounds instead)
+    int pad[3];
 };
+static_assert(sizeof(TopoDev) == 96, "TopoDev size");
 
 struct SlotState {
     int topo;                     // topology id
@@ -91,6 +98,9 @@ struct KernelArgs {
     int nfmax;                    // gather form: max pieces of a system in this launch
     const int2* a2f;              // gather form: per atom (first piece-index entry, count)
     const int* a2f_idx;           // gather form: piece indices
+    const short4* own_geo;        // owner form: hneigh indices (+ dihedral half in .w)
+    const float4* own_par;        // owner form: term parameters
+    const int* own_meta;          // owner form, per atom: n_ang | n_inv << 8 | n_dih << 16 | back slots << 24
 };
 
 // ---- host topology (topology.cpp)
@@ -112,6 +122,14 @@ struct PackedTerms {
     int ang_rounds = 0, dih_rounds = 0, inv_rounds = 0;
 };
 
+struct OwnerTerms {                // owner form of one topology
+    std::vector<short4> geo;       // angle rows, then inversion rows, then dihedral rows
+    std::vector<float4> par;
+    std::vector<int> meta;         // per atom
+    int rows_a = 0, rows_i = 0, rows_d = 0;
+    bool ok = false;
+};
+
 struct FlatTerms {                 // gather form of one topology
     std::vector<AngRec> ang; std::vector<DihRec> dih; std::vector<InvRec> inv;
     std::vector<int2> a2f;         // per atom (start into idx, count)
@@ -127,10 +145,11 @@ int build_desc_topology(int natoms, const double* req, const int* neighs, const 
                         int ninv, const int* invs, const double* invp, HostTopo& T, char* err, int errlen);
 void pack_rounds(const HostTopo& T, int team, PackedTerms& out);
 void flat_terms(const HostTopo& T, FlatTerms& out);
+bool owner_terms(const HostTopo& T, OwnerTerms& out);
 const char* type_name(int id);
 
 // relax.cu
-enum KernelForm { FORM_ROUNDS = 0, FORM_GATHER = 1 };
+enum KernelForm { FORM_ROUNDS = 0, FORM_GATHER = 1, FORM_OWNER = 2 };
 int launch_relax(const KernelArgs& a, int team, int form, int eval_only, cudaStream_t s, int num_sms, long long* launches);
 size_t team_smem_bytes(int nmax, int nfmax, int team, int form);
 

@@ -497,6 +497,74 @@ void flat_terms(const HostTopo& T, FlatTerms& F) {
     }
 }
 
+// Owner form: each term goes to an atom whose neighbour slots hold all its other atoms, so the
+// owner keeps its own piece and the pieces of its neighbours in registers and a per-atom gather
+// over the bond back-slots assembles them (the reference's a2f assembly, opencl/UFF.cl:801-880,
+// with the piece buffer indexed by bond slot).  Angles go to the apex j, inversions to the centre
+// i, and each dihedral i-j-k-l twice: to j (keeping the pieces of j and i) and to k (k and l).
+// Needs symmetric neighbour lists (the back slot of every bond) and at most 255 terms of a kind
+// per owner; otherwise ok = false and the caller uses another form.
+bool owner_terms(const HostTopo& T, OwnerTerms& O) {
+    const int n = T.n;
+    const int na = (int)T.angs.size() / 3, nd = (int)T.dihs.size() / 4, ni = (int)T.invs.size() / 4;
+    O = OwnerTerms{};
+    O.meta.assign(n, 0);
+    std::vector<int> back(4 * (size_t)n, 0);
+    for (int i = 0; i < n; i++)
+        for (int s = 0; s < 4; s++) {
+            const int g = T.neighs[4 * i + s];
+            if (g < 0) continue;
+            int b = -1;
+            for (int t = 0; t < 4; t++) if (T.neighs[4 * g + t] == i) b = t;
+            if (b < 0) return false;
+            back[4 * i + s] = b;
+        }
+    std::vector<std::vector<std::pair<short4, float4>>> A(n), I(n), D(n);
+    for (int t = 0; t < na; t++) {
+        const int* a = &T.angs[3 * t]; const int* s = &T.ang_ngs[2 * t]; const double* p = &T.angp[5 * t];
+        if (s[0] >> 2 != a[1] || s[1] >> 2 != a[1]) return false;
+        A[a[1]].push_back({make_short4((short)s[0], (short)s[1], 0, 0),
+                           make_float4((float)(p[0] * p[1]), (float)(p[0] * p[2]), (float)(p[0] * p[3]), (float)(p[0] * p[4]))});
+    }
+    for (int t = 0; t < ni; t++) {
+        const int* a = &T.invs[4 * t]; const int* s = &T.inv_ngs[3 * t]; const double* p = &T.invp[4 * t];
+        if (s[0] >> 2 != a[0] || s[1] >> 2 != a[0] || s[2] >> 2 != a[0]) return false;
+        I[a[0]].push_back({make_short4((short)s[0], (short)s[1], (short)s[2], 0),
+                           make_float4((float)p[0], (float)p[1], (float)p[2], (float)p[3])});
+    }
+    for (int t = 0; t < nd; t++) {
+        const int* a = &T.dihs[4 * t]; const int* s = &T.dih_ngs[3 * t]; const double* p = &T.dihp[3 * t];
+        if (s[0] >> 2 != a[1] || s[1] >> 2 != a[1] || s[2] >> 2 != a[2]) return false;
+        const float4 pp = make_float4((float)p[0], (float)p[1], (float)p[2], 0.f);
+        D[a[1]].push_back({make_short4((short)s[0], (short)s[1], (short)s[2], 0), pp});
+        D[a[2]].push_back({make_short4((short)s[0], (short)s[1], (short)s[2], 1), pp});
+    }
+    for (int i = 0; i < n; i++) {
+        if (A[i].size() > 255 || I[i].size() > 255 || D[i].size() > 255) return false;
+        O.rows_a = std::max(O.rows_a, (int)A[i].size());
+        O.rows_i = std::max(O.rows_i, (int)I[i].size());
+        O.rows_d = std::max(O.rows_d, (int)D[i].size());
+        int m = (int)A[i].size() | ((int)I[i].size() << 8) | ((int)D[i].size() << 16);
+        for (int s = 0; s < 4; s++) m |= back[4 * i + s] << (24 + 2 * s);
+        O.meta[i] = m;
+    }
+    const size_t rows = (size_t)O.rows_a + O.rows_i + O.rows_d;
+    O.geo.assign(rows * n, make_short4(0, 0, 0, 0));
+    O.par.assign(rows * n, make_float4(0.f, 0.f, 0.f, 0.f));
+    auto put = [&](const std::vector<std::vector<std::pair<short4, float4>>>& L, size_t row0) {
+        for (int i = 0; i < n; i++)
+            for (size_t r = 0; r < L[i].size(); r++) {
+                O.geo[(row0 + r) * n + i] = L[i][r].first;
+                O.par[(row0 + r) * n + i] = L[i][r].second;
+            }
+    };
+    put(A, 0);
+    put(I, O.rows_a);
+    put(D, (size_t)O.rows_a + O.rows_i);
+    O.ok = true;
+    return true;
+}
+
 void pack_rounds(const HostTopo& T, int team, PackedTerms& P) {
     const int na = (int)T.angs.size() / 3, nd = (int)T.dihs.size() / 4, ni = (int)T.invs.size() / 4;
     std::vector<int> ro, po, oo;

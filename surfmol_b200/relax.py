@@ -17,6 +17,7 @@ from . import _native as N
 
 GRID_F32, GRID_F16, GRID_BF16 = 0, 1, 2
 MODE_BATCHED, MODE_PLAIN = 0, 1
+FORM_ROUNDS, FORM_GATHER, FORM_OWNER = 0, 1, 2
 ST_RUNNING, ST_CONVERGED, ST_MAXSTEPS, ST_NONFINITE = 0, 1, 2, 3
 E_TOTAL, E_BOND, E_ANGLE, E_DIH, E_INV, E_NB, E_GRID = range(7)
 
@@ -198,20 +199,21 @@ class RelaxMulti:
         self._chk(self.L.smr_get_schedule(self.h, C.byref(a), C.byref(b), C.byref(c)), "smr_get_schedule")
         return a.value, b.value, c.value
 
-    def set_stages(self, starts, teams, eval_form=0):
-        """Multi-stage schedule: stage k runs FIRE steps [starts[k], starts[k+1]); stage 0 in the
-        rounds form, later stages in the gather form with teams[k] threads (0: by size)."""
-        st, tm = _i(starts), _i(teams)
-        if len(st) != len(tm):
-            raise ValueError("starts and teams differ in length")
-        self._chk(self.L.smr_set_stages(self.h, len(st), _p(st, N.IP), _p(tm, N.IP), eval_form), "smr_set_stages")
+    def set_stages(self, starts, forms, teams, eval_form=FORM_ROUNDS):
+        """Multi-stage schedule: stage k runs FIRE steps [starts[k], starts[k+1]) in forms[k]
+        (FORM_ROUNDS / FORM_GATHER / FORM_OWNER) with teams[k] threads per system (0: by size)."""
+        st, fm, tm = _i(starts), _i(forms), _i(teams)
+        if not (len(st) == len(fm) == len(tm)):
+            raise ValueError("starts, forms and teams differ in length")
+        self._chk(self.L.smr_set_stages(self.h, len(st), _p(st, N.IP), _p(fm, N.IP), _p(tm, N.IP), eval_form),
+                  "smr_set_stages")
 
     def get_stages(self):
         n = C.c_int(16)
-        st = np.zeros(16, np.int32)
-        tm = np.zeros(16, np.int32)
-        self._chk(self.L.smr_get_stages(self.h, C.byref(n), _p(st, N.IP), _p(tm, N.IP)), "smr_get_stages")
-        return st[:n.value].tolist(), tm[:n.value].tolist()
+        st, fm, tm = (np.zeros(16, np.int32) for _ in range(3))
+        self._chk(self.L.smr_get_stages(self.h, C.byref(n), _p(st, N.IP), _p(fm, N.IP), _p(tm, N.IP)), "smr_get_stages")
+        k = n.value
+        return st[:k].tolist(), fm[:k].tolist(), tm[:k].tolist()
 
     def set_team_size(self, max_atoms, threads):
         self._chk(self.L.smr_set_team_size(self.h, max_atoms, threads), "smr_set_team_size")
@@ -336,6 +338,14 @@ class RelaxMulti:
                                       _p(steps, N.IP), _p(status, N.IP)), "smr_download")
         return dict(pos=self._split(slots, P, 3) if pos else None, forces=self._split(slots, F, 4) if forces else None,
                     energy=E[:, 0], steps=steps, status=status)
+
+    def download_pos64(self, slots):
+        """Positions at full precision (float + its accumulated rounding error), list of (n, 3) float64."""
+        slots = _i(slots)
+        tot = sum(self.natoms_of[int(s)] for s in slots)
+        P = np.zeros((tot, 3), np.float64)
+        self._chk(self.L.smr_download_pos64(self.h, len(slots), _p(slots, N.IP), _p(P, N.DP)), "smr_download_pos64")
+        return self._split(slots, P, 3)
 
     def download_pos_multi(self, slots):
         return self.download(slots, pos=True, forces=False)["pos"]

@@ -70,9 +70,12 @@ def test_pentacene_bonded(R, oracle):
 
 
 @pytest.mark.parametrize("n,team,form", [(40, 32, 0), (40, 64, 0), (21, 32, 0), (90, 64, 0), (90, 128, 0), (250, 128, 0),
-                                         (250, 256, 0), (600, 512, 0), (40, 128, 1), (40, 32, 1), (90, 256, 1), (250, 512, 1)])
+                                         (250, 256, 0), (600, 512, 0), (40, 128, 1), (40, 32, 1), (90, 256, 1), (250, 512, 1),
+                                         (40, 32, 2), (21, 32, 2), (90, 32, 2), (90, 64, 2), (250, 128, 2), (600, 512, 2),
+                                         (40, 256, 2)])
 def test_forces_energies_match_oracle(R, oracle, slab_grid, n, team, form):
-    """Rounds form (bonded terms in conflict-free rounds) and gather form (pieces + per-atom sums)."""
+    """Rounds form (bonded terms in conflict-free rounds), gather form (pieces + per-atom sums) and
+    owner form (terms evaluated by their owner atom, pieces gathered over bond back-slots)."""
     slab, g = slab_grid
     R.set_team_size(1 << 20, team)
     R.set_schedule(0, team, form)
@@ -140,8 +143,13 @@ def test_relaxed_structure_is_oracle_minimum(R, oracle, slab_grid):
     out = R.download(s)
     assert out["status"][0] == 1, out
     S = oracle.System.from_molecule(Z, P, q)
-    Fo, _, Eco = S.eval(out["pos"][0].astype(np.float64), oracle.Grid(g["coef"], g["p0"], g["step"]))
-    assert np.sqrt((Fo ** 2).sum(1)).max() < 1e-3 + 1e-4 * max(1.0, np.abs(Fo).max()) + 2e-4
+    # at the float32 positions alone one ulp of a stiff bond moves |F| by ~1e-3 eV/A; at the
+    # compensated positions the oracle sees the state FIRE converged
+    Fo, _, Eco = S.eval(R.download_pos64(s)[0], oracle.Grid(g["coef"], g["p0"], g["step"]))
+    # the convergence test uses the forces before the step's last move (relax_fire order,
+    # crates/apps/molengine/src/main.rs:242-275), so the returned structure is one move further on
+    assert np.sqrt((out["forces"][0][:, :3].astype(np.float64) ** 2).sum(1)).max() < 1e-3
+    assert np.sqrt((Fo ** 2).sum(1)).max() < 3e-3
     ro = S.relax(P.astype(np.float32).astype(np.float64), oracle.Grid(g["coef"], g["p0"], g["step"]), max_steps=2000,
                  fconv=1e-3)
     assert ro["conv"]
@@ -173,19 +181,19 @@ def test_batched_plain_alone_mix_bitwise(R, oracle, slab_grid):
     assert mix["steps"][2] == alone["steps"][0] == plain["steps"][0] == 150
 
 
-@pytest.mark.parametrize("starts,teams", [([0, 60], [0, 128]), ([0, 1], [0, 256]), ([0, 60], [0, 32]),
-                                          ([0, 30, 80], [0, 64, 256])])
-def test_staged_schedule_bitwise(R, oracle, slab_grid, starts, teams):
-    """Rounds form until starts[1] steps, gather form stages after: batched, plain and chunked-alone runs
-    agree bit for bit (chunk ends fall inside and on stage boundaries), and the relaxed structure is an
-    oracle minimum."""
+@pytest.mark.parametrize("starts,forms,teams", [([0, 60], [0, 1], [0, 128]), ([0, 1], [0, 1], [0, 256]),
+                                                ([0, 60], [0, 1], [0, 32]), ([0, 30, 80], [0, 1, 1], [0, 64, 256]),
+                                                ([0, 50, 90], [2, 0, 2], [0, 0, 64]), ([0, 70], [2, 1], [0, 128])])
+def test_staged_schedule_bitwise(R, oracle, slab_grid, starts, forms, teams):
+    """Stages of different forms and team sizes: batched, plain and chunked-alone runs agree bit for bit
+    (chunk ends fall inside and on stage boundaries), and the relaxed structure is an oracle minimum."""
     slab, g = slab_grid
-    if len(starts) == 2:
+    if forms == [0, 1]:
         R.set_schedule(starts[1], teams[1], 0)
         assert R.get_schedule() == (starts[1], teams[1], 0)
     else:
-        R.set_stages(starts, teams)
-    assert R.get_stages() == (starts, teams)
+        R.set_stages(starts, forms, teams)
+    assert R.get_stages() == (starts, forms, teams)
     rng = np.random.default_rng(21 + starts[1])
     mols = [molecule_on_slab(rng, n, slab) for n in (40, 30, 120)]
     tids = [R.add_molecule(Z, P, q) for Z, P, q in mols]
@@ -209,10 +217,17 @@ def test_staged_schedule_bitwise(R, oracle, slab_grid, starts, teams):
     out = R.download(d)
     assert out["status"][0] in (1, 2)
     S = oracle.System.from_molecule(*mols[1])
-    Fo, _, _ = S.eval(out["pos"][0].astype(np.float64), oracle.Grid(g["coef"], g["p0"], g["step"]))
-    assert force_err(out["forces"][0], Fo) < 1e-3          # forces of the last step were taken 1 move earlier
+    P64 = R.download_pos64(d)[0]                           # the compensated positions FIRE converged
+    assert np.abs(P64 - out["pos"][0]).max() < 1e-5
+    Fo, _, _ = S.eval(P64, oracle.Grid(g["coef"], g["p0"], g["step"]))
+    Fe, _ = R.eval_forces(d)                               # forces at the final positions
+    assert force_err(Fe[0], Fo) < F_RTOL
     if out["status"][0] == 1:
-        assert np.sqrt((Fo ** 2).sum(1)).max() < 1e-3 + 3e-4
+        # relax_fire tests the forces of the step and then still moves the atoms
+        # (crates/apps/molengine/src/main.rs:242-275): the reported forces are below fconv, the
+        # returned structure is one FIRE move further on
+        assert np.sqrt((out["forces"][0][:, :3].astype(np.float64) ** 2).sum(1)).max() < 1e-3
+        assert np.sqrt((Fo ** 2).sum(1)).max() < 3e-3
     R.remove_systems(d)
     R.set_schedule(0, 0, 0)
 
