@@ -324,13 +324,183 @@ def run_ours(args, ws, rank, local):
     return 0
 
 
+# ---------------------------------------------------------------------------------------- ragged workload
+RAGGED = dict(nsys=16384, nmin=20, nmax=400, rcut=10.0, fconv=1e-4, max_steps=3000, tune_sample=1024)
+
+
+def ragged_desc(w, nsys):
+    g = w.grid
+    return (f"ragged: {nsys} distinct planar C/H/N/O molecules, atoms log-uniform in [{RAGGED['nmin']}, {RAGGED['nmax']}], "
+            f"over NaCl(100) 3 layers 8x8 cells, fp32 B-spline grid {g.nx}x{g.ny}x{g.nz} at 0.1 A; intramolecular "
+            f"cutoff {RAGGED['rcut']} A; FIRE to max|F|<{RAGGED['fconv']} or {RAGGED['max_steps']} steps")
+
+
+def ragged_workload(seed, nsys):
+    from surfmol_b200 import synth
+    return synth.ragged(seed, nsys, RAGGED["nmin"], RAGGED["nmax"], ncell=8, nlayers=3, nz=161,
+                        workers=min(32, os.cpu_count() or 1))
+
+
+def run_reference_ragged(args, ws, rank):
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    nsys = args.nsys or RAGGED["nsys"]
+    w = ragged_workload(SEED, nsys)
+    slab, g = w.slab, w.grid
+    coef = O.build_grid_fast(slab.ions, slab.req(), slab.Lx, slab.Ly, g.nx, g.ny, g.nz, g.p0, g.step)
+    grid = O.Grid(coef.astype(np.float32), g.p0, g.step)
+    threads = os.cpu_count() or 1
+    sample = max(threads, args.ref_sample)
+    nb = dict(rdamp=1.0, alpha=1.5, rcut=RAGGED["rcut"])
+    fire = dict(FIRE, fconv=RAGGED["fconv"])
+
+    def one(k0):
+        idx = [(k0 + i) % nsys for i in range(sample)]
+        systems = [O.System.from_molecule(w.Z[i], w.pos[i], w.q[i]) for i in idx]
+        t = time.perf_counter()
+        r = O.relax_batch(systems, [w.pos[i] for i in idx], grid, max_steps=RAGGED["max_steps"], nthreads=threads, nb=nb, **fire)
+        return time.perf_counter() - t, r, sum(len(w.Z[i]) for i in idx)
+
+    for k in range(args.warmup):
+        one(k * sample)
+    tt, conv = 0.0, 0
+    for k in range(args.steps):
+        dt, r, _ = one((args.warmup + k) * sample)
+        tt += dt
+        conv += int(r["conv"].sum())
+    v = sample * args.steps / tt
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "systems/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * tt / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": ragged_desc(w, nsys), "sample_per_step": sample, "converged_fraction": conv / (sample * args.steps)},
+            "cpu_baseline": {"value": v, "unit": "systems/s", "cores": threads, "kind": "port",
+                             "sample": f"{sample} molecules of the workload per step, FP64 oracle, OpenMP one system per thread"},
+            "e2e": {"value": v, "unit": "systems/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ragged(args, ws, rank, local):
+    nsys = args.nsys or RAGGED["nsys"]
+    t0 = time.perf_counter()
+    w = ragged_workload(SEED + 7919 * rank, nsys)          # generated before any CUDA work (spawned pool)
+    tgen = time.perf_counter() - t0
+    import torch
+    from surfmol_b200 import RelaxMulti
+    from surfmol_b200.autotune import Autotuner, TuneResult
+    torch.cuda.set_device(local)
+    slab, g = w.slab, w.grid
+    natoms = np.array([len(z) for z in w.Z])
+    fire = dict(FIRE, fconv=RAGGED["fconv"])
+    max_steps = args.max_steps if args.max_steps != MAX_STEPS else RAGGED["max_steps"]
+
+    def make_handle(ms, ma):
+        R = RelaxMulti(max_systems=ms, max_atoms=ma, device=local)
+        R.set_nb(rdamp=1.0, alpha_morse=1.5, rcut=RAGGED["rcut"])
+        R.build_grid(slab.ions, slab.req()[:, :2], slab.Lx, slab.Ly, g.nx, g.ny, g.nz, g.p0, g.step, alpha_morse=1.5, npbc=1)
+        return R
+
+    t0 = time.perf_counter()
+    if args.no_tune:
+        tune = None
+    else:
+        rng = np.random.default_rng(SEED)
+        pick = np.sort(rng.choice(nsys, size=min(nsys, RAGGED["tune_sample"]), replace=False))
+        tune = Autotuner(make_handle, fire, probe_steps=100, max_steps=max_steps, max_probe_systems=4096).tune(
+            [w.Z[i] for i in pick], [w.pos[i] for i in pick], [w.q[i] for i in pick], full_count=nsys)
+    ttune = time.perf_counter() - t0
+    R = make_handle(nsys, int(natoms.sum()))
+    if tune is not None:
+        tune.apply(R)
+    t0 = time.perf_counter()
+    tids = R.add_molecules(w.Z, w.pos, w.q)
+    tadd = time.perf_counter() - t0
+    slots = R.add_systems(tids, w.pos)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+
+    def step():
+        R.set_positions(slots, w.pos)
+        R.reset_fire(slots)
+        flush.zero_()
+        torch.cuda.synchronize()
+        R.run_fire(max_steps, step_budget=max_steps, **fire)
+        return R.last_timing()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    dev_ms, launches, atom_steps, conv, steps_all = 0.0, 0, 0, 0, []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            ms, nl = step()
+            dev_ms += ms
+            launches += nl
+            out = R.download(slots, pos=False, forces=False)
+            atom_steps += int((out["steps"] * natoms).sum())
+            conv += int((out["status"] == 1).sum())
+            steps_all += list(out["steps"])
+        torch.cuda.synchronize()
+    dev_ms = barrier_max(ws, dev_ms)
+    ms_step = dev_ms / args.steps
+    value = ws * nsys / (ms_step * 1e-3)
+    e2e_k = max(1, min(args.steps, 2))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_k):
+        R.set_positions(slots, w.pos)
+        R.reset_fire(slots)
+        R.run_fire(max_steps, step_budget=max_steps, **fire)
+        R.download(slots, pos=True, forces=False)
+    t_e2e = barrier_max(ws, time.perf_counter() - t0)
+    hbm, peak_kind = peaks()
+    achieved = 1024.0 * atom_steps / args.steps / (ms_step * 1e-3) / 1e9
+    line = {"metric": METRIC, "value": value, "unit": "systems/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": ragged_desc(w, nsys), "nsys_per_gpu": nsys, "atoms_total": int(natoms.sum()),
+                       "atoms_mean": float(natoms.mean()), "parallelism": f"systems sharded over {ws} GPU(s), no collective",
+                       "l2": "flushed (256 MB write) before every timed step", "converged_fraction": conv / (nsys * args.steps),
+                       "fire_steps_p50": float(np.percentile(steps_all, 50)), "fire_steps_p99": float(np.percentile(steps_all, 99)),
+                       "host_s": {"generate": round(tgen, 2), "autotune": round(ttune, 2), "add_molecules": round(tadd, 2)},
+                       "tuned": None if tune is None else {"team_by_class": tune.team_by_class, "form0": tune.form0,
+                                                            "nb_lanes": tune.nb_lanes, "stages": tune.stages}},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                         "traffic": None, "peak_source": peak_kind,
+                         "algorithmic_bytes": "1024 B per atom-step (64 float4 grid voxels), state resident in shared memory"},
+            "e2e": {"value": ws * nsys * e2e_k / t_e2e, "unit": "systems/s", "h2d_bytes_per_step": int(16 * natoms.sum() + 76 * nsys),
+                    "d2h_bytes_per_step": int(16 * natoms.sum() + 128 * nsys)},
+            "gpu_launches": launches, "clocks": clk.summary()}
+    R.finish()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ragged_dist(args):
+    # the workload is generated in a spawned pool before CUDA and before the process group exists
+    ws, rank, local = int(os.environ["WORLD_SIZE"]), int(os.environ["RANK"]), int(os.environ.get("LOCAL_RANK", "0"))
+    import datetime
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
+    r = run_ragged(args, ws, rank, local)
+    dist.barrier()
+    dist.destroy_process_group()
+    return r
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--nsys", type=int, default=4096)
+    ap.add_argument("--workload", default="uniform", choices=["uniform", "ragged"],
+                    help="uniform: 4096 replicas of the 40-atom molecule (default); ragged: 16384 molecules of 20-400 atoms")
+    ap.add_argument("--nsys", type=int, default=0, help="systems per GPU (0: the workload's default)")
+    ap.add_argument("--no-tune", action="store_true", help="ragged: skip the autotuner (library defaults)")
     ap.add_argument("--ref-sample", type=int, default=64)
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -341,7 +511,18 @@ def main():
     if args.impl == "reference":
         ws = int(os.environ.get("WORLD_SIZE", "1"))
         rank = int(os.environ.get("RANK", "0"))
+        if args.workload == "ragged":
+            return run_reference_ragged(args, ws, rank)
+        args.nsys = args.nsys or 4096
         return run_reference(args, ws, rank)
+    if args.workload == "ragged":
+        ws = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        if ws > 1:
+            return run_ragged_dist(args)
+        return run_ragged(args, ws, rank, local)
+    args.nsys = args.nsys or 4096
     ws, rank, local = dist_init()
     return run_ours(args, ws, rank, local)
 

@@ -155,6 +155,11 @@ int smr_convert_grid(smr_handle* h, int dtype);
 /* Molecule -> bonds by cutoff, UFF typing, terms and parameters (host, native), upload. */
 int smr_add_molecule(smr_handle* h, int natoms, const int* Z, const double* pos, const double* charges,
                      double bond_cut, int* topo_id);
+/* Batch form of smr_add_molecule: nmol molecules with natoms[i] atoms each, their Z / pos (x 3) /
+ * charges (may be null) concatenated; typing and term packing run on all host cores, the device
+ * upload happens once.  topo_ids: nmol ids out.  On error nothing is added. */
+int smr_add_molecules(smr_handle* h, int nmol, const int* natoms, const int* Z, const double* pos, const double* charges,
+                      double bond_cut, int* topo_ids);
 int smr_add_topology(smr_handle* h, const smr_topology_desc* d, int* topo_id);
 /* counts[6] = natoms, nbonds, nang, ndih, ninv, type-rounds (schedule length) */
 int smr_topology_counts(smr_handle* h, int topo_id, int counts[6]);
@@ -251,6 +256,13 @@ int smr_get_schedule(smr_handle* h, int* switch_step, int* latency_team, int* ev
 /* Team configuration of the persistent kernel: threads per system team for systems of
  * up to n atoms (0 = library default / autotuned). */
 int smr_set_team_size(smr_handle* h, int max_atoms, int threads);
+
+/* Tuning knobs (no counterpart in the reference; set by the autotuner or by hand):
+ *   SMR_TUNE_NB_LANES  lanes per atom splitting the intramolecular NB partner loop
+ *                      (1, 2, 4, 8, 16, 32; 0 = chosen from the system size and team) */
+#define SMR_TUNE_NB_LANES 1
+int smr_set_tuning(smr_handle* h, int key, int value);
+int smr_get_tuning(smr_handle* h, int key, int* value);
 
 #ifdef __cplusplus
 }

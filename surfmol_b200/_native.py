@@ -66,6 +66,7 @@ SIGNATURES = {
     "smr_build_grid_static": (C.c_int, [C.c_int, DP, DP, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, DP, DP,
                                         C.POINTER(SmrGridBuildParamsStatic), VP, VP, C.c_char_p, C.c_int]),
     "smr_add_molecule": (C.c_int, [VP, C.c_int, IP, DP, DP, C.c_double, IP]),
+    "smr_add_molecules": (C.c_int, [VP, C.c_int, IP, IP, DP, DP, C.c_double, IP]),
     "smr_add_topology": (C.c_int, [VP, C.POINTER(SmrTopologyDesc), IP]),
     "smr_topology_counts": (C.c_int, [VP, C.c_int, IP]),
     "smr_topology_export": (C.c_int, [VP, C.c_int, IP, IP, IP, DP, IP, IP, DP, IP, IP, DP, IP, IP, DP, DP, IP]),
@@ -87,6 +88,8 @@ SIGNATURES = {
     "smr_download_pos64": (C.c_int, [VP, C.c_int, IP, DP]),
     "smr_last_timing": (C.c_int, [VP, DP, LLP]),
     "smr_set_team_size": (C.c_int, [VP, C.c_int, C.c_int]),
+    "smr_set_tuning": (C.c_int, [VP, C.c_int, C.c_int]),
+    "smr_get_tuning": (C.c_int, [VP, C.c_int, IP]),
     "smr_set_schedule": (C.c_int, [VP, C.c_int, C.c_int, C.c_int]),
     "smr_get_schedule": (C.c_int, [VP, IP, IP, IP]),
     "smr_set_stages": (C.c_int, [VP, C.c_int, IP, IP, IP, C.c_int]),

@@ -1,6 +1,7 @@
 // abi.cpp -- the C ABI of include/surfmol_relax.h: handle, device arenas, slot
 // allocator, launches and transfers.  Host-side only; kernels live in relax.cu / grid.cu.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdarg>
 #include <cstdio>
@@ -102,6 +103,7 @@ struct smr_handle {
     std::vector<int> stage_form{FORM_ROUNDS};
     int eval_form = FORM_ROUNDS;        // form and team (0: by size) of smr_eval_forces
     int eval_team = 0;
+    int nb_lanes = 0;                   // tuning: lanes per atom of the NB loop (0: by size)
 
     // grid
     void* grid = nullptr;
@@ -114,6 +116,11 @@ struct smr_handle {
     smr_nb_params nb{1.0f, 1.5f, 0.0f, 0};
 
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // the launch segments of one schedule stage (disjoint sets of systems, one team size each) run
+    // concurrently on side streams, so one class's tail overlaps the next class's work
+    static constexpr int kSide = 4;
+    cudaStream_t side[kSide] = {};
+    cudaEvent_t ev_fork = nullptr, ev_join[kSide] = {};
     double last_ms = 0.0;
     long long last_launches = 0;
 };
@@ -137,12 +144,42 @@ int team_for(const smr_handle* h, int n) {
     return default_team(n);
 }
 
+// a topology's records in every kernel form, prepared off the handle (thread-safe)
+struct PreparedTopo { int team = 32; PackedTerms P; FlatTerms F; OwnerTerms O; bool own_ok = false; };
+
+void prepare_topology(const HostTopo& T, int team, PreparedTopo& p) {
+    p.team = team;
+    pack_rounds(T, team, p.P);
+    flat_terms(T, p.F);
+    p.own_ok = owner_terms(T, p.O);
+}
+
+// run f(i) for i in [0, n) on the host cores
+template <class F>
+void parallel_for(int n, F f) {
+    const int nt = std::max(1, std::min<int>(n, (int)std::thread::hardware_concurrency()));
+    if (nt <= 1 || n < 4) { for (int i = 0; i < n; i++) f(i); return; }
+    std::atomic<int> next{0};
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nt; t++)
+        pool.emplace_back([&]() { for (int i = next++; i < n; i = next++) f(i); });
+    for (auto& th : pool) th.join();
+}
+
+void commit_topology(smr_handle* h, const HostTopo& T, const PreparedTopo& pt);
+
 // append a topology's device records (packed for its team) to the arenas
 void append_topology(smr_handle* h, const HostTopo& T) {
+    PreparedTopo p;
+    prepare_topology(T, team_for(h, T.n), p);
+    commit_topology(h, T, p);
+}
+
+void commit_topology(smr_handle* h, const HostTopo& T, const PreparedTopo& pt) {
     TopoDev td{};
     td.natoms = T.n;
     td.atom_off = (int)h->hreq.size();
-    td.team = team_for(h, T.n);
+    td.team = pt.team;
     for (int a = 0; a < T.n; a++) {
         const double* r = &T.req[4 * a];
         h->hreq.push_back(make_float4((float)r[0], (float)r[1], (float)r[2], (float)r[3]));
@@ -151,13 +188,11 @@ void append_topology(smr_handle* h, const HostTopo& T) {
         h->hbk.push_back(make_float4((float)kl[0], (float)kl[2], (float)kl[4], (float)kl[6]));
         h->hbl.push_back(make_float4((float)kl[1], (float)kl[3], (float)kl[5], (float)kl[7]));
     }
-    PackedTerms P;
-    pack_rounds(T, td.team, P);
+    const PackedTerms& P = pt.P;
     td.ang_off = (int)h->hang.size(); td.ang_rounds = P.ang_rounds; h->hang.insert(h->hang.end(), P.ang.begin(), P.ang.end());
     td.dih_off = (int)h->hdih.size(); td.dih_rounds = P.dih_rounds; h->hdih.insert(h->hdih.end(), P.dih.begin(), P.dih.end());
     td.inv_off = (int)h->hinv.size(); td.inv_rounds = P.inv_rounds; h->hinv.insert(h->hinv.end(), P.inv.begin(), P.inv.end());
-    FlatTerms F;
-    flat_terms(T, F);
+    const FlatTerms& F = pt.F;
     td.nang = (int)F.ang.size(); td.ndih = (int)F.dih.size(); td.ninv = (int)F.inv.size(); td.npieces = F.npieces;
     td.fang_off = (int)h->hang.size(); h->hang.insert(h->hang.end(), F.ang.begin(), F.ang.end());
     td.fdih_off = (int)h->hdih.size(); h->hdih.insert(h->hdih.end(), F.dih.begin(), F.dih.end());
@@ -165,8 +200,8 @@ void append_topology(smr_handle* h, const HostTopo& T) {
     td.a2f_off = (int)h->hidx.size();
     h->ha2f.insert(h->ha2f.end(), F.a2f.begin(), F.a2f.end());
     h->hidx.insert(h->hidx.end(), F.idx.begin(), F.idx.end());
-    OwnerTerms O;
-    td.own_ok = owner_terms(T, O) ? 1 : 0;
+    const OwnerTerms& O = pt.O;
+    td.own_ok = pt.own_ok ? 1 : 0;
     if (td.own_ok) {
         td.own_a_off = (int)h->hown_geo.size();
         td.own_i_off = td.own_a_off + O.rows_a * T.n;
@@ -218,7 +253,9 @@ int repack_all(smr_handle* h) {
     h->hang.clear(); h->hdih.clear(); h->hinv.clear(); h->ha2f.clear(); h->hidx.clear();
     h->hown_geo.clear(); h->hown_par.clear(); h->hown_meta.clear();
     h->up_atoms = h->up_ang = h->up_dih = h->up_inv = h->up_topo = h->up_idx = h->up_own = 0;
-    for (const HostTopo& T : h->topos) append_topology(h, T);
+    std::vector<PreparedTopo> prep(h->topos.size());
+    parallel_for((int)prep.size(), [&](int i) { prepare_topology(h->topos[i], team_for(h, h->topos[i].n), prep[i]); });
+    for (size_t i = 0; i < prep.size(); i++) commit_topology(h, h->topos[i], prep[i]);
     return upload_all(h);
 }
 
@@ -286,6 +323,7 @@ KernelArgs base_args(smr_handle* h) {
     a.angs = h->dang.d; a.dihs = h->ddih.d; a.invs = h->dinv.d;
     a.a2f = h->da2f.d; a.a2f_idx = h->didx.d;
     a.own_geo = h->down_geo.d; a.own_par = h->down_par.d; a.own_meta = h->down_meta.d;
+    a.nb_lanes = h->nb_lanes;
     a.pos = h->pos; a.plo = h->plo; a.vel = h->vel; a.force = h->force;
     a.has_grid = h->has_grid ? 1 : 0;
     a.grid.data = h->grid;
@@ -412,6 +450,11 @@ int smr_create(const smr_config* cfg, smr_handle** out) {
     h->free_atoms[0] = (long long)na;
     cudaEventCreate(&h->ev0);
     cudaEventCreate(&h->ev1);
+    if (cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess) return bail(SMR_ERR_CUDA);
+    for (int k = 0; k < smr_handle::kSide; k++)
+        if (cudaStreamCreateWithFlags(&h->side[k], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&h->ev_join[k], cudaEventDisableTiming) != cudaSuccess)
+            return bail(SMR_ERR_CUDA);
     *out = h;
     return SMR_OK;
 }
@@ -425,6 +468,11 @@ int smr_destroy(smr_handle* h) {
     if (h->grid) cudaFree(h->grid);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    for (int k = 0; k < smr_handle::kSide; k++) {
+        if (h->side[k]) cudaStreamDestroy(h->side[k]);
+        if (h->ev_join[k]) cudaEventDestroy(h->ev_join[k]);
+    }
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return SMR_OK;
@@ -435,6 +483,23 @@ int smr_set_nb_params(smr_handle* h, const smr_nb_params* p) {
     if (!(p->rdamp >= 0.f) || !(p->alpha_morse > 0.f)) return fail(h, SMR_ERR_ARG, "rdamp must be >= 0 and alpha_morse > 0");
     h->nb = *p;
     return SMR_OK;
+}
+
+int smr_set_tuning(smr_handle* h, int key, int value) {
+    if (!h) return SMR_ERR_ARG;
+    if (key == SMR_TUNE_NB_LANES) {
+        if (value != 0 && value != 1 && value != 2 && value != 4 && value != 8 && value != 16 && value != 32)
+            return fail(h, SMR_ERR_ARG, "NB lanes per atom must be 0, 1, 2, 4, 8, 16 or 32");
+        h->nb_lanes = value;
+        return SMR_OK;
+    }
+    return fail(h, SMR_ERR_ARG, "unknown tuning key %d", key);
+}
+
+int smr_get_tuning(smr_handle* h, int key, int* value) {
+    if (!h || !value) return SMR_ERR_ARG;
+    if (key == SMR_TUNE_NB_LANES) { *value = h->nb_lanes; return SMR_OK; }
+    return fail(h, SMR_ERR_ARG, "unknown tuning key %d", key);
 }
 
 int smr_set_team_size(smr_handle* h, int max_atoms, int threads) {
@@ -561,6 +626,33 @@ int smr_add_molecule(smr_handle* h, int natoms, const int* Z, const double* pos,
     if (r) return r;
     *topo_id = (int)h->topos.size() - 1;
     return SMR_OK;
+}
+
+int smr_add_molecules(smr_handle* h, int nmol, const int* natoms, const int* Z, const double* pos, const double* charges,
+                      double bond_cut, int* topo_ids) {
+    if (!h || nmol < 0 || (nmol && (!natoms || !Z || !pos || !topo_ids))) return SMR_ERR_ARG;
+    std::vector<long long> off(nmol + 1, 0);
+    for (int i = 0; i < nmol; i++) {
+        if (natoms[i] <= 0) return fail(h, SMR_ERR_ARG, "molecule %d has %d atoms", i, natoms[i]);
+        off[i + 1] = off[i] + natoms[i];
+    }
+    std::vector<HostTopo> T(nmol);
+    std::vector<PreparedTopo> prep(nmol);
+    std::vector<std::string> err(nmol);
+    const double cut = bond_cut > 0 ? bond_cut : 1.8;
+    parallel_for(nmol, [&](int i) {
+        char msg[300] = {0};
+        if (build_molecule_topology(natoms[i], Z + off[i], pos + 3 * off[i], charges ? charges + off[i] : nullptr, cut, T[i],
+                                    msg, sizeof(msg))) { err[i] = msg[0] ? msg : "invalid molecule"; return; }
+        prepare_topology(T[i], team_for(h, T[i].n), prep[i]);
+    });
+    for (int i = 0; i < nmol; i++) if (!err[i].empty()) return fail(h, SMR_ERR_ARG, "molecule %d: %s", i, err[i].c_str());
+    for (int i = 0; i < nmol; i++) {
+        h->topos.push_back(std::move(T[i]));
+        commit_topology(h, h->topos.back(), prep[i]);
+        topo_ids[i] = (int)h->topos.size() - 1;
+    }
+    return upload_all(h);
 }
 
 int smr_add_topology(smr_handle* h, const smr_topology_desc* d, int* topo_id) {
@@ -831,20 +923,33 @@ int smr_run_fire(smr_handle* h, int max_steps, int step_budget, const smr_fire_p
     for (int k = 0; k < nst; k++) ssegs[k] = group_by(h, sids[k], h->stage_form[k], h->stage_team[k]);
     for (auto& sg : ssegs) for (auto& g : sg) { r = check_smem(h, g); if (r) return r; }
     cudaEventRecord(h->ev0, s);
-    auto launch = [&](const Seg& g, const int* work_base, int limit, int nwork_override) -> int {
+    auto launch = [&](const Seg& g, const int* work_base, int limit, int nwork_override, cudaStream_t ls, int* counter) -> int {
         a.work = work_base + g.begin; a.nwork = nwork_override > 0 ? nwork_override : g.end - g.begin;
-        a.nmax = g.nmax; a.nfmax = g.nfmax; a.phase_limit = limit;
-        CU(h, cudaMemsetAsync(h->counter, 0, 4, s));
-        int e = launch_relax(a, g.team, g.form, 0, s, h->num_sms, &h->last_launches);
+        a.nmax = g.nmax; a.nfmax = g.nfmax; a.phase_limit = limit; a.counter = counter;
+        CU(h, cudaMemsetAsync(counter, 0, 4, ls));
+        int e = launch_relax(a, g.team, g.form, 0, ls, h->num_sms, &h->last_launches);
         if (e) return fail(h, SMR_ERR_CUDA, "relax launch: %s", cudaGetErrorString((cudaError_t)e));
         return 0;
     };
     if (mode == SMR_MODE_BATCHED) {
-        // stages run in order; every launch redistributes the systems still running over the GPU
+        // stages run in order (every stage's launches redistribute the systems still running over
+        // the GPU); the segments of one stage hold disjoint systems and run concurrently
         for (int k = 0; k < nst; k++) {
             if (sids[k].empty()) continue;
             CU(h, cudaMemcpyAsync(h->work, sids[k].data(), sids[k].size() * 4, cudaMemcpyHostToDevice, s));
-            for (auto& g : ssegs[k]) { r = launch(g, h->work, stage_end(k), 0); if (r) return r; }
+            const int m = (int)ssegs[k].size();
+            if (m == 1) { r = launch(ssegs[k][0], h->work, stage_end(k), 0, s, h->counter); if (r) return r; continue; }
+            CU(h, cudaEventRecord(h->ev_fork, s));
+            const int nside = std::min(m, smr_handle::kSide);
+            for (int j = 0; j < nside; j++) CU(h, cudaStreamWaitEvent(h->side[j], h->ev_fork, 0));
+            for (int j = 0; j < m; j++) {
+                r = launch(ssegs[k][j], h->work, stage_end(k), 0, h->side[j % nside], h->counter + (j % nside));
+                if (r) return r;
+            }
+            for (int j = 0; j < nside; j++) {
+                CU(h, cudaEventRecord(h->ev_join[j], h->side[j]));
+                CU(h, cudaStreamWaitEvent(s, h->ev_join[j], 0));
+            }
         }
     } else {
         // plain form: one launch per system per FIRE step, status read back after each step
@@ -861,7 +966,7 @@ int smr_run_fire(smr_handle* h, int max_steps, int step_budget, const smr_fire_p
             for (int steps = start[slot]; steps < st.target; steps++) {
                 int k = 0;
                 while (k + 1 < nst && steps >= h->stage_start[k + 1]) k++;
-                r = launch(per_stage[k], h->work, steps + 1, 1);
+                r = launch(per_stage[k], h->work, steps + 1, 1, s, h->counter);
                 if (r) return r;
                 int stt = 0;
                 CU(h, cudaMemcpyAsync(&stt, &h->slots[slot].status, 4, cudaMemcpyDeviceToHost, s));

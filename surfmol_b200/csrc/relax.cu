@@ -507,7 +507,7 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
     // (opencl/UFF.cl:57-95, 1595-1665).  Excluded pairs are evaluated at r2 = 1 and masked out,
     // so the partner loop has no branch and independent pairs overlap.
     {
-        const int L = nb_lanes(N, T), G = T / L;
+        const int L = a.nb_lanes > 0 ? min(a.nb_lanes, min(T, 32)) : nb_lanes(N, T), G = T / L;
         const int c = rank & (L - 1);
         const bool small = N <= 64;
         for (int i0 = 0; i0 < N; i0 += G) {

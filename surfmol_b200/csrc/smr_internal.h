@@ -101,6 +101,7 @@ struct KernelArgs {
     const short4* own_geo;        // owner form: hneigh indices (+ dihedral half in .w)
     const float4* own_par;        // owner form: term parameters
     const int* own_meta;          // owner form, per atom: n_ang | n_inv << 8 | n_dih << 16 | back slots << 24
+    int nb_lanes;                 // lanes per atom in the NB partner loop (0: chosen from N and the team)
 };
 
 // ---- host topology (topology.cpp)

@@ -215,6 +215,15 @@ class RelaxMulti:
         k = n.value
         return st[:k].tolist(), fm[:k].tolist(), tm[:k].tolist()
 
+    def set_nb_lanes(self, lanes):
+        """Lanes per atom in the NB partner loop (0: chosen from system size and team)."""
+        self._chk(self.L.smr_set_tuning(self.h, 1, int(lanes)), "smr_set_tuning")
+
+    def get_nb_lanes(self):
+        v = C.c_int()
+        self._chk(self.L.smr_get_tuning(self.h, 1, C.byref(v)), "smr_get_tuning")
+        return v.value
+
     def set_team_size(self, max_atoms, threads):
         self._chk(self.L.smr_set_team_size(self.h, max_atoms, threads), "smr_set_team_size")
 
@@ -228,6 +237,18 @@ class RelaxMulti:
                                           C.byref(tid)), "smr_add_molecule")
         self.topo_n.append(len(Z))
         return tid.value
+
+    def add_molecules(self, Zs, poss, charges=None, bond_cut=1.8):
+        """Many molecules at once (typing and packing on all host cores); returns their topology ids."""
+        n = _i([len(z) for z in Zs])
+        Z = _i(np.concatenate([np.asarray(z) for z in Zs])) if len(Zs) else _i([])
+        P = _d(np.concatenate([np.asarray(p).reshape(-1, 3) for p in poss])) if len(Zs) else _d(np.zeros((0, 3)))
+        q = _d(np.concatenate([np.asarray(c) for c in charges])) if charges is not None and len(Zs) else None
+        ids = np.zeros(len(Zs), np.int32)
+        self._chk(self.L.smr_add_molecules(self.h, len(Zs), _p(n, N.IP), _p(Z, N.IP), _p(P, N.DP), _p(q, N.DP), bond_cut,
+                                           _p(ids, N.IP)), "smr_add_molecules")
+        self.topo_n.extend(int(k) for k in n)
+        return ids
 
     def add_topo(self, topo: Topology) -> int:
         tid = C.c_int()

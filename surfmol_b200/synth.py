@@ -260,18 +260,32 @@ def config1(seed: int = 0, nsys: int = 4096) -> Workload:
     return Workload(Zs, Ps, Qs, np.zeros(nsys, np.int32), slab, g, seed)
 
 
+def _ragged_one(args):
+    """Molecule i of a ragged workload, from its own generator (seed, i): any subset can be made alone."""
+    seed, i, nmin, nmax, Lx, Ly, z_top = args
+    rng = np.random.default_rng([seed, i])
+    target = int(round(math.exp(rng.uniform(math.log(nmin), math.log(nmax)))))
+    mol = ragged_molecule(rng, target)
+    q = charges(rng, mol.n)
+    xy0 = (rng.uniform(0, Lx), rng.uniform(0, Ly))
+    return mol.Z, place(rng, mol, xy0, rng.uniform(2.5, 4.0), z_top=z_top), q
+
+
 def ragged(seed: int, nsys: int, nmin: int = 20, nmax: int = 400, ncell: int = 8, nlayers: int = 3,
-           nz: int = 161) -> Workload:
-    """Ragged batch: atom counts log-uniform in [nmin, nmax], each molecule distinct."""
-    rng = np.random.default_rng(seed)
+           nz: int = 161, workers: int = 0) -> Workload:
+    """Ragged batch: atom counts log-uniform in [nmin, nmax], each molecule distinct; molecule i is
+    drawn from its own generator seeded (seed, i).  workers > 1 generates in a spawned process pool
+    (call it before any CUDA work in the process)."""
     slab = rocksalt_slab(ncell, nlayers)
     g = grid_for(slab, nz=nz)
-    Zs, Ps, Qs = [], [], []
-    for _ in range(nsys):
-        target = int(round(math.exp(rng.uniform(math.log(nmin), math.log(nmax)))))
-        mol = ragged_molecule(rng, target)
-        Qs.append(charges(rng, mol.n))
-        xy0 = (rng.uniform(0, slab.Lx), rng.uniform(0, slab.Ly))
-        Ps.append(place(rng, mol, xy0, rng.uniform(2.5, 4.0)))
-        Zs.append(mol.Z)
+    jobs = [(seed, i, nmin, nmax, slab.Lx, slab.Ly, slab.z_top) for i in range(nsys)]
+    if workers > 1:
+        import multiprocessing as mp
+        with mp.get_context("spawn").Pool(workers) as pool:
+            out = pool.map(_ragged_one, jobs, chunksize=max(1, nsys // (8 * workers)))
+    else:
+        out = [_ragged_one(j) for j in jobs]
+    Zs = [o[0] for o in out]
+    Ps = [o[1] for o in out]
+    Qs = [o[2] for o in out]
     return Workload(Zs, Ps, Qs, np.arange(nsys, dtype=np.int32), slab, g, seed)

@@ -1,0 +1,98 @@
+"""Ragged batching on the GPU: batch admission, concurrent size classes, interaction tiling and the
+autotuner, through the C ABI, against one-by-one admission and the FP64 oracle."""
+import numpy as np
+import pytest
+
+from tests.gpu_helpers import F_RTOL, build_device_grid, force_err, molecule_on_slab, small_slab_grid
+
+pytestmark = pytest.mark.gpu
+
+
+def make_handle(ms, ma, slab, dims, p0, step, rcut=0.0):
+    from surfmol_b200 import RelaxMulti
+    R = RelaxMulti(max_systems=ms, max_atoms=ma)
+    R.set_nb(1.0, 1.5, rcut)
+    build_device_grid(R, slab, dims, p0, step)
+    return R
+
+
+@pytest.fixture(scope="module")
+def setup():
+    slab, dims, p0, step = small_slab_grid()
+    rng = np.random.default_rng(314)
+    mols = [molecule_on_slab(rng, n, slab) for n in (22, 40, 57, 90, 150, 210, 330)]
+    return slab, dims, p0, step, mols
+
+
+def test_batch_admission_matches_one_by_one(setup):
+    """smr_add_molecules (parallel host typing and packing, one upload) gives the topologies and the
+    trajectories of smr_add_molecule, bit for bit, with the size classes running concurrently."""
+    slab, dims, p0, step, mols = setup
+    tot = sum(len(m[0]) for m in mols)
+    A = make_handle(16, tot, slab, dims, p0, step)
+    B = make_handle(16, tot, slab, dims, p0, step)
+    try:
+        ta = [A.add_molecule(Z, P, q) for Z, P, q in mols]
+        tb = list(B.add_molecules([m[0] for m in mols], [m[1] for m in mols], [m[2] for m in mols]))
+        for a, b in zip(ta, tb):
+            ea, eb = A.topology(a), B.topology(b)
+            for k in ea:
+                assert np.array_equal(np.asarray(ea[k]), np.asarray(eb[k])), k
+        sa = A.add_systems(ta, [m[1] for m in mols])
+        sb = B.add_systems(tb, [m[1] for m in mols])
+        for R in (A, B):
+            R.set_stages([0, 40], [0, 1], [0, 0])
+            R.run_fire(120, step_budget=120, fconv=1e-6)
+        oa, ob = A.download(sa), B.download(sb)
+        for i in range(len(mols)):
+            assert np.array_equal(oa["pos"][i], ob["pos"][i]) and oa["steps"][i] == ob["steps"][i] == 120
+    finally:
+        A.finish()
+        B.finish()
+
+
+@pytest.mark.parametrize("lanes", [1, 2, 8, 32])
+def test_nb_lanes_forces_match_oracle(setup, oracle, lanes):
+    """Every NB interaction tiling gives oracle forces (with and without the 10 A cutoff)."""
+    slab, dims, p0, step, mols = setup
+    from oracle import oracle as O
+    for rcut in (0.0, 10.0):
+        R = make_handle(4, 2000, slab, dims, p0, step, rcut)
+        try:
+            R.set_nb_lanes(lanes)
+            assert R.get_nb_lanes() == lanes
+            g = R.get_grid()
+            for Z, P, q in (mols[1], mols[5]):
+                s = R.add_systems([R.add_molecule(Z, P, q)], [P])
+                F, _ = R.eval_forces(s)
+                Fo, _, _ = O.System.from_molecule(Z, P, q).eval(P.astype(np.float32).astype(np.float64),
+                                                                O.Grid(g["coef"], g["p0"], g["step"]), rcut=rcut)
+                assert force_err(F[0], Fo) < F_RTOL, (lanes, rcut, len(Z))
+                R.remove_systems(s)
+        finally:
+            R.finish()
+
+
+def test_autotuner_runs_and_applies(setup):
+    """The autotuner measures candidates on the device and its result applies to a handle; the tuned
+    launch shape gives the same relaxation as any other up to rounding (same step counts within a few)."""
+    slab, dims, p0, step, mols = setup
+    from surfmol_b200.autotune import Autotuner
+    fire = dict(dt0=0.001, dt_max=0.05, fconv=1e-3)
+    mk = lambda ms, ma: make_handle(ms, ma, slab, dims, p0, step)
+    res = Autotuner(mk, fire, probe_steps=30, max_steps=400).tune([m[0] for m in mols], [m[1] for m in mols],
+                                                                  [m[2] for m in mols])
+    assert res.team_by_class and res.nb_lanes in (0, 1, 2, 4, 8)
+    assert res.timings["relax_ms_tuned"] <= res.timings["relax_ms_single_stage"] + 1e-9
+    R = mk(16, 4000)
+    try:
+        res.apply(R)
+        st = R.get_stages()
+        assert tuple(st[0]) == tuple(res.stages[0]) and tuple(st[1]) == tuple(res.stages[1])
+        tids = R.add_molecules([m[0] for m in mols], [m[1] for m in mols], [m[2] for m in mols])
+        s = R.add_systems(tids, [m[1] for m in mols])
+        R.run_fire(400, step_budget=400, **fire)
+        out = R.download(s)
+        assert np.all(np.isfinite(np.concatenate(out["pos"])))
+    finally:
+        R.finish()
