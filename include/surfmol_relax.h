@@ -185,6 +185,15 @@ int  smr_topo_export(const smr_topo* t, int* neighs, int* neighBs, int* bonds, d
                      int* invs, int* inv_ngs, double* invp, double* req, int* type_id);
 int  smr_topo_rounds(const smr_topo* t, int team, int rounds[3], short* ang_at, short* dih_at, short* inv_at);
 int  smr_add_topo(smr_handle* h, const smr_topo* t, int* topo_id);
+/* Pack a host topology's term records for a team size (0: the default for its size) without a
+ * handle; thread-safe, so request topologies can be packed while the GPU works.  smr_add_topo then
+ * uploads them as they are when the handle's team for that size matches.  No counterpart in the
+ * reference. */
+int  smr_topo_prepare(smr_topo* t, int team);
+/* Release a topology no active slot uses; its id stays reserved.  The device records of removed
+ * topologies are dropped by an automatic compaction once they outnumber the live ones (long-running
+ * servers admit and retire molecules without growing the arenas).  No counterpart in the reference. */
+int  smr_remove_topology(smr_handle* h, int topo_id);
 
 /* Systems: one slot per system; positions are float32 x,y,z concatenated over the systems. */
 int smr_add_systems(smr_handle* h, int nsys, const int* topo_ids, const float* pos, int* slot_ids);

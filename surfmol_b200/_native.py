@@ -77,6 +77,8 @@ SIGNATURES = {
     "smr_topo_export": (C.c_int, [VP, IP, IP, IP, DP, IP, IP, DP, IP, IP, DP, IP, IP, DP, DP, IP]),
     "smr_topo_rounds": (C.c_int, [VP, C.c_int, IP, SP, SP, SP]),
     "smr_add_topo": (C.c_int, [VP, VP, IP]),
+    "smr_topo_prepare": (C.c_int, [VP, C.c_int]),
+    "smr_remove_topology": (C.c_int, [VP, C.c_int]),
     "smr_add_systems": (C.c_int, [VP, C.c_int, IP, FP, IP]),
     "smr_remove_systems": (C.c_int, [VP, C.c_int, IP]),
     "smr_set_positions": (C.c_int, [VP, C.c_int, IP, FP]),

@@ -83,6 +83,9 @@ struct smr_handle {
 
     // topologies
     std::vector<HostTopo> topos;
+    std::vector<char> topo_alive;       // 0 after smr_remove_topology (records dropped at compaction)
+    std::vector<size_t> own_len;        // owner-form records of each topology
+    size_t dead_atoms = 0;              // arena atoms of removed topologies not yet compacted
     std::vector<TopoDev> htd;
     DArr<TopoDev> dtd;
     std::vector<float4> hreq, hbk, hbl;
@@ -115,6 +118,7 @@ struct smr_handle {
 
     smr_nb_params nb{1.0f, 1.5f, 0.0f, 0};
 
+    DArr<char> gscr;                    // team state of systems too large for shared memory
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // the launch segments of one schedule stage (disjoint sets of systems, one team size each) run
     // concurrently on side streams, so one class's tail overlaps the next class's work
@@ -213,6 +217,16 @@ void commit_topology(smr_handle* h, const HostTopo& T, const PreparedTopo& pt) {
         h->hown_meta.insert(h->hown_meta.end(), T.n, 0);
     }
     h->htd.push_back(td);
+    h->own_len.push_back(pt.own_ok ? pt.O.geo.size() : 0);
+}
+
+// the arena record of a removed topology (kept so that topology ids stay stable)
+void commit_dead(smr_handle* h) {
+    TopoDev td{};
+    td.atom_off = (int)h->hreq.size();
+    td.team = 32;
+    h->htd.push_back(td);
+    h->own_len.push_back(0);
 }
 
 template <class T>
@@ -253,9 +267,53 @@ int repack_all(smr_handle* h) {
     h->hang.clear(); h->hdih.clear(); h->hinv.clear(); h->ha2f.clear(); h->hidx.clear();
     h->hown_geo.clear(); h->hown_par.clear(); h->hown_meta.clear();
     h->up_atoms = h->up_ang = h->up_dih = h->up_inv = h->up_topo = h->up_idx = h->up_own = 0;
+    h->own_len.clear();
+    h->dead_atoms = 0;
     std::vector<PreparedTopo> prep(h->topos.size());
-    parallel_for((int)prep.size(), [&](int i) { prepare_topology(h->topos[i], team_for(h, h->topos[i].n), prep[i]); });
-    for (size_t i = 0; i < prep.size(); i++) commit_topology(h, h->topos[i], prep[i]);
+    parallel_for((int)prep.size(), [&](int i) {
+        if (h->topo_alive[i]) prepare_topology(h->topos[i], team_for(h, h->topos[i].n), prep[i]);
+    });
+    for (size_t i = 0; i < prep.size(); i++) {
+        if (h->topo_alive[i]) commit_topology(h, h->topos[i], prep[i]);
+        else commit_dead(h);
+    }
+    return upload_all(h);
+}
+
+// Drop the records of removed topologies from every arena: each live topology's ranges are
+// copied in id order into fresh host mirrors, its offsets updated, and everything re-uploaded.
+int compact_topologies(smr_handle* h) {
+    smr_handle& o = *h;
+    std::vector<float4> req, bk, bl; std::vector<short4> neigh; std::vector<int2> a2f; std::vector<int> meta, idx;
+    std::vector<AngRec> ang; std::vector<DihRec> dih; std::vector<InvRec> inv;
+    std::vector<short4> geo; std::vector<float4> par;
+    auto cp = [](auto& dst, const auto& src, size_t off, size_t n) { dst.insert(dst.end(), src.begin() + off, src.begin() + off + n); };
+    for (size_t id = 0; id < o.htd.size(); id++) {
+        TopoDev& td = o.htd[id];
+        if (!o.topo_alive[id]) { td = TopoDev{}; td.atom_off = (int)req.size(); td.team = 32; o.own_len[id] = 0; continue; }
+        const size_t n = td.natoms, a0 = td.atom_off;
+        td.atom_off = (int)req.size();
+        cp(req, o.hreq, a0, n); cp(neigh, o.hneigh, a0, n); cp(bk, o.hbk, a0, n); cp(bl, o.hbl, a0, n);
+        cp(a2f, o.ha2f, a0, n); cp(meta, o.hown_meta, a0, n);
+        const size_t T = td.team;
+        size_t x;
+        x = td.ang_off; td.ang_off = (int)ang.size(); cp(ang, o.hang, x, td.ang_rounds * T);
+        x = td.fang_off; td.fang_off = (int)ang.size(); cp(ang, o.hang, x, td.nang);
+        x = td.dih_off; td.dih_off = (int)dih.size(); cp(dih, o.hdih, x, td.dih_rounds * T);
+        x = td.fdih_off; td.fdih_off = (int)dih.size(); cp(dih, o.hdih, x, td.ndih);
+        x = td.inv_off; td.inv_off = (int)inv.size(); cp(inv, o.hinv, x, td.inv_rounds * T);
+        x = td.finv_off; td.finv_off = (int)inv.size(); cp(inv, o.hinv, x, td.ninv);
+        x = td.a2f_off; td.a2f_off = (int)idx.size(); cp(idx, o.hidx, x, td.npieces);
+        if (td.own_ok) {
+            const int shift = (int)geo.size() - td.own_a_off;
+            cp(geo, o.hown_geo, td.own_a_off, o.own_len[id]); cp(par, o.hown_par, td.own_a_off, o.own_len[id]);
+            td.own_a_off += shift; td.own_i_off += shift; td.own_d_off += shift;
+        }
+    }
+    o.hreq.swap(req); o.hneigh.swap(neigh); o.hbk.swap(bk); o.hbl.swap(bl); o.ha2f.swap(a2f); o.hown_meta.swap(meta);
+    o.hang.swap(ang); o.hdih.swap(dih); o.hinv.swap(inv); o.hidx.swap(idx); o.hown_geo.swap(geo); o.hown_par.swap(par);
+    o.up_atoms = o.up_ang = o.up_dih = o.up_inv = o.up_topo = o.up_idx = o.up_own = 0;
+    o.dead_atoms = 0;
     return upload_all(h);
 }
 
@@ -338,7 +396,7 @@ KernelArgs base_args(smr_handle* h) {
 }
 
 // group slots by launch configuration; returns (team, form, begin, end, nmax, nfmax) segments
-struct Seg { int team, form, begin, end, nmax, nfmax; };
+struct Seg { int team, form, begin, end, nmax, nfmax; bool gstate; };   // gstate: team state in global memory
 
 int latency_team_for(int requested, int n) {
     if (requested) return requested;
@@ -378,12 +436,14 @@ std::vector<Seg> group_by(smr_handle* h, std::vector<int>& ids, int form, int re
         if (!segs.empty()) {
             Seg& g = segs.back();
             if (g.form == k.form && g.team == k.team &&
-                team_smem_bytes(std::max(g.nmax, k.n), std::max(g.nfmax, k.nf), k.team, k.form) <= h->smem_optin) {
+                (g.gstate || team_smem_bytes(std::max(g.nmax, k.n), std::max(g.nfmax, k.nf), k.team, k.form) <= h->smem_optin)) {
                 g.end = i + 1; g.nmax = std::max(g.nmax, k.n); g.nfmax = std::max(g.nfmax, k.nf);
                 continue;
             }
         }
-        segs.push_back({k.team, k.form, i, i + 1, k.n, k.nf});
+        // a system whose state does not fit in shared memory starts a global-state segment
+        const bool gs = team_smem_bytes(k.n, k.nf, k.team, k.form) > h->smem_optin;
+        segs.push_back({k.team, k.form, i, i + 1, k.n, k.nf, gs});
     }
     return segs;
 }
@@ -392,10 +452,27 @@ bool fits(const smr_handle* h, const Seg& g) {
     return team_smem_bytes(g.nmax, g.nfmax, g.team, g.form) <= h->smem_optin;
 }
 
-int check_smem(smr_handle* h, const Seg& g) {
-    if (fits(h, g)) return 0;
-    return fail(h, SMR_ERR_CAPACITY, "systems of %d atoms need %zu B of shared memory per block (device limit %zu); "
-                "use a larger team or smaller systems", g.nmax, team_smem_bytes(g.nmax, g.nfmax, g.team, g.form), h->smem_optin);
+// Global-memory team state for the segments that do not fit in shared memory: each such segment
+// gets its own region (segments of one stage run concurrently) of two blocks' state per SM.
+// Returns the bytes needed; off[j] / len[j] are segment j's region (len 0: shared memory).
+size_t plan_gscratch(const smr_handle* h, const std::vector<Seg>& segs, std::vector<size_t>& off, std::vector<size_t>& len) {
+    size_t tot = 0;
+    off.assign(segs.size(), 0);
+    len.assign(segs.size(), 0);
+    for (size_t j = 0; j < segs.size(); j++) {
+        if (!segs[j].gstate) continue;
+        const size_t b = (team_smem_bytes(segs[j].nmax, segs[j].nfmax, segs[j].team, segs[j].form) + 255) & ~size_t(255);
+        off[j] = tot;
+        len[j] = b * 2 * (size_t)h->num_sms;
+        tot += len[j];
+    }
+    return tot;
+}
+
+int reserve_gscratch(smr_handle* h, size_t bytes) {
+    cudaError_t e = h->gscr.reserve(bytes, 0, h->stream);
+    if (e != cudaSuccess) return fail(h, SMR_ERR_CAPACITY, "global team state of %zu B: %s", bytes, cudaGetErrorString(e));
+    return 0;
 }
 
 // a batch of slots must be distinct, active and fit the staging buffers
@@ -621,6 +698,7 @@ int smr_add_molecule(smr_handle* h, int natoms, const int* Z, const double* pos,
     if (build_molecule_topology(natoms, Z, pos, charges, bond_cut > 0 ? bond_cut : 1.8, T, msg, sizeof(msg)))
         return fail(h, SMR_ERR_ARG, "molecule: %s", msg);
     h->topos.push_back(std::move(T));
+    h->topo_alive.push_back(1);
     append_topology(h, h->topos.back());
     int r = upload_all(h);
     if (r) return r;
@@ -649,6 +727,7 @@ int smr_add_molecules(smr_handle* h, int nmol, const int* natoms, const int* Z, 
     for (int i = 0; i < nmol; i++) if (!err[i].empty()) return fail(h, SMR_ERR_ARG, "molecule %d: %s", i, err[i].c_str());
     for (int i = 0; i < nmol; i++) {
         h->topos.push_back(std::move(T[i]));
+        h->topo_alive.push_back(1);
         commit_topology(h, h->topos.back(), prep[i]);
         topo_ids[i] = (int)h->topos.size() - 1;
     }
@@ -665,6 +744,7 @@ int smr_add_topology(smr_handle* h, const smr_topology_desc* d, int* topo_id) {
                             d->ninv, d->invs, d->invp, T, msg, sizeof(msg)))
         return fail(h, SMR_ERR_ARG, "topology: %s", msg);
     h->topos.push_back(std::move(T));
+    h->topo_alive.push_back(1);
     append_topology(h, h->topos.back());
     int r = upload_all(h);
     if (r) return r;
@@ -702,7 +782,8 @@ int smr_add_systems(smr_handle* h, int nsys, const int* topo_ids, const float* p
     if ((int)h->free_slots.size() < nsys) return fail(h, SMR_ERR_CAPACITY, "only %zu free slots for %d systems", h->free_slots.size(), nsys);
     long long need = 0;
     for (int i = 0; i < nsys; i++) {
-        if (topo_ids[i] < 0 || topo_ids[i] >= (int)h->topos.size()) return fail(h, SMR_ERR_ARG, "system %d: unknown topology %d", i, topo_ids[i]);
+        if (topo_ids[i] < 0 || topo_ids[i] >= (int)h->topos.size() || !h->topo_alive[topo_ids[i]])
+            return fail(h, SMR_ERR_ARG, "system %d: unknown topology %d", i, topo_ids[i]);
         need += h->topos[topo_ids[i]].n;
     }
     std::vector<int> ids(nsys), src(nsys), len(nsys), dst(nsys);
@@ -803,7 +884,8 @@ int smr_eval_forces(smr_handle* h, int nsys, const int* slot_ids, float* forces,
     if (nsys == 0) return SMR_OK;
     std::vector<int> sorted(slot_ids, slot_ids + nsys);
     auto segs = group_by(h, sorted, h->eval_form, h->eval_team);
-    for (auto& g : segs) { int r = check_smem(h, g); if (r) return r; }
+    std::vector<size_t> goff, glen;
+    { int r = reserve_gscratch(h, plan_gscratch(h, segs, goff, glen)); if (r) return r; }
     std::vector<int> pos_in_input(h->max_systems);
     for (int i = 0; i < nsys; i++) pos_in_input[slot_ids[i]] = i;
     cudaStream_t s = h->stream;
@@ -811,8 +893,10 @@ int smr_eval_forces(smr_handle* h, int nsys, const int* slot_ids, float* forces,
     KernelArgs a = base_args(h);
     h->last_launches = 0;
     cudaEventRecord(h->ev0, s);
-    for (auto& g : segs) {
+    for (size_t j = 0; j < segs.size(); j++) {
+        const Seg& g = segs[j];
         a.work = h->work + g.begin; a.nwork = g.end - g.begin; a.nmax = g.nmax; a.nfmax = g.nfmax;
+        a.gscratch = glen[j] ? h->gscr.d + goff[j] : nullptr; a.gscratch_bytes = glen[j];
         a.ecomp = h->ecomp + (size_t)g.begin * 8;
         CU(h, cudaMemsetAsync(h->counter, 0, 4, s));
         int r = launch_relax(a, g.team, g.form, 1, s, h->num_sms, &h->last_launches);
@@ -921,11 +1005,17 @@ int smr_run_fire(smr_handle* h, int max_steps, int step_budget, const smr_fire_p
     std::vector<std::vector<int>> sids(nst, ids);
     std::vector<std::vector<Seg>> ssegs(nst);
     for (int k = 0; k < nst; k++) ssegs[k] = group_by(h, sids[k], h->stage_form[k], h->stage_team[k]);
-    for (auto& sg : ssegs) for (auto& g : sg) { r = check_smem(h, g); if (r) return r; }
+    std::vector<std::vector<size_t>> goff(nst), glen(nst);
+    size_t gneed = 0;
+    for (int k = 0; k < nst; k++) gneed = std::max(gneed, plan_gscratch(h, ssegs[k], goff[k], glen[k]));
+    r = reserve_gscratch(h, gneed);
+    if (r) return r;
     cudaEventRecord(h->ev0, s);
-    auto launch = [&](const Seg& g, const int* work_base, int limit, int nwork_override, cudaStream_t ls, int* counter) -> int {
+    auto launch = [&](const Seg& g, const int* work_base, int limit, int nwork_override, cudaStream_t ls, int* counter,
+                      size_t goffset, size_t gbytes) -> int {
         a.work = work_base + g.begin; a.nwork = nwork_override > 0 ? nwork_override : g.end - g.begin;
         a.nmax = g.nmax; a.nfmax = g.nfmax; a.phase_limit = limit; a.counter = counter;
+        a.gscratch = gbytes ? h->gscr.d + goffset : nullptr; a.gscratch_bytes = gbytes;
         CU(h, cudaMemsetAsync(counter, 0, 4, ls));
         int e = launch_relax(a, g.team, g.form, 0, ls, h->num_sms, &h->last_launches);
         if (e) return fail(h, SMR_ERR_CUDA, "relax launch: %s", cudaGetErrorString((cudaError_t)e));
@@ -938,12 +1028,12 @@ int smr_run_fire(smr_handle* h, int max_steps, int step_budget, const smr_fire_p
             if (sids[k].empty()) continue;
             CU(h, cudaMemcpyAsync(h->work, sids[k].data(), sids[k].size() * 4, cudaMemcpyHostToDevice, s));
             const int m = (int)ssegs[k].size();
-            if (m == 1) { r = launch(ssegs[k][0], h->work, stage_end(k), 0, s, h->counter); if (r) return r; continue; }
+            if (m == 1) { r = launch(ssegs[k][0], h->work, stage_end(k), 0, s, h->counter, goff[k][0], glen[k][0]); if (r) return r; continue; }
             CU(h, cudaEventRecord(h->ev_fork, s));
             const int nside = std::min(m, smr_handle::kSide);
             for (int j = 0; j < nside; j++) CU(h, cudaStreamWaitEvent(h->side[j], h->ev_fork, 0));
             for (int j = 0; j < m; j++) {
-                r = launch(ssegs[k][j], h->work, stage_end(k), 0, h->side[j % nside], h->counter + (j % nside));
+                r = launch(ssegs[k][j], h->work, stage_end(k), 0, h->side[j % nside], h->counter + (j % nside), goff[k][j], glen[k][j]);
                 if (r) return r;
             }
             for (int j = 0; j < nside; j++) {
@@ -958,15 +1048,21 @@ int smr_run_fire(smr_handle* h, int max_steps, int step_budget, const smr_fire_p
             const int slot = ids[kk];
             const SlotState& st = h->hs[slot];
             std::vector<Seg> per_stage(nst);
+            std::vector<size_t> pglen(nst, 0);
             for (int k = 0; k < nst; k++) {
                 std::vector<int> one{slot};
                 per_stage[k] = group_by(h, one, h->stage_form[k], h->stage_team[k])[0];
                 per_stage[k].begin = kk; per_stage[k].end = kk + 1;
+                std::vector<size_t> o1, l1;
+                std::vector<Seg> g1{per_stage[k]};
+                pglen[k] = plan_gscratch(h, g1, o1, l1);
+                r = reserve_gscratch(h, pglen[k]);
+                if (r) return r;
             }
             for (int steps = start[slot]; steps < st.target; steps++) {
                 int k = 0;
                 while (k + 1 < nst && steps >= h->stage_start[k + 1]) k++;
-                r = launch(per_stage[k], h->work, steps + 1, 1, s, h->counter);
+                r = launch(per_stage[k], h->work, steps + 1, 1, s, h->counter, 0, pglen[k]);
                 if (r) return r;
                 int stt = 0;
                 CU(h, cudaMemcpyAsync(&stt, &h->slots[slot].status, 4, cudaMemcpyDeviceToHost, s));
@@ -1057,7 +1153,28 @@ int smr_download_pos64(smr_handle* h, int nsys, const int* slot_ids, double* pos
     return SMR_OK;
 }
 
-struct smr_topo { HostTopo T; };
+struct smr_topo { HostTopo T; PreparedTopo prep; bool prepared = false; };
+
+int smr_topo_prepare(smr_topo* t, int team) {
+    if (!t) return SMR_ERR_ARG;
+    if (team == 0) team = default_team(t->T.n);
+    if (team != 32 && team != 64 && team != 128 && team != 256 && team != 512) return SMR_ERR_ARG;
+    prepare_topology(t->T, team, t->prep);
+    t->prepared = true;
+    return SMR_OK;
+}
+
+int smr_remove_topology(smr_handle* h, int id) {
+    if (!h || id < 0 || id >= (int)h->topos.size() || !h->topo_alive[id]) return fail(h, SMR_ERR_ARG, "topology %d not live", id);
+    for (int s = 0; s < h->max_systems; s++)
+        if (h->hs[s].active && h->hs[s].topo == id) return fail(h, SMR_ERR_STATE, "topology %d is used by slot %d", id, s);
+    h->topo_alive[id] = 0;
+    h->dead_atoms += h->topos[id].n;
+    h->topos[id] = HostTopo{};
+    const size_t live = h->hreq.size() - h->dead_atoms;
+    if (h->dead_atoms > 4096 && h->dead_atoms > live) return compact_topologies(h);
+    return SMR_OK;
+}
 
 int smr_topo_build(int natoms, const int* Z, const double* pos, const double* charges, double bond_cut, smr_topo** out,
                    char* err, int errlen) {
@@ -1116,7 +1233,10 @@ int smr_topo_rounds(const smr_topo* t, int team, int rounds[3], short* ang_at, s
 int smr_add_topo(smr_handle* h, const smr_topo* t, int* topo_id) {
     if (!h || !t || !topo_id) return SMR_ERR_ARG;
     h->topos.push_back(t->T);
-    append_topology(h, h->topos.back());
+    h->topo_alive.push_back(1);
+    const int team = team_for(h, t->T.n);
+    if (t->prepared && t->prep.team == team) commit_topology(h, h->topos.back(), t->prep);   // packed off the handle
+    else append_topology(h, h->topos.back());
     int r = upload_all(h);
     if (r) return r;
     *topo_id = (int)h->topos.size() - 1;

@@ -755,7 +755,11 @@ relax_kernel(const KernelArgs a) {
     extern __shared__ __align__(16) char smem[];
     const int team = (T == 32) ? (threadIdx.x >> 5) : 0;
     const int rank = (T == 32) ? (threadIdx.x & 31) : threadIdx.x;
-    const Smem S = carve(smem + (size_t)team * team_bytes(a.nmax, a.nfmax, T, FORM), a.nmax);
+    const size_t tb = team_bytes(a.nmax, a.nfmax, T, FORM);
+    // the team's state: shared memory, or for systems too large for it a slot of the global
+    // scratch (team syncs order global memory within the block just as shared memory)
+    char* tbase = a.gscratch ? a.gscratch + ((size_t)blockIdx.x * (T == 32 ? 4 : 1) + team) * tb : smem + (size_t)team * tb;
+    const Smem S = carve(tbase, a.nmax);
     __shared__ int s_w;
     for (;;) {
         int w;
@@ -777,7 +781,8 @@ template <int T, int GDT, bool EVAL, int FORM>
 int launch_t(const KernelArgs& a, cudaStream_t s, int num_sms) {
     const int tpb = (T == 32) ? 4 : 1;           // teams per block
     const int block = T * tpb;
-    const size_t smem = (size_t)tpb * team_bytes(a.nmax, a.nfmax, T, FORM);
+    const size_t state = (size_t)tpb * team_bytes(a.nmax, a.nfmax, T, FORM);
+    const size_t smem = a.gscratch ? 0 : state;   // global-state launches use no dynamic shared memory
     auto kern = relax_kernel<T, GDT, EVAL, FORM>;
     static std::map<size_t, int> occ_cache;
     int occ;
@@ -797,6 +802,7 @@ int launch_t(const KernelArgs& a, cudaStream_t s, int num_sms) {
     if (occ < 1) return (int)cudaErrorInvalidConfiguration;
     int blocks_needed = (a.nwork + tpb - 1) / tpb;
     int grid = min(blocks_needed, occ * num_sms);
+    if (a.gscratch) grid = min(grid, (int)(a.gscratch_bytes / state));   // one scratch slot per block
     if (grid < 1) grid = 1;
     kern<<<grid, block, smem, s>>>(a);
     return (int)cudaGetLastError();

@@ -102,6 +102,10 @@ struct KernelArgs {
     const float4* own_par;        // owner form: term parameters
     const int* own_meta;          // owner form, per atom: n_ang | n_inv << 8 | n_dih << 16 | back slots << 24
     int nb_lanes;                 // lanes per atom in the NB partner loop (0: chosen from N and the team)
+    // systems too large for shared memory: each team's state lives in this global buffer instead
+    // (team k of the launch at k * team bytes); null for shared-memory launches
+    char* gscratch;
+    size_t gscratch_bytes;
 };
 
 // ---- host topology (topology.cpp)

@@ -114,6 +114,12 @@ class Topology:
         out["types"] = [type_name(t) for t in out["type_id"]]
         return out
 
+    def prepare(self, team=0):
+        """Pack the term records for a team size off any handle (thread-safe; releases the GIL)."""
+        r = N.lib().smr_topo_prepare(self.h, int(team))
+        if r != 0:
+            raise SmrError(f"smr_topo_prepare ({r})")
+
     def rounds(self, team):
         L = N.lib()
         r = (C.c_int * 3)()
@@ -255,6 +261,9 @@ class RelaxMulti:
         self._chk(self.L.smr_add_topo(self.h, topo.h, C.byref(tid)), "smr_add_topo")
         self.topo_n.append(topo.n)
         return tid.value
+
+    def remove_topology(self, tid):
+        self._chk(self.L.smr_remove_topology(self.h, int(tid)), "smr_remove_topology")
 
     def add_topology(self, req, neighs, bond_kl, angs=None, angp=None, dihs=None, dihp=None, invs=None, invp=None):
         req = _d(req)

@@ -96,3 +96,34 @@ def test_autotuner_runs_and_applies(setup):
         assert np.all(np.isfinite(np.concatenate(out["pos"])))
     finally:
         R.finish()
+
+
+def test_large_systems_global_state(setup, oracle):
+    """Systems whose team state exceeds shared memory (1800 atoms: ~280 KB) keep it in global memory:
+    forces match the oracle, and batched (mixed with a shared-memory system) and plain runs agree bit
+    for bit."""
+    from oracle import oracle as O
+    from tests.gpu_helpers import molecule_on_slab
+    slab, dims, p0, step, _ = setup
+    rng = np.random.default_rng(1800)
+    mols = [molecule_on_slab(rng, n, slab) for n in (1800, 1200)]
+    assert len(mols[0][0]) > 1500
+    R = make_handle(8, 8000, slab, dims, p0, step, rcut=10.0)
+    try:
+        g = R.get_grid()
+        tids = [R.add_molecule(Z, P, q) for Z, P, q in mols]
+        s = R.add_systems(tids, [m[1] for m in mols])
+        F, _ = R.eval_forces(s)
+        for i, (Z, P, q) in enumerate(mols):
+            Fo, _, _ = O.System.from_molecule(Z, P, q).eval(P.astype(np.float32).astype(np.float64),
+                                                            O.Grid(g["coef"], g["p0"], g["step"]), rcut=10.0)
+            assert force_err(F[i], Fo) < F_RTOL, (len(Z), force_err(F[i], Fo))
+        R.run_fire(30, step_budget=30, fconv=1e-6)
+        mix = R.download(s)
+        R.remove_systems(s)
+        c = R.add_systems([tids[0]], [mols[0][1]])
+        R.run_fire(30, step_budget=30, fconv=1e-6, mode=1)
+        plain = R.download(c)
+        assert np.array_equal(mix["pos"][0], plain["pos"][0]) and plain["steps"][0] == 30
+    finally:
+        R.finish()
