@@ -477,6 +477,151 @@ def run_ragged(args, ws, rank, local):
     return 0
 
 
+# ---------------------------------------------------------------------------------------- served workload
+SERVE = dict(nmin=20, nmax=2000, rcut=10.0, fconv=1e-4, max_steps=3000, chunk=200, budget_gb=150.0,
+             rates=(2000.0, 10000.0, 50000.0), per_rate=1500, max_systems=2048, plain_sample=8)
+
+
+def run_serve(args, local):
+    from surfmol_b200 import synth
+    slab, g = synth.config3_slab_grid()
+    per = args.nsys or SERVE["per_rate"]
+    workers = min(32, os.cpu_count() or 1)
+    # every request stream generated up front in a spawned pool, before any CUDA work
+    streams = {"warm": synth.serve_requests(SEED + 1, 64, 1e5, slab, SERVE["nmin"], SERVE["nmax"], workers),
+               "plain": synth.serve_requests(SEED + 999, SERVE["plain_sample"], 1e5, slab, SERVE["nmin"], SERVE["nmax"])}
+    for k, rate in enumerate(SERVE["rates"]):
+        streams[k] = synth.serve_requests(SEED + 100 + k, per, rate, slab, SERVE["nmin"], SERVE["nmax"], workers)
+    import torch
+    from surfmol_b200 import RelaxMulti
+    from surfmol_b200.relax import GRID_F16
+    from surfmol_b200.serve import Request, Server
+    torch.cuda.set_device(local)
+    fire = dict(FIRE, fconv=SERVE["fconv"])
+    max_atoms = SERVE["max_systems"] * 1200
+    R = RelaxMulti(max_systems=SERVE["max_systems"], max_atoms=max_atoms, device=local)
+    R.set_nb(rdamp=1.0, alpha_morse=1.5, rcut=SERVE["rcut"])
+    t0 = time.perf_counter()
+    R.build_grid(slab.ions, slab.req()[:, :2], slab.Lx, slab.Ly, g.nx, g.ny, g.nz, g.p0, g.step, alpha_morse=1.5,
+                 npbc=1, dtype=GRID_F16)
+    tgrid = time.perf_counter() - t0
+    srv = Server(R, SERVE["max_systems"], max_atoms, SERVE["budget_gb"] * 1e9, chunk_steps=SERVE["chunk"],
+                 max_steps=SERVE["max_steps"], fire=fire, typers=min(16, os.cpu_count() or 1))
+
+    def reqs(key):
+        return [Request(i, Z, P, q, t) for i, (Z, P, q, t) in enumerate(streams[key])]
+    srv.run(reqs("warm"))                                  # warm-up: loads every kernel shape
+    points = []
+    for k, rate in enumerate(SERVE["rates"]):
+        rq = reqs(k)
+        st = srv.run(rq)
+        d = st.summary()
+        d.update(rate_req_s=rate, atoms_mean=float(np.mean([len(r.Z) for r in rq])),
+                 converged_fraction=float(np.mean([r.status == 1 for r in rq])))
+        points.append(d)
+        print(json.dumps({"serve_point": d}), file=sys.stderr, flush=True)
+    # the plain form: each request alone, one kernel launch per FIRE step
+    rq = reqs("plain")
+    tp = time.perf_counter()
+    for r in rq:
+        s = R.add_systems([R.add_molecule(r.Z, r.pos, r.q)], [r.pos])
+        R.run_fire(SERVE["max_steps"], step_budget=SERVE["max_steps"], mode=1, **fire)
+        R.remove_systems(s)
+    tp = time.perf_counter() - tp
+    plain = {"requests": len(rq), "wall_s": tp, "throughput_req_s": len(rq) / tp,
+             "atoms_mean": float(np.mean([len(r.Z) for r in rq]))}
+    best = max(p["throughput_req_s"] for p in points)
+    line = {"metric": METRIC, "value": best, "unit": "requests/s", "n_gpus": 1, "higher_is_better": True,
+            "dtype": "f32 (fp16 grid)", "data": "synthetic",
+            "config": {"workload": f"served: Poisson arrivals at {list(SERVE['rates'])} req/s, {per} requests per rate, "
+                                   f"molecules log-uniform {SERVE['nmin']}-{SERVE['nmax']} atoms, fp16 grid "
+                                   f"{g.nx}x{g.ny}x{g.nz} of a 3-layer 16x16-cell NaCl(100) slab, intramolecular cutoff "
+                                   f"{SERVE['rcut']} A, FIRE to {SERVE['fconv']} or {SERVE['max_steps']} steps, "
+                                   f"chunks of {SERVE['chunk']} steps, HBM budget {SERVE['budget_gb']} GB",
+                       "grid_build_s": round(tgrid, 2)},
+            "serve": points, "plain": plain, "served_over_plain": best / plain["throughput_req_s"]}
+    R.finish()
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------------------- grid precision
+PREC = dict(nsys=8192, nmin=20, nmax=400, rcut=10.0, fconv=1e-4, max_steps=3000, sample=256)
+
+
+def run_precision(args, local):
+    """Config-3 grid (3-layer 16x16-cell slab, 904x904x160) stored as FP32, FP16 and BF16 with
+    per-channel scales: relax the same molecules on each and report the force / energy error
+    against the FP64 oracle (evaluated on the FP32 coefficients) at the same positions."""
+    from surfmol_b200 import synth
+    slab, g = synth.config3_slab_grid()
+    nsys = args.nsys or PREC["nsys"]
+    w = synth.ragged(SEED + 3, nsys, PREC["nmin"], PREC["nmax"], ncell=16, nlayers=3, nz=160,
+                     workers=min(32, os.cpu_count() or 1))
+    import torch
+    from oracle import oracle as O
+    from surfmol_b200 import RelaxMulti
+    from surfmol_b200.relax import GRID_BF16, GRID_F16, GRID_F32
+    torch.cuda.set_device(local)
+    natoms = np.array([len(z) for z in w.Z])
+    fire = dict(FIRE, fconv=PREC["fconv"])
+    R = RelaxMulti(max_systems=nsys, max_atoms=int(natoms.sum()), device=local)
+    R.set_nb(rdamp=1.0, alpha_morse=1.5, rcut=PREC["rcut"])
+    t0 = time.perf_counter()
+    R.build_grid(slab.ions, slab.req()[:, :2], slab.Lx, slab.Ly, g.nx, g.ny, g.nz, g.p0, g.step, alpha_morse=1.5, npbc=1)
+    tgrid = time.perf_counter() - t0
+    gd = R.get_grid()
+    og = O.Grid(gd["coef"], gd["p0"], gd["step"])
+    tids = R.add_molecules(w.Z, w.pos, w.q)
+    slots = R.add_systems(tids, w.pos)
+    pick = np.linspace(0, nsys - 1, min(nsys, PREC["sample"])).astype(int)
+    osys = {int(i): O.System.from_molecule(w.Z[i], w.pos[i], w.q[i]) for i in pick}
+    nb = dict(rdamp=1.0, alpha=1.5, rcut=PREC["rcut"])
+    relaxed = None
+    variants = {}
+    for name, dt in (("f32", GRID_F32), ("f16", GRID_F16), ("bf16", GRID_BF16)):
+        R.set_grid(gd["coef"], gd["p0"], gd["step"])          # from the FP32 coefficients each time
+        if dt != GRID_F32:
+            R.convert_grid(dt)
+        scale = R.get_grid()["scale"] if dt != GRID_F32 else np.ones(4)
+        R.set_positions(slots, w.pos)
+        R.reset_fire(slots)
+        R.run_fire(PREC["max_steps"], step_budget=PREC["max_steps"], **fire)
+        ms = R.last_timing()[0]
+        st = R.download(slots, pos=False, forces=False)
+        if relaxed is None:
+            relaxed = R.download_pos64([slots[i] for i in pick])
+        errs = {}
+        for label, P in (("start", [w.pos[i].astype(np.float32).astype(np.float64) for i in pick]), ("relaxed", relaxed)):
+            sel = [slots[i] for i in pick]
+            R.set_positions(sel, [p.astype(np.float32) for p in P])
+            F, E = R.eval_forces(sel)
+            fa, fr, er = [], [], []
+            for k, i in enumerate(pick):
+                P32 = P[k].astype(np.float32).astype(np.float64)
+                Fo, _, Eo = osys[int(i)].eval(P32, og, **nb)
+                d = np.abs(F[k][:, :3].astype(np.float64) - Fo).max()
+                fa.append(d)
+                fr.append(d / max(1.0, np.abs(Fo).max()))
+                er.append(abs(E[k, 0] - Eo[0]) / max(1.0, np.abs(Eo[1:7]).sum()))
+            errs[label] = {"force_abs_max": float(np.max(fa)), "force_abs_p99": float(np.percentile(fa, 99)),
+                           "force_rel_max": float(np.max(fr)), "energy_rel_max": float(np.max(er))}
+        variants[name] = {"grid_bytes": int(g.nx * g.ny * g.nz * (16 if dt == GRID_F32 else 8)),
+                          "channel_scales": [float(x) for x in scale], "relax_ms": ms, "systems_per_s": nsys / (ms * 1e-3),
+                          "converged_fraction": float((st["status"] == 1).mean()),
+                          "fire_steps_p50": float(np.median(st["steps"])), "error_vs_fp64_oracle": errs}
+        print(json.dumps({name: variants[name]}), file=sys.stderr, flush=True)
+    line = {"metric": "FP64-oracle force / energy error per grid storage type", "n_gpus": 1, "data": "synthetic",
+            "config": {"workload": f"{nsys} molecules log-uniform {PREC['nmin']}-{PREC['nmax']} atoms over a 3-layer "
+                                   f"16x16-cell NaCl(100) slab, grid {g.nx}x{g.ny}x{g.nz}; errors on {len(pick)} systems "
+                                   f"at their start and FP32-relaxed positions; FIRE to {PREC['fconv']} or {PREC['max_steps']}",
+                       "grid_build_s": round(tgrid, 2), "atoms_total": int(natoms.sum())},
+            "variants": variants}
+    R.finish()
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_ragged_dist(args):
     # the workload is generated in a spawned pool before CUDA and before the process group exists
     ws, rank, local = int(os.environ["WORLD_SIZE"]), int(os.environ["RANK"]), int(os.environ.get("LOCAL_RANK", "0"))
@@ -497,7 +642,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="uniform", choices=["uniform", "ragged"],
+    ap.add_argument("--workload", default="uniform", choices=["uniform", "ragged", "serve", "precision"],
                     help="uniform: 4096 replicas of the 40-atom molecule (default); ragged: 16384 molecules of 20-400 atoms")
     ap.add_argument("--nsys", type=int, default=0, help="systems per GPU (0: the workload's default)")
     ap.add_argument("--no-tune", action="store_true", help="ragged: skip the autotuner (library defaults)")
@@ -515,6 +660,10 @@ def main():
             return run_reference_ragged(args, ws, rank)
         args.nsys = args.nsys or 4096
         return run_reference(args, ws, rank)
+    if args.workload == "serve":
+        return run_serve(args, int(os.environ.get("LOCAL_RANK", "0")))
+    if args.workload == "precision":
+        return run_precision(args, int(os.environ.get("LOCAL_RANK", "0")))
     if args.workload == "ragged":
         ws = int(os.environ.get("WORLD_SIZE", "1"))
         rank = int(os.environ.get("RANK", "0"))

@@ -180,6 +180,16 @@ __device__ __forceinline__ void bspline(float u, float b[4], float d[4]) {
 
 __device__ __forceinline__ int imod(int i, int m) { int r = i % m; return r < 0 ? r + m : r; }
 
+// Cutoff decision for a pair whose FP32 r^2 lies within 1e-4 of rc^2: the squared distance from
+// the exact coordinate differences in FP64, as the CPU evaluators compute it.  Not inlined: the
+// rare path keeps its registers out of the partner loop.
+__device__ __noinline__ bool beyond_cutoff_fp64(float4 pi, float4 li, float4 pj, float4 lj, float rc2) {
+    const double dx = ((double)pj.x - (double)pi.x) + ((double)lj.x - (double)li.x);
+    const double dy = ((double)pj.y - (double)pi.y) + ((double)lj.y - (double)li.y);
+    const double dz = ((double)pj.z - (double)pi.z) + ((double)lj.z - (double)li.z);
+    return dx * dx + dy * dy + dz * dz > (double)rc2;
+}
+
 // lanes per atom for the NB partner loop: minimise passes x partners per lane
 __device__ __forceinline__ int nb_lanes(int N, int T) {
     int best = 1; long long bc = 1LL << 60;
@@ -527,8 +537,11 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
                     const float4 qj = S.Q()[j];
                     const float dx = (pj.x - pi.x) + (lj.x - li.x), dy = (pj.y - pi.y) + (lj.y - li.y), dz = (pj.z - pi.z) + (lj.z - li.z);
                     float r2 = dx * dx + dy * dy + dz * dz;
+                    bool out = r2 > a.rc2;
+                    // at the cutoff: decide in FP64, so FP32 rounding never moves a pair across it
+                    if (fabsf(r2 - a.rc2) < 1e-4f * a.rc2) out = beyond_cutoff_fp64(pi, li, pj, lj, a.rc2);
                     const bool skip = (small ? (bool)((ex >> j) & 1ull)
-                                             : (j == i || j == ng.x || j == ng.y || j == ng.z || j == ng.w)) || r2 > a.rc2;
+                                             : (j == i || j == ng.x || j == ng.y || j == ng.z || j == ng.w)) || out;
                     r2 = skip ? 1.0f : r2;
                     const float R0 = qi.x + qj.x, E0 = qi.y * qj.y, Q = qi.z * qj.z;
                     const float rs = rsqrtf(r2 + a.R2damp);          // 1/sqrt(r^2 + Rdamp^2)

@@ -78,7 +78,7 @@ class ServeStats:
 class Server:
     def __init__(self, R: RelaxMulti, max_systems: int, max_atoms: int, hbm_budget_bytes: float,
                  chunk_steps: int = 200, max_steps: int = 3000, fire: dict | None = None,
-                 bytes_per_atom: int = BYTES_PER_ATOM, keep_pos64: bool = False):
+                 bytes_per_atom: int = BYTES_PER_ATOM, keep_pos64: bool = False, typers: int = 8):
         self.R = R
         self.max_systems = max_systems
         self.max_atoms = max_atoms
@@ -88,21 +88,44 @@ class Server:
         self.fire = dict(fire or {})
         self.bpa = int(bytes_per_atom)
         self.keep_pos64 = keep_pos64
+        self.typers = max(1, int(typers))
 
-    # -- background typing: Topology objects for arrived requests, in arrival order
+    # -- background typing: Topology objects of arrived requests, made by a pool of host threads
+    #    (the native typing and packing release the GIL) and queued as they complete
     def _typer(self, reqs, t0, out: queue.Queue, stop: threading.Event):
-        for r in reqs:
+        lock = threading.Lock()
+        nxt = [0]
+        left = [self.typers]
+
+        def work():
             while not stop.is_set():
-                dt = r.arrival - (time.perf_counter() - t0)
-                if dt <= 0:
+                with lock:
+                    i = nxt[0]
+                    nxt[0] += 1
+                if i >= len(reqs):
                     break
-                time.sleep(min(dt, 0.005))
-            if stop.is_set():
-                return
-            topo = Topology(r.Z, r.pos, r.q)
-            topo.prepare(0)
-            out.put((r, topo))
-        out.put(None)
+                r = reqs[i]
+                while not stop.is_set():
+                    dt = r.arrival - (time.perf_counter() - t0)
+                    if dt <= 0:
+                        break
+                    time.sleep(min(dt, 0.002))
+                if stop.is_set():
+                    break
+                topo = Topology(r.Z, r.pos, r.q)
+                topo.prepare(0)
+                out.put((r, topo))
+            with lock:
+                left[0] -= 1
+                last = left[0] == 0
+            if last:
+                out.put(None)
+
+        pool = [threading.Thread(target=work, daemon=True) for _ in range(self.typers)]
+        for t in pool:
+            t.start()
+        for t in pool:
+            t.join()
 
     def run(self, requests: list[Request]) -> ServeStats:
         """Serve the requests (sorted by arrival) in real time; returns the statistics.  Each
@@ -132,6 +155,7 @@ class Server:
                         typer_done = True
                         break
                     waiting.append(item)
+                    waiting.sort(key=lambda x: x[0].arrival)
                     if not resident:
                         break
                 # admit in arrival order while slots, atoms and the HBM budget allow

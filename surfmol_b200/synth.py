@@ -289,3 +289,35 @@ def ragged(seed: int, nsys: int, nmin: int = 20, nmax: int = 400, ncell: int = 8
     Ps = [o[1] for o in out]
     Qs = [o[2] for o in out]
     return Workload(Zs, Ps, Qs, np.arange(nsys, dtype=np.int32), slab, g, seed)
+
+
+def config3_slab_grid():
+    """3-layer 16x16-cell NaCl(100) slab and its 904 x 904 x 160 grid (~0.1 A, z over 16 A)."""
+    slab = rocksalt_slab(16, 3)
+    nx = ny = 904
+    return slab, GridSpec(nx, ny, 160, (0.0, 0.0, slab.z_top + 1.0), (slab.Lx / nx, slab.Ly / ny, 0.1))
+
+
+def _serve_one(args):
+    seed, i, nmin, nmax, Lx, Ly, z_top = args
+    r = np.random.default_rng([seed, i])
+    target = int(round(math.exp(r.uniform(math.log(nmin), math.log(nmax)))))
+    mol = ragged_molecule(r, target)
+    q = charges(r, mol.n)
+    return mol.Z, place(r, mol, (r.uniform(0, Lx), r.uniform(0, Ly)), r.uniform(2.5, 4.0), z_top=z_top), q
+
+
+def serve_requests(seed: int, n: int, rate: float, slab: Slab, nmin: int = 20, nmax: int = 2000, workers: int = 0):
+    """n requests with Poisson arrivals at `rate` per second: (Z, pos, q, arrival) of molecules with
+    log-uniform atom counts in [nmin, nmax]; request i is drawn from its own generator (seed, i).
+    workers > 1 generates in a spawned process pool (call it before any CUDA work)."""
+    rng = np.random.default_rng([seed, 1 << 20])
+    t = np.cumsum(rng.exponential(1.0 / rate, n))
+    jobs = [(seed, i, nmin, nmax, slab.Lx, slab.Ly, slab.z_top) for i in range(n)]
+    if workers > 1 and n > 8:
+        import multiprocessing as mp
+        with mp.get_context("spawn").Pool(workers) as pool:
+            mols = pool.map(_serve_one, jobs, chunksize=max(1, n // (8 * workers)))
+    else:
+        mols = [_serve_one(j) for j in jobs]
+    return [(Z, P, q, float(t[i])) for i, (Z, P, q) in enumerate(mols)]
