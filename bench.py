@@ -125,14 +125,11 @@ def dist_init():
 
 
 def barrier_max(ws, value):
-    """Barrier + max over ranks of a float (device time)."""
+    """Max over ranks of a float (device time); the all-reduce is also the barrier."""
     if ws == 1:
         return value
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from surfmol_b200.shard import max_over_ranks
+    return max_over_ranks(value)
 
 
 def make_workload(seed, nsys):
