@@ -476,7 +476,7 @@ def run_ragged(args, ws, rank, local):
 
 # ---------------------------------------------------------------------------------------- served workload
 SERVE = dict(nmin=20, nmax=2000, rcut=10.0, fconv=1e-4, max_steps=3000, chunk=200, budget_gb=150.0,
-             rates=(2000.0, 10000.0, 50000.0), per_rate=1500, max_systems=2048, plain_sample=8)
+             rates=(2000.0, 10000.0, 50000.0), per_rate=1500, max_systems=2048, plain_sample=8, resident=0)
 
 
 def run_serve(args, local):
@@ -502,7 +502,8 @@ def run_serve(args, local):
     R.build_grid(slab.ions, slab.req()[:, :2], slab.Lx, slab.Ly, g.nx, g.ny, g.nz, g.p0, g.step, alpha_morse=1.5,
                  npbc=1, dtype=GRID_F16)
     tgrid = time.perf_counter() - t0
-    srv = Server(R, SERVE["max_systems"], max_atoms, SERVE["budget_gb"] * 1e9, chunk_steps=SERVE["chunk"],
+    resident = args.resident or SERVE["resident"] or SERVE["max_systems"]
+    srv = Server(R, resident, max_atoms, SERVE["budget_gb"] * 1e9, chunk_steps=SERVE["chunk"],
                  max_steps=SERVE["max_steps"], fire=fire, typers=min(16, os.cpu_count() or 1))
 
     def reqs(key):
@@ -535,7 +536,7 @@ def run_serve(args, local):
                                    f"{g.nx}x{g.ny}x{g.nz} of a 3-layer 16x16-cell NaCl(100) slab, intramolecular cutoff "
                                    f"{SERVE['rcut']} A, FIRE to {SERVE['fconv']} or {SERVE['max_steps']} steps, "
                                    f"chunks of {SERVE['chunk']} steps, HBM budget {SERVE['budget_gb']} GB",
-                       "grid_build_s": round(tgrid, 2)},
+                       "grid_build_s": round(tgrid, 2), "resident_cap": resident},
             "serve": points, "plain": plain, "served_over_plain": best / plain["throughput_req_s"]}
     R.finish()
     print(json.dumps(line), flush=True)
@@ -643,6 +644,7 @@ def main():
                     help="uniform: 4096 replicas of the 40-atom molecule (default); ragged: 16384 molecules of 20-400 atoms")
     ap.add_argument("--nsys", type=int, default=0, help="systems per GPU (0: the workload's default)")
     ap.add_argument("--no-tune", action="store_true", help="ragged: skip the autotuner (library defaults)")
+    ap.add_argument("--resident", type=int, default=0, help="serve: cap on resident systems (0: the handle's slots)")
     ap.add_argument("--ref-sample", type=int, default=64)
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")

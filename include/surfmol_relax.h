@@ -273,6 +273,14 @@ int smr_set_team_size(smr_handle* h, int max_atoms, int threads);
 int smr_set_tuning(smr_handle* h, int key, int value);
 int smr_get_tuning(smr_handle* h, int key, int* value);
 
+/* CUDA-graph replay of smr_run_fire's batched launch sequence (work-list copies, counter resets,
+ * one persistent launch per stage segment, the side-stream fork / join).  With it on, a call whose
+ * launch plan (systems, stages, segments, every kernel argument) equals the previous captured one
+ * replays that graph in a single launch; a new plan is captured, instantiated and launched.  Off
+ * by default.  smr_graph_stats: replays so far.  No counterpart in the reference. */
+int smr_set_graph(smr_handle* h, int on);
+int smr_graph_stats(smr_handle* h, long long* replays);
+
 #ifdef __cplusplus
 }
 #endif

@@ -92,6 +92,8 @@ SIGNATURES = {
     "smr_set_team_size": (C.c_int, [VP, C.c_int, C.c_int]),
     "smr_set_tuning": (C.c_int, [VP, C.c_int, C.c_int]),
     "smr_get_tuning": (C.c_int, [VP, C.c_int, IP]),
+    "smr_set_graph": (C.c_int, [VP, C.c_int]),
+    "smr_graph_stats": (C.c_int, [VP, LLP]),
     "smr_set_schedule": (C.c_int, [VP, C.c_int, C.c_int, C.c_int]),
     "smr_get_schedule": (C.c_int, [VP, IP, IP, IP]),
     "smr_set_stages": (C.c_int, [VP, C.c_int, IP, IP, IP, C.c_int]),

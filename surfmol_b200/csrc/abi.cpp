@@ -2,6 +2,7 @@
 // allocator, launches and transfers.  Host-side only; kernels live in relax.cu / grid.cu.
 #include <algorithm>
 #include <atomic>
+#include <cstdint>
 #include <chrono>
 #include <cstdarg>
 #include <cstdio>
@@ -119,6 +120,14 @@ struct smr_handle {
     smr_nb_params nb{1.0f, 1.5f, 0.0f, 0};
 
     DArr<char> gscr;                    // team state of systems too large for shared memory
+    // graph replay of the batched launch sequence: when a call repeats the previous call's launch
+    // plan (same systems, stages, segments and arguments) the plan is captured once and replayed
+    bool graph_on = false;
+    std::vector<long long> g_sig;          // plan of the captured graph
+    cudaGraphExec_t g_exec = nullptr;
+    long long g_launches = 0, g_replays = 0;
+    int* work_pinned = nullptr;          // per-stage work lists (pinned: captured copies read them)
+    size_t work_pinned_cap = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // the launch segments of one schedule stage (disjoint sets of systems, one team size each) run
     // concurrently on side streams, so one class's tail overlaps the next class's work
@@ -546,6 +555,8 @@ int smr_destroy(smr_handle* h) {
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    if (h->g_exec) cudaGraphExecDestroy(h->g_exec);
+    if (h->work_pinned) cudaFreeHost(h->work_pinned);
     for (int k = 0; k < smr_handle::kSide; k++) {
         if (h->side[k]) cudaStreamDestroy(h->side[k]);
         if (h->ev_join[k]) cudaEventDestroy(h->ev_join[k]);
@@ -975,6 +986,37 @@ int smr_get_schedule(smr_handle* h, int* switch_step, int* latency_team, int* ev
     return SMR_OK;
 }
 
+// every field a launch reads from its arguments, for comparing launch plans
+static void sig_args(std::vector<long long>& v, const KernelArgs& a) {
+    auto P = [&](const void* p) { v.push_back((long long)(uintptr_t)p); };
+    auto F = [&](float x) { int b; std::memcpy(&b, &x, 4); v.push_back(b); };
+    auto D = [&](double x) { long long b; std::memcpy(&b, &x, 8); v.push_back(b); };
+    P(a.work); v.push_back(a.nwork); P(a.counter); P(a.slots); P(a.topos); P(a.req); P(a.neigh); P(a.bk); P(a.bl);
+    P(a.angs); P(a.dihs); P(a.invs); P(a.pos); P(a.plo); P(a.vel); P(a.force);
+    P(a.grid.data); v.push_back(a.grid.dtype); v.push_back(a.grid.nx); v.push_back(a.grid.ny); v.push_back(a.grid.nz);
+    for (int k = 0; k < 3; k++) { F(a.grid.p0[k]); F(a.grid.inv_step[k]); }
+    for (int k = 0; k < 4; k++) F(a.grid.scale[k]);
+    v.push_back(a.has_grid); F(a.R2damp); F(a.alpha_morse); F(a.rc2);
+    D(a.fire.dt0); D(a.fire.dt_max); D(a.fire.alpha0); D(a.fire.f_inc); D(a.fire.f_dec); D(a.fire.f_alpha);
+    D(a.fire.fconv); D(a.fire.flimit); v.push_back(a.fire.n_min);
+    v.push_back(a.phase_limit); v.push_back(a.step_budget); P(a.ecomp); v.push_back(a.nmax); v.push_back(a.nfmax);
+    P(a.a2f); P(a.a2f_idx); P(a.own_geo); P(a.own_par); P(a.own_meta); v.push_back(a.nb_lanes);
+    P(a.gscratch); v.push_back((long long)a.gscratch_bytes);
+}
+
+int smr_set_graph(smr_handle* h, int on) {
+    if (!h) return SMR_ERR_ARG;
+    h->graph_on = on != 0;
+    if (!h->graph_on && h->g_exec) { cudaGraphExecDestroy(h->g_exec); h->g_exec = nullptr; h->g_sig.clear(); }
+    return SMR_OK;
+}
+
+int smr_graph_stats(smr_handle* h, long long* replays) {
+    if (!h || !replays) return SMR_ERR_ARG;
+    *replays = h->g_replays;
+    return SMR_OK;
+}
+
 int smr_run_fire(smr_handle* h, int max_steps, int step_budget, const smr_fire_params* p, int mode, int* nfinished) {
     if (!h || !p || max_steps < 0) return SMR_ERR_ARG;
     if (mode != SMR_MODE_BATCHED && mode != SMR_MODE_PLAIN) return fail(h, SMR_ERR_ARG, "unknown mode %d", mode);
@@ -1011,35 +1053,96 @@ int smr_run_fire(smr_handle* h, int max_steps, int step_budget, const smr_fire_p
     r = reserve_gscratch(h, gneed);
     if (r) return r;
     cudaEventRecord(h->ev0, s);
-    auto launch = [&](const Seg& g, const int* work_base, int limit, int nwork_override, cudaStream_t ls, int* counter,
-                      size_t goffset, size_t gbytes) -> int {
+    auto set_args = [&](const Seg& g, const int* work_base, int limit, int nwork_override, int* counter, size_t goffset, size_t gbytes) {
         a.work = work_base + g.begin; a.nwork = nwork_override > 0 ? nwork_override : g.end - g.begin;
         a.nmax = g.nmax; a.nfmax = g.nfmax; a.phase_limit = limit; a.counter = counter;
         a.gscratch = gbytes ? h->gscr.d + goffset : nullptr; a.gscratch_bytes = gbytes;
+    };
+    auto launch = [&](const Seg& g, const int* work_base, int limit, int nwork_override, cudaStream_t ls, int* counter,
+                      size_t goffset, size_t gbytes) -> int {
+        set_args(g, work_base, limit, nwork_override, counter, goffset, gbytes);
         CU(h, cudaMemsetAsync(counter, 0, 4, ls));
         int e = launch_relax(a, g.team, g.form, 0, ls, h->num_sms, &h->last_launches);
         if (e) return fail(h, SMR_ERR_CUDA, "relax launch: %s", cudaGetErrorString((cudaError_t)e));
         return 0;
     };
     if (mode == SMR_MODE_BATCHED) {
+        // work lists of all stages in pinned memory (copied on the stream; a captured graph reads them)
+        const size_t need = (size_t)nst * h->max_systems;
+        if (need > h->work_pinned_cap) {
+            if (h->work_pinned) cudaFreeHost(h->work_pinned);
+            h->work_pinned = nullptr; h->work_pinned_cap = 0;
+            CU(h, cudaMallocHost(&h->work_pinned, need * sizeof(int)));
+            h->work_pinned_cap = need;
+        }
+        for (int k = 0; k < nst; k++) std::copy(sids[k].begin(), sids[k].end(), h->work_pinned + (size_t)k * h->max_systems);
         // stages run in order (every stage's launches redistribute the systems still running over
         // the GPU); the segments of one stage hold disjoint systems and run concurrently
-        for (int k = 0; k < nst; k++) {
-            if (sids[k].empty()) continue;
-            CU(h, cudaMemcpyAsync(h->work, sids[k].data(), sids[k].size() * 4, cudaMemcpyHostToDevice, s));
-            const int m = (int)ssegs[k].size();
-            if (m == 1) { r = launch(ssegs[k][0], h->work, stage_end(k), 0, s, h->counter, goff[k][0], glen[k][0]); if (r) return r; continue; }
-            CU(h, cudaEventRecord(h->ev_fork, s));
-            const int nside = std::min(m, smr_handle::kSide);
-            for (int j = 0; j < nside; j++) CU(h, cudaStreamWaitEvent(h->side[j], h->ev_fork, 0));
-            for (int j = 0; j < m; j++) {
-                r = launch(ssegs[k][j], h->work, stage_end(k), 0, h->side[j % nside], h->counter + (j % nside), goff[k][j], glen[k][j]);
-                if (r) return r;
+        auto issue = [&]() -> int {
+            for (int k = 0; k < nst; k++) {
+                if (sids[k].empty()) continue;
+                CU(h, cudaMemcpyAsync(h->work, h->work_pinned + (size_t)k * h->max_systems, sids[k].size() * 4, cudaMemcpyHostToDevice, s));
+                const int m = (int)ssegs[k].size();
+                const int nside = std::min(m, smr_handle::kSide);
+                if (m > 1) {
+                    CU(h, cudaEventRecord(h->ev_fork, s));
+                    for (int j = 0; j < nside; j++) CU(h, cudaStreamWaitEvent(h->side[j], h->ev_fork, 0));
+                }
+                for (int j = 0; j < m; j++) {
+                    cudaStream_t ls = m == 1 ? s : h->side[j % nside];
+                    int* ctr = m == 1 ? h->counter : h->counter + (j % nside);
+                    r = launch(ssegs[k][j], h->work, stage_end(k), 0, ls, ctr, goff[k][j], glen[k][j]);
+                    if (r) return r;
+                }
+                if (m > 1)
+                    for (int j = 0; j < nside; j++) {
+                        CU(h, cudaEventRecord(h->ev_join[j], h->side[j]));
+                        CU(h, cudaStreamWaitEvent(s, h->ev_join[j], 0));
+                    }
             }
-            for (int j = 0; j < nside; j++) {
-                CU(h, cudaEventRecord(h->ev_join[j], h->side[j]));
-                CU(h, cudaStreamWaitEvent(s, h->ev_join[j], 0));
+            return 0;
+        };
+        if (!h->graph_on) {
+            r = issue();
+            if (r) return r;
+        } else {
+            // the launch plan of this call (work lists, segments, every kernel argument), without issuing
+            std::vector<long long> sig;
+            long long nlaunch = 0;
+            for (int k = 0; k < nst; k++) {
+                if (sids[k].empty()) continue;
+                sig.push_back(-1 - k);
+                sig.insert(sig.end(), sids[k].begin(), sids[k].end());
+                const int m = (int)ssegs[k].size();
+                const int nside = std::min(m, smr_handle::kSide);
+                for (int j = 0; j < m; j++) {
+                    set_args(ssegs[k][j], h->work, stage_end(k), 0, m == 1 ? h->counter : h->counter + (j % nside), goff[k][j], glen[k][j]);
+                    sig.push_back(ssegs[k][j].team); sig.push_back(ssegs[k][j].form); sig.push_back(m == 1 ? -1 : j % nside);
+                    sig_args(sig, a);
+                    nlaunch++;
+                }
             }
+            if (h->g_exec && sig == h->g_sig) {
+                h->g_replays++;                                    // the same plan: replay it
+            } else {
+                cudaGraph_t graph = nullptr;
+                const long long before = h->last_launches;
+                CU(h, cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+                r = issue();
+                cudaError_t ce = cudaStreamEndCapture(s, &graph);
+                h->last_launches = before;
+                if (r) { if (graph) cudaGraphDestroy(graph); return r; }
+                if (ce != cudaSuccess) return fail(h, SMR_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+                cudaGraphExec_t ex = nullptr;
+                cudaError_t ie = cudaGraphInstantiate(&ex, graph, 0);
+                cudaGraphDestroy(graph);
+                if (ie != cudaSuccess) return fail(h, SMR_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ie));
+                if (h->g_exec) cudaGraphExecDestroy(h->g_exec);
+                h->g_exec = ex;
+                h->g_sig.swap(sig);
+            }
+            CU(h, cudaGraphLaunch(h->g_exec, s));
+            h->last_launches += nlaunch;
         }
     } else {
         // plain form: one launch per system per FIRE step, status read back after each step

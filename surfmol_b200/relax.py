@@ -230,6 +230,15 @@ class RelaxMulti:
         self._chk(self.L.smr_get_tuning(self.h, 1, C.byref(v)), "smr_get_tuning")
         return v.value
 
+    def set_graph(self, on=True):
+        """Replay the batched launch sequence as a CUDA graph when a call repeats the last plan."""
+        self._chk(self.L.smr_set_graph(self.h, 1 if on else 0), "smr_set_graph")
+
+    def graph_replays(self):
+        v = C.c_longlong()
+        self._chk(self.L.smr_graph_stats(self.h, C.byref(v)), "smr_graph_stats")
+        return v.value
+
     def set_team_size(self, max_atoms, threads):
         self._chk(self.L.smr_set_team_size(self.h, max_atoms, threads), "smr_set_team_size")
 

@@ -127,3 +127,28 @@ def test_large_systems_global_state(setup, oracle):
         assert np.array_equal(mix["pos"][0], plain["pos"][0]) and plain["steps"][0] == 30
     finally:
         R.finish()
+
+
+def test_graph_replay_bitwise(setup):
+    """With graph replay on, a repeated relaxation call replays the captured launch sequence and gives
+    bit for bit the trajectories of directly issued launches (several stages, concurrent classes)."""
+    slab, dims, p0, step, mols = setup
+    R = make_handle(16, 4000, slab, dims, p0, step)
+    try:
+        tids = R.add_molecules([m[0] for m in mols], [m[1] for m in mols], [m[2] for m in mols])
+        s = R.add_systems(tids, [m[1] for m in mols])
+        R.set_stages([0, 30, 60], [0, 1, 1], [0, 64, 128])
+        outs = []
+        for graph in (False, True, True, True):
+            R.set_graph(graph)
+            R.set_positions(s, [m[1] for m in mols])
+            R.reset_fire(s)
+            R.run_fire(90, step_budget=90, fconv=1e-6)
+            assert R.last_timing()[1] > 0
+            outs.append(R.download(s))
+        assert R.graph_replays() == 2
+        for o in outs[1:]:
+            for i in range(len(mols)):
+                assert np.array_equal(o["pos"][i], outs[0]["pos"][i]) and o["steps"][i] == 90
+    finally:
+        R.finish()
