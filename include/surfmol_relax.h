@@ -270,6 +270,15 @@ int smr_set_team_size(smr_handle* h, int max_atoms, int threads);
  *   SMR_TUNE_NB_LANES  lanes per atom splitting the intramolecular NB partner loop
  *                      (1, 2, 4, 8, 16, 32; 0 = chosen from the system size and team) */
 #define SMR_TUNE_NB_LANES 1
+/*   SMR_TUNE_NBLIST_MIN     systems of at least this many atoms use NB neighbour lists during FIRE
+ *                           when a cutoff is set (default 128; 0 = never): partners within
+ *                           rc + skin, rebuilt when an atom has moved more than skin / 2
+ *   SMR_TUNE_NBLIST_SKIN_MA skin in milli-Angstrom (default 1000)
+ *   SMR_TUNE_NBLIST_CAP     partners per atom a list row holds (default 256; an atom with more
+ *                           uses the all-pairs loop) */
+#define SMR_TUNE_NBLIST_MIN 2
+#define SMR_TUNE_NBLIST_SKIN_MA 3
+#define SMR_TUNE_NBLIST_CAP 4
 int smr_set_tuning(smr_handle* h, int key, int value);
 int smr_get_tuning(smr_handle* h, int key, int* value);
 

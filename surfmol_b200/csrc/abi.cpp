@@ -108,6 +108,10 @@ struct smr_handle {
     int eval_form = FORM_ROUNDS;        // form and team (0: by size) of smr_eval_forces
     int eval_team = 0;
     int nb_lanes = 0;                   // tuning: lanes per atom of the NB loop (0: by size)
+    // NB neighbour lists for systems of at least nbl_min atoms under a cutoff (0: off)
+    int nbl_min = 128, nbl_cap = 256, nbl_skin_ma = 1000;
+    DArr<unsigned short> nbl; DArr<int> nbl_cnt; DArr<float4> nbl_ref;
+    bool nbl_ready = false;
 
     // grid
     void* grid = nullptr;
@@ -391,6 +395,10 @@ KernelArgs base_args(smr_handle* h) {
     a.a2f = h->da2f.d; a.a2f_idx = h->didx.d;
     a.own_geo = h->down_geo.d; a.own_par = h->down_par.d; a.own_meta = h->down_meta.d;
     a.nb_lanes = h->nb_lanes;
+    if (h->nbl_ready) {
+        a.nbl = h->nbl.d; a.nbl_cnt = h->nbl_cnt.d; a.nbl_ref = h->nbl_ref.d;
+        a.nbl_cap = h->nbl_cap; a.nbl_min = h->nbl_min; a.nbl_skin = 1e-3f * (float)h->nbl_skin_ma;
+    }
     a.pos = h->pos; a.plo = h->plo; a.vel = h->vel; a.force = h->force;
     a.has_grid = h->has_grid ? 1 : 0;
     a.grid.data = h->grid;
@@ -581,12 +589,33 @@ int smr_set_tuning(smr_handle* h, int key, int value) {
         h->nb_lanes = value;
         return SMR_OK;
     }
+    if (key == SMR_TUNE_NBLIST_MIN) {
+        if (value < 0) return fail(h, SMR_ERR_ARG, "neighbour-list size threshold must be >= 0");
+        h->nbl_min = value;
+        return SMR_OK;
+    }
+    if (key == SMR_TUNE_NBLIST_SKIN_MA) {
+        if (value < 50 || value > 5000) return fail(h, SMR_ERR_ARG, "neighbour-list skin must be 50..5000 mA");
+        h->nbl_skin_ma = value;
+        return SMR_OK;
+    }
+    if (key == SMR_TUNE_NBLIST_CAP) {
+        if (value < 32 || value > 4096) return fail(h, SMR_ERR_ARG, "neighbour-list capacity must be 32..4096");
+        if (h->nbl_ready && value != h->nbl_cap) {           // rows change shape: drop the lists
+            h->nbl_ready = false;
+        }
+        h->nbl_cap = value;
+        return SMR_OK;
+    }
     return fail(h, SMR_ERR_ARG, "unknown tuning key %d", key);
 }
 
 int smr_get_tuning(smr_handle* h, int key, int* value) {
     if (!h || !value) return SMR_ERR_ARG;
     if (key == SMR_TUNE_NB_LANES) { *value = h->nb_lanes; return SMR_OK; }
+    if (key == SMR_TUNE_NBLIST_MIN) { *value = h->nbl_min; return SMR_OK; }
+    if (key == SMR_TUNE_NBLIST_SKIN_MA) { *value = h->nbl_skin_ma; return SMR_OK; }
+    if (key == SMR_TUNE_NBLIST_CAP) { *value = h->nbl_cap; return SMR_OK; }
     return fail(h, SMR_ERR_ARG, "unknown tuning key %d", key);
 }
 
@@ -1036,6 +1065,22 @@ int smr_run_fire(smr_handle* h, int max_steps, int step_budget, const smr_fire_p
     }
     int r = upload_slots(h, ids);
     if (r) return r;
+    // neighbour lists: allocated (max_atoms rows, all marked for rebuild) the first time a running
+    // system is large enough under a cutoff
+    if (!h->nbl_ready && h->nbl_min > 0 && h->nb.rcut > 0) {
+        bool any = false;
+        for (int sl : ids) any = any || h->hs[sl].natoms >= h->nbl_min;
+        if (any) {
+            const size_t na = (size_t)h->max_atoms;
+            cudaError_t e = h->nbl.reserve(na * h->nbl_cap, 0, h->stream);
+            if (e == cudaSuccess) e = h->nbl_cnt.reserve(na, 0, h->stream);
+            if (e == cudaSuccess) e = h->nbl_ref.reserve(na, 0, h->stream);
+            if (e == cudaSuccess) e = cudaMemsetAsync(h->nbl_cnt.d, 0xff, na * sizeof(int), h->stream);
+            if (e == cudaSuccess) e = cudaMemsetAsync(h->nbl_ref.d, 0, na * sizeof(float4), h->stream);
+            if (e != cudaSuccess) return fail(h, SMR_ERR_CAPACITY, "neighbour lists (%zu atoms x %d): %s", na, h->nbl_cap, cudaGetErrorString(e));
+            h->nbl_ready = true;
+        }
+    }
     h->last_launches = 0;
     cudaStream_t s = h->stream;
     KernelArgs a = base_args(h);

@@ -190,6 +190,28 @@ __device__ __noinline__ bool beyond_cutoff_fp64(float4 pi, float4 li, float4 pj,
     return dx * dx + dy * dy + dz * dz > (double)rc2;
 }
 
+// One LJ + damped-Coulomb pair (getLJQH, opencl/UFF.cl:82-95) added to the force / energy of atom i;
+// excluded pairs and pairs beyond the cutoff are evaluated at r^2 = 1 and weighted 0.
+__device__ __forceinline__ void nb_pair(const KernelArgs& a, float4 pi, float4 li, float4 qi, float4 pj, float4 lj, float4 qj,
+                                        bool excluded, float& fx, float& fy, float& fz, float& E) {
+    const float dx = (pj.x - pi.x) + (lj.x - li.x), dy = (pj.y - pi.y) + (lj.y - li.y), dz = (pj.z - pi.z) + (lj.z - li.z);
+    float r2 = dx * dx + dy * dy + dz * dz;
+    bool out = r2 > a.rc2;
+    // at the cutoff: decide in FP64, so FP32 rounding never moves a pair across it
+    if (fabsf(r2 - a.rc2) < 1e-4f * a.rc2) out = beyond_cutoff_fp64(pi, li, pj, lj, a.rc2);
+    const bool skip = excluded || out;
+    r2 = skip ? 1.0f : r2;
+    const float R0 = qi.x + qj.x, E0 = qi.y * qj.y, Q = qi.z * qj.z;
+    const float rs = rsqrtf(r2 + a.R2damp);          // 1/sqrt(r^2 + Rdamp^2)
+    const float Ec = kCoulomb * Q * rs;
+    const float ir2 = 1.0f / r2;
+    const float u2 = R0 * R0 * ir2, u6 = u2 * u2 * u2, vdW = u6 * E0;
+    const float w = skip ? 0.0f : 1.0f;
+    E += w * ((u6 - 2.0f) * vdW + Ec);
+    const float fr = w * (-12.0f * (u6 - 1.0f) * vdW * ir2 - Ec * (rs * rs));
+    fx += dx * fr; fy += dy * fr; fz += dz * fr;
+}
+
 // lanes per atom for the NB partner loop: minimise passes x partners per lane
 __device__ __forceinline__ int nb_lanes(int N, int T) {
     int best = 1; long long bc = 1LL << 60;
@@ -292,7 +314,8 @@ template <> struct EAcc<true> {
 
 // ------------------------------------------------------------------ force evaluation
 template <int T, int GDT, bool EVAL, int FORM>
-__device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* __restrict__ tpp, int N, int rank, EAcc<EVAL>& acc) {
+__device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* __restrict__ tpp, int N, int rank, EAcc<EVAL>& acc,
+                            bool use_list = false, size_t ga0 = 0) {
 #define TP(f) __ldg(&tpp->f)
     // A: bonds and hneigh, one atom per rank (opencl/UFF.cl:141-322)
     for (int i = rank; i < N; i += T) {
@@ -517,7 +540,9 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
     // (opencl/UFF.cl:57-95, 1595-1665).  Excluded pairs are evaluated at r2 = 1 and masked out,
     // so the partner loop has no branch and independent pairs overlap.
     {
-        const int L = a.nb_lanes > 0 ? min(a.nb_lanes, min(T, 32)) : nb_lanes(N, T), G = T / L;
+        // with a neighbour list the partner count, not N, sets the lanes per atom
+        const int Neff = use_list ? min(N, 160) : N;
+        const int L = a.nb_lanes > 0 ? min(a.nb_lanes, min(T, 32)) : nb_lanes(Neff, T), G = T / L;
         const int c = rank & (L - 1);
         const bool small = N <= 64;
         for (int i0 = 0; i0 < N; i0 += G) {
@@ -525,33 +550,27 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
             float fx = 0.f, fy = 0.f, fz = 0.f, E = 0.f;
             if (i < N) {
                 const float4 pi = S.P()[i], qi = S.Q()[i], li = S.Lo()[i];
-                const short4 ng = S.Ng()[i];
-                unsigned long long ex = 1ull << (i & 63);
-                if (ng.x >= 0) ex |= 1ull << (ng.x & 63);
-                if (ng.y >= 0) ex |= 1ull << (ng.y & 63);
-                if (ng.z >= 0) ex |= 1ull << (ng.z & 63);
-                if (ng.w >= 0) ex |= 1ull << (ng.w & 63);
+                const int cnt = use_list ? a.nbl_cnt[ga0 + i] : -1;
+                if (cnt >= 0) {
+                    // partners within rc + skin, ascending; exclusions were removed at the build
+                    const unsigned short* row = a.nbl + (ga0 + i) * (size_t)a.nbl_cap;
 #pragma unroll 4
-                for (int j = c; j < N; j += L) {
-                    const float4 pj = S.P()[j], lj = S.Lo()[j];
-                    const float4 qj = S.Q()[j];
-                    const float dx = (pj.x - pi.x) + (lj.x - li.x), dy = (pj.y - pi.y) + (lj.y - li.y), dz = (pj.z - pi.z) + (lj.z - li.z);
-                    float r2 = dx * dx + dy * dy + dz * dz;
-                    bool out = r2 > a.rc2;
-                    // at the cutoff: decide in FP64, so FP32 rounding never moves a pair across it
-                    if (fabsf(r2 - a.rc2) < 1e-4f * a.rc2) out = beyond_cutoff_fp64(pi, li, pj, lj, a.rc2);
-                    const bool skip = (small ? (bool)((ex >> j) & 1ull)
-                                             : (j == i || j == ng.x || j == ng.y || j == ng.z || j == ng.w)) || out;
-                    r2 = skip ? 1.0f : r2;
-                    const float R0 = qi.x + qj.x, E0 = qi.y * qj.y, Q = qi.z * qj.z;
-                    const float rs = rsqrtf(r2 + a.R2damp);          // 1/sqrt(r^2 + Rdamp^2)
-                    const float Ec = kCoulomb * Q * rs;
-                    const float ir2 = 1.0f / r2;
-                    const float u2 = R0 * R0 * ir2, u6 = u2 * u2 * u2, vdW = u6 * E0;
-                    const float w = skip ? 0.0f : 1.0f;
-                    E += w * ((u6 - 2.0f) * vdW + Ec);
-                    const float fr = w * (-12.0f * (u6 - 1.0f) * vdW * ir2 - Ec * (rs * rs));
-                    fx += dx * fr; fy += dy * fr; fz += dz * fr;
+                    for (int e = c; e < cnt; e += L) {
+                        const int j = row[e];
+                        nb_pair(a, pi, li, qi, S.P()[j], S.Lo()[j], S.Q()[j], false, fx, fy, fz, E);
+                    }
+                } else {
+                    const short4 ng = S.Ng()[i];
+                    unsigned long long ex = 1ull << (i & 63);
+                    if (ng.x >= 0) ex |= 1ull << (ng.x & 63);
+                    if (ng.y >= 0) ex |= 1ull << (ng.y & 63);
+                    if (ng.z >= 0) ex |= 1ull << (ng.z & 63);
+                    if (ng.w >= 0) ex |= 1ull << (ng.w & 63);
+#pragma unroll 4
+                    for (int j = c; j < N; j += L) {
+                        const bool excl = small ? (bool)((ex >> j) & 1ull) : (j == i || j == ng.x || j == ng.y || j == ng.z || j == ng.w);
+                        nb_pair(a, pi, li, qi, S.P()[j], S.Lo()[j], S.Q()[j], excl, fx, fy, fz, E);
+                    }
                 }
             }
             for (int o = 1; o < L; o <<= 1) {
@@ -629,6 +648,62 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
 }
 #undef TP
 
+// ------------------------------------------------------------------ NB neighbour lists
+// Rows of partners within rc + skin in ascending order, one warp per atom: lane c tests partner
+// j0 + c and a ballot places the accepted ones.  Rows longer than nbl_cap mark the atom -2 (all
+// pairs).  Also records each atom's position at the build.
+template <int T>
+__device__ void build_nblist(const KernelArgs& a, const Smem& S, int N, size_t ga0, int rank) {
+    const int lane = rank & 31, warp = rank >> 5;
+    const float rl = sqrtf(a.rc2) + a.nbl_skin, rl2 = rl * rl;
+    for (int i = warp; i < N; i += T / 32) {
+        const float4 pi = S.P()[i], li = S.Lo()[i];
+        const short4 ng = S.Ng()[i];
+        unsigned short* row = a.nbl + (ga0 + i) * (size_t)a.nbl_cap;
+        int base = 0;
+        for (int j0 = 0; j0 < N; j0 += 32) {
+            const int j = j0 + lane;
+            bool inc = false;
+            if (j < N && j != i && j != ng.x && j != ng.y && j != ng.z && j != ng.w) {
+                const float4 pj = S.P()[j], lj = S.Lo()[j];
+                const float dx = (pj.x - pi.x) + (lj.x - li.x), dy = (pj.y - pi.y) + (lj.y - li.y), dz = (pj.z - pi.z) + (lj.z - li.z);
+                inc = dx * dx + dy * dy + dz * dz < rl2;
+            }
+            const unsigned m = __ballot_sync(FULL, inc);
+            const int pos = base + __popc(m & ((1u << lane) - 1u));
+            if (inc && pos < a.nbl_cap) row[pos] = (unsigned short)j;
+            base += __popc(m);
+        }
+        if (lane == 0) {
+            a.nbl_cnt[ga0 + i] = base <= a.nbl_cap ? base : -2;
+            a.nbl_ref[ga0 + i] = make_float4(pi.x + li.x, pi.y + li.y, pi.z + li.z, 0.f);
+        }
+    }
+    team_sync<T>();
+}
+
+// true when some atom moved more than skin / 2 since the last build (same answer on every rank)
+template <int T>
+__device__ bool nblist_stale(const KernelArgs& a, const Smem& S, int N, size_t ga0, int rank) {
+    float m = 0.f;
+    for (int i = rank; i < N; i += T) {
+        const float4 p = S.P()[i], l = S.Lo()[i], r = a.nbl_ref[ga0 + i];
+        const float dx = (p.x - r.x) + l.x, dy = (p.y - r.y) + l.y, dz = (p.z - r.z) + l.z;
+        m = fmaxf(m, dx * dx + dy * dy + dz * dz);
+    }
+    m = warp_max(m);
+    if (T > 32) {
+        double* red = S.red();
+        if ((rank & 31) == 0) red[rank >> 5] = (double)m;
+        __syncthreads();
+        m = 0.f;
+        for (int k = 0; k < T / 32; k++) m = fmaxf(m, (float)red[k]);
+        __syncthreads();
+    }
+    const float h = 0.5f * a.nbl_skin;
+    return m > h * h;
+}
+
 // ------------------------------------------------------------------ one system
 template <int T, int GDT, bool EVAL, int FORM>
 __device__ void run_system(const KernelArgs& a, const Smem& S, int w, int rank) {
@@ -674,13 +749,22 @@ __device__ void run_system(const KernelArgs& a, const Smem& S, int w, int rank) 
         return;
     }
 
+    // neighbour list: rebuilt on the first step after positions were set (fresh FIRE state) and
+    // whenever an atom has moved more than skin / 2; both depend only on this system's trajectory
+    const bool use_list = a.nbl != nullptr && N >= a.nbl_min && a.rc2 < 1e37f;
+    const size_t ga0 = (size_t)st.atom_off;
+    bool need_build = use_list && fresh;
     double dt = fresh ? a.fire.dt0 : st.dt, alpha = fresh ? a.fire.alpha0 : st.alpha;
     int npos = fresh ? 0 : st.npos, status = st.status;
     float fmax = st.fmax;
     const float flim = (float)a.fire.flimit, flim2 = flim * flim;
     int ran = 0;
     for (int it = 0; it < nsteps; it++) {
-        eval_forces<T, GDT, EVAL, FORM>(a, S, tpp, N, rank, acc);
+        if (use_list) {
+            if (need_build || nblist_stale<T>(a, S, N, ga0, rank)) build_nblist<T>(a, S, N, ga0, rank);
+            need_build = false;
+        }
+        eval_forces<T, GDT, EVAL, FORM>(a, S, tpp, N, rank, acc, use_list, ga0);
         ran = 1;
         const double dt_old = dt;
         const float dtf = (float)dt_old;

@@ -106,6 +106,15 @@ struct KernelArgs {
     // (team k of the launch at k * team bytes); null for shared-memory launches
     char* gscratch;
     size_t gscratch_bytes;
+    // NB neighbour lists (systems of at least nbl_min atoms under a cutoff, FIRE steps only): row of
+    // state atom g at nbl + g * nbl_cap holds the partners within rc + skin in ascending order,
+    // nbl_cnt[g] their number (-1: rebuild, -2: overflow, use all pairs), nbl_ref[g] the
+    // position at the last build
+    unsigned short* nbl;
+    int* nbl_cnt;
+    float4* nbl_ref;
+    int nbl_cap, nbl_min;
+    float nbl_skin;
 };
 
 // ---- host topology (topology.cpp)

@@ -225,6 +225,15 @@ class RelaxMulti:
         """Lanes per atom in the NB partner loop (0: chosen from system size and team)."""
         self._chk(self.L.smr_set_tuning(self.h, 1, int(lanes)), "smr_set_tuning")
 
+    def set_nblist(self, min_atoms=None, skin=None, cap=None):
+        """NB neighbour lists for systems of >= min_atoms atoms under a cutoff (0: off); skin in A."""
+        if min_atoms is not None:
+            self._chk(self.L.smr_set_tuning(self.h, 2, int(min_atoms)), "smr_set_tuning")
+        if skin is not None:
+            self._chk(self.L.smr_set_tuning(self.h, 3, int(round(skin * 1000))), "smr_set_tuning")
+        if cap is not None:
+            self._chk(self.L.smr_set_tuning(self.h, 4, int(cap)), "smr_set_tuning")
+
     def get_nb_lanes(self):
         v = C.c_int()
         self._chk(self.L.smr_get_tuning(self.h, 1, C.byref(v)), "smr_get_tuning")

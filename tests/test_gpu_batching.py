@@ -152,3 +152,38 @@ def test_graph_replay_bitwise(setup):
                 assert np.array_equal(o["pos"][i], outs[0]["pos"][i]) and o["steps"][i] == 90
     finally:
         R.finish()
+
+
+@pytest.mark.parametrize("cap", [256, 32])
+def test_nblist_forces_and_bitwise(setup, oracle, cap):
+    """NB neighbour lists (systems >= 128 atoms under the 10 A cutoff): the forces of the first FIRE
+    step match the oracle (cap 32 forces row overflow, i.e. the all-pairs fallback for crowded
+    atoms), and batched, chunked and plain runs stay bitwise identical across list rebuilds."""
+    from oracle import oracle as O
+    slab, dims, p0, step, mols = setup
+    big = [mols[4], mols[5], mols[6]]                       # 150-330 atoms
+    R = make_handle(8, 4000, slab, dims, p0, step, rcut=10.0)
+    try:
+        R.set_nblist(min_atoms=128, skin=1.0, cap=cap)
+        g = R.get_grid()
+        tids = [R.add_molecule(Z, P, q) for Z, P, q in big]
+        s = R.add_systems(tids, [m[1] for m in big])
+        R.run_fire(1, step_budget=1, fconv=1e-9)
+        out = R.download(s)
+        for k, (Z, P, q) in enumerate(big):
+            Fo, _, _ = O.System.from_molecule(Z, P, q).eval(P.astype(np.float32).astype(np.float64),
+                                                            O.Grid(g["coef"], g["p0"], g["step"]), rcut=10.0)
+            assert force_err(out["forces"][k], Fo) < F_RTOL, (len(Z), cap)
+        R.remove_systems(s)
+        runs = []
+        for mode, chunks in ((0, [150]), (0, [40, 40, 70]), (1, [150])):
+            s = R.add_systems(tids, [m[1] for m in big])
+            for c in chunks:
+                R.run_fire(c, step_budget=150, fconv=1e-6, mode=mode)
+            runs.append(R.download(s))
+            R.remove_systems(s)
+        for o in runs[1:]:
+            for k in range(len(big)):
+                assert np.array_equal(o["pos"][k], runs[0]["pos"][k]) and o["steps"][k] == runs[0]["steps"][k] == 150
+    finally:
+        R.finish()
