@@ -121,6 +121,15 @@ int smr_set_nb_params(smr_handle* h, const smr_nb_params* p);
 int smr_set_grid(smr_handle* h, const void* coef, int dtype, const float scale[4],
                  int nx, int ny, int nz, const double p0[3], const double step[3]);
 int smr_get_grid(smr_handle* h, void* coef_out, int* dtype, float scale[4], int dims[3], double p0[3], double step[3]);
+/* 16-bit grids with one scale per z plane and channel (value = stored * plane_scale[4*iz + c]);
+ * smr_convert_grid to F16 / BF16 produces such grids (power-of-two scales fitted per plane: the
+ * channels grow by orders of magnitude towards the surface, one scale per channel would waste
+ * most of fp16's precision on the far planes).  smr_get_grid's scale[] then holds each channel's
+ * largest plane scale; smr_get_grid_planes returns the nz x 4 table (the channel scales on every
+ * plane for grids without one).  No counterpart in the reference (its grids are float32). */
+int smr_set_grid_planes(smr_handle* h, const void* coef, int dtype, const float* plane_scale, int nx, int ny, int nz,
+                        const double p0[3], const double step[3]);
+int smr_get_grid_planes(smr_handle* h, float* plane_scale);
 /* Build on the device from ions (x, y, z, q) and their Morse (R, sqrt(E)); the slab is periodic
  * in an orthogonal Lx x Ly cell and lies entirely below p0[2]. */
 int smr_build_grid(smr_handle* h, int nions, const double* ions, const double* ion_re, double Lx, double Ly,

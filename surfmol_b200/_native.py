@@ -60,6 +60,8 @@ SIGNATURES = {
     "smr_set_nb_params": (C.c_int, [VP, C.POINTER(SmrNbParams)]),
     "smr_set_grid": (C.c_int, [VP, VP, C.c_int, FP, C.c_int, C.c_int, C.c_int, DP, DP]),
     "smr_get_grid": (C.c_int, [VP, VP, IP, FP, IP, DP, DP]),
+    "smr_set_grid_planes": (C.c_int, [VP, VP, C.c_int, FP, C.c_int, C.c_int, C.c_int, DP, DP]),
+    "smr_get_grid_planes": (C.c_int, [VP, FP]),
     "smr_build_grid": (C.c_int, [VP, C.c_int, DP, DP, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, DP, DP,
                                  C.POINTER(SmrGridBuildParams)]),
     "smr_convert_grid": (C.c_int, [VP, C.c_int]),

@@ -119,6 +119,8 @@ struct smr_handle {
     int gdim[3] = {0, 0, 0};
     double gp0[3] = {0, 0, 0}, gstep[3] = {1, 1, 1};
     float gscale[4] = {1, 1, 1, 1};
+    std::vector<float> gzscale;         // 16-bit grids: nz x 4 per-plane channel scales (empty: gscale)
+    DArr<float4> dzscale;
     bool has_grid = false;
 
     smr_nb_params nb{1.0f, 1.5f, 0.0f, 0};
@@ -406,6 +408,7 @@ KernelArgs base_args(smr_handle* h) {
     a.grid.nx = h->gdim[0]; a.grid.ny = h->gdim[1]; a.grid.nz = h->gdim[2];
     for (int k = 0; k < 3; k++) { a.grid.p0[k] = (float)h->gp0[k]; a.grid.inv_step[k] = (float)(1.0 / h->gstep[k]); }
     for (int k = 0; k < 4; k++) a.grid.scale[k] = h->has_grid ? h->gscale[k] : 1.f;
+    a.grid.zscale = (h->has_grid && !h->gzscale.empty()) ? h->dzscale.d : nullptr;
     a.R2damp = h->nb.rdamp * h->nb.rdamp;
     a.alpha_morse = h->nb.alpha_morse;
     a.rc2 = h->nb.rcut > 0 ? h->nb.rcut * h->nb.rcut : 3.0e38f;
@@ -630,6 +633,41 @@ int smr_set_team_size(smr_handle* h, int max_atoms, int threads) {
 
 static size_t voxel_bytes(int dtype) { return dtype == SMR_GRID_F32 ? 16 : 8; }
 
+// install per-plane scales (nz x 4 host floats; null: none) on the device
+static int set_plane_scales(smr_handle* h, const float* ps, int nz) {
+    if (!ps) { h->gzscale.clear(); return SMR_OK; }
+    h->gzscale.assign(ps, ps + 4 * (size_t)nz);
+    cudaError_t e = h->dzscale.reserve((size_t)nz, 0, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h->dzscale.d, h->gzscale.data(), (size_t)nz * 16, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return fail(h, SMR_ERR_CUDA, "plane scales: %s", cudaGetErrorString(e));
+    for (int c = 0; c < 4; c++) {                          // per-channel summary: the largest plane scale
+        float m = 0.f;
+        for (int z = 0; z < nz; z++) m = std::max(m, h->gzscale[4 * (size_t)z + c]);
+        h->gscale[c] = m;
+    }
+    return SMR_OK;
+}
+
+int smr_set_grid_planes(smr_handle* h, const void* coef, int dtype, const float* plane_scale, int nx, int ny, int nz,
+                        const double p0[3], const double step[3]) {
+    if (!h || !plane_scale) return SMR_ERR_ARG;
+    if (dtype != SMR_GRID_F16 && dtype != SMR_GRID_BF16) return fail(h, SMR_ERR_ARG, "per-plane scales are for 16-bit grids");
+    int r = smr_set_grid(h, coef, dtype, nullptr, nx, ny, nz, p0, step);
+    if (r) return r;
+    return set_plane_scales(h, plane_scale, nz);
+}
+
+int smr_get_grid_planes(smr_handle* h, float* plane_scale) {
+    if (!h || !plane_scale) return SMR_ERR_ARG;
+    if (!h->has_grid) return fail(h, SMR_ERR_STATE, "no grid set");
+    const int nz = h->gdim[2];
+    for (int z = 0; z < nz; z++)
+        for (int c = 0; c < 4; c++)
+            plane_scale[4 * (size_t)z + c] = h->gzscale.empty() ? h->gscale[c] : h->gzscale[4 * (size_t)z + c];
+    return SMR_OK;
+}
+
 int smr_set_grid(smr_handle* h, const void* coef, int dtype, const float scale[4], int nx, int ny, int nz,
                  const double p0[3], const double step[3]) {
     if (!h || !coef || !p0 || !step) return SMR_ERR_ARG;
@@ -647,6 +685,7 @@ int smr_set_grid(smr_handle* h, const void* coef, int dtype, const float scale[4
     h->gdim[0] = nx; h->gdim[1] = ny; h->gdim[2] = nz;
     for (int k = 0; k < 3; k++) { h->gp0[k] = p0[k]; h->gstep[k] = step[k]; }
     for (int k = 0; k < 4; k++) h->gscale[k] = scale ? scale[k] : 1.f;
+    h->gzscale.clear();
     return SMR_OK;
 }
 
@@ -675,21 +714,29 @@ int smr_convert_grid(smr_handle* h, int dtype) {
     if (h->grid_dtype == SMR_GRID_F32) f32 = (float4*)h->grid;
     else {
         CU(h, cudaMalloc(&f32, nv * 16));
-        if (decode_grid_16(h->grid, f32, nv, h->grid_dtype, h->gscale, h->stream)) { cudaFree(f32); return fail(h, SMR_ERR_CUDA, "grid decode failed"); }
+        // the decode table: the per-plane scales, or the channel scales on every plane
+        const int nz = h->gdim[2];
+        std::vector<float> tab(4 * (size_t)nz);
+        smr_get_grid_planes(h, tab.data());
+        int r = set_plane_scales(h, tab.data(), nz);
+        if (r) { cudaFree(f32); return r; }
+        if (decode_grid_16(h->grid, f32, nv, nz, h->grid_dtype, h->dzscale.d, h->stream)) { cudaFree(f32); return fail(h, SMR_ERR_CUDA, "grid decode failed"); }
     }
     void* out = nullptr;
-    float sc[4] = {1, 1, 1, 1};
+    std::vector<float> ps;
     if (dtype == SMR_GRID_F32) out = f32;
     else {
         cudaError_t e = cudaMalloc(&out, nv * 8);
         if (e != cudaSuccess) { if ((void*)f32 != h->grid) cudaFree(f32); return fail(h, SMR_ERR_CUDA, "grid alloc: %s", cudaGetErrorString(e)); }
-        if (encode_grid_16(f32, out, nv, dtype, sc, h->stream)) { cudaFree(out); return fail(h, SMR_ERR_CUDA, "grid encode failed"); }
+        ps.resize(4 * (size_t)h->gdim[2]);
+        if (encode_grid_16(f32, out, nv, h->gdim[2], dtype, ps.data(), h->stream)) { cudaFree(out); return fail(h, SMR_ERR_CUDA, "grid encode failed"); }
         if ((void*)f32 != h->grid) cudaFree(f32);
     }
     CU(h, cudaStreamSynchronize(h->stream));
     if (out != h->grid) cudaFree(h->grid);
     h->grid = out; h->grid_dtype = dtype;
-    for (int k = 0; k < 4; k++) h->gscale[k] = sc[k];
+    if (dtype == SMR_GRID_F32) { for (int k = 0; k < 4; k++) h->gscale[k] = 1.f; h->gzscale.clear(); }
+    else { int r = set_plane_scales(h, ps.data(), h->gdim[2]); if (r) return r; }
     return SMR_OK;
 }
 
@@ -1025,6 +1072,7 @@ static void sig_args(std::vector<long long>& v, const KernelArgs& a) {
     P(a.grid.data); v.push_back(a.grid.dtype); v.push_back(a.grid.nx); v.push_back(a.grid.ny); v.push_back(a.grid.nz);
     for (int k = 0; k < 3; k++) { F(a.grid.p0[k]); F(a.grid.inv_step[k]); }
     for (int k = 0; k < 4; k++) F(a.grid.scale[k]);
+    P(a.grid.zscale);
     v.push_back(a.has_grid); F(a.R2damp); F(a.alpha_morse); F(a.rc2);
     D(a.fire.dt0); D(a.fire.dt_max); D(a.fire.alpha0); D(a.fire.f_inc); D(a.fire.f_dec); D(a.fire.f_alpha);
     D(a.fire.fconv); D(a.fire.flimit); v.push_back(a.fire.n_min);

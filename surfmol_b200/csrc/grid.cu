@@ -287,22 +287,29 @@ int fit_channel(double* d, int nx, int ny, int nz, cudaStream_t s, DevBuf& buf, 
 }
 
 // ---------------------------------------------------------------- 16-bit encoding
-__global__ void absmax_kernel(size_t N, const float4* __restrict__ src, unsigned int* __restrict__ mx) {
-    float m[4] = {0.f, 0.f, 0.f, 0.f};
+// per (z plane, channel) max |c|: each block reduces a contiguous voxel range into shared memory
+// (voxel i lies on plane i % nz), then merges into the global table
+__global__ void plane_absmax_kernel(size_t N, int nz, const float4* __restrict__ src, unsigned int* __restrict__ mx) {
+    extern __shared__ unsigned int sm[];
+    for (int k = threadIdx.x; k < 4 * nz; k += blockDim.x) sm[k] = 0u;
+    __syncthreads();
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x) {
         const float4 v = src[i];
-        m[0] = fmaxf(m[0], fabsf(v.x)); m[1] = fmaxf(m[1], fabsf(v.y)); m[2] = fmaxf(m[2], fabsf(v.z)); m[3] = fmaxf(m[3], fabsf(v.w));
+        const int z = (int)(i % (size_t)nz);
+        atomicMax(sm + 4 * z + 0, __float_as_uint(fabsf(v.x)));    // non-negative floats order as uints
+        atomicMax(sm + 4 * z + 1, __float_as_uint(fabsf(v.y)));
+        atomicMax(sm + 4 * z + 2, __float_as_uint(fabsf(v.z)));
+        atomicMax(sm + 4 * z + 3, __float_as_uint(fabsf(v.w)));
     }
-    for (int c = 0; c < 4; c++) {
-        float v = m[c];
-        for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
-        if ((threadIdx.x & 31) == 0) atomicMax(mx + c, __float_as_uint(v));   // non-negative floats order as uints
-    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < 4 * nz; k += blockDim.x)
+        if (sm[k]) atomicMax(mx + k, sm[k]);
 }
-__global__ void encode_kernel(size_t N, const float4* __restrict__ src, uint2* __restrict__ dst, int dtype, float4 inv) {
+__global__ void encode_kernel(size_t N, int nz, const float4* __restrict__ src, uint2* __restrict__ dst, int dtype,
+                              const float4* __restrict__ inv_tab) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
-    const float4 v = src[i];
+    const float4 v = src[i], inv = inv_tab[i % (size_t)nz];
     uint2 o;
     if (dtype == GRID_F16) {
         __half2 a = __floats2half2_rn(v.x * inv.x, v.y * inv.y), b = __floats2half2_rn(v.z * inv.z, v.w * inv.w);
@@ -313,10 +320,12 @@ __global__ void encode_kernel(size_t N, const float4* __restrict__ src, uint2* _
     }
     dst[i] = o;
 }
-__global__ void decode_kernel(size_t N, const uint2* __restrict__ src, float4* __restrict__ dst, int dtype, float4 sc) {
+__global__ void decode_kernel(size_t N, int nz, const uint2* __restrict__ src, float4* __restrict__ dst, int dtype,
+                              const float4* __restrict__ sc_tab) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     const uint2 u = src[i];
+    const float4 sc = sc_tab[i % (size_t)nz];
     float2 a, b;
     if (dtype == GRID_F16) { a = __half22float2(*reinterpret_cast<const __half2*>(&u.x)); b = __half22float2(*reinterpret_cast<const __half2*>(&u.y)); }
     else { a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.x)); b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.y)); }
@@ -325,32 +334,40 @@ __global__ void decode_kernel(size_t N, const uint2* __restrict__ src, float4* _
 
 }  // namespace
 
-int encode_grid_16(const float4* src, void* dst, size_t nvox, int dtype, float scale_out[4], cudaStream_t s) {
-    unsigned int* dmx;
-    if (cudaMalloc(&dmx, 16) != cudaSuccess) return -1;
-    cudaMemsetAsync(dmx, 0, 16, s);
-    absmax_kernel<<<1024, 256, 0, s>>>(nvox, src, dmx);
-    unsigned int hm[4];
-    cudaMemcpyAsync(hm, dmx, 16, cudaMemcpyDeviceToHost, s);
-    if (cudaStreamSynchronize(s) != cudaSuccess) { cudaFree(dmx); return -1; }
-    cudaFree(dmx);
-    float inv[4];
-    for (int c = 0; c < 4; c++) {
+// Per plane and channel a power-of-two scale: fp16 maps the plane's max |c| to [16384, 32768)
+// (headroom below 65504, the full normal range below it), so the coefficients of every plane
+// keep fp16's 11-bit relative precision however fast the channel grows towards the surface;
+// bf16 has the fp32 exponent range and only needs max |c| ~ 1.
+int encode_grid_16(const float4* src, void* dst, size_t nvox, int nz, int dtype, float* plane_scale_out, cudaStream_t s) {
+    if (nz <= 0 || nz > 3072) return -1;             // the per-plane table lives in 48 KB of shared memory
+    unsigned int* dmx = nullptr;
+    float4* dinv = nullptr;
+    if (cudaMalloc(&dmx, (size_t)nz * 16) != cudaSuccess) return -1;
+    if (cudaMalloc(&dinv, (size_t)nz * 16) != cudaSuccess) { cudaFree(dmx); return -1; }
+    cudaMemsetAsync(dmx, 0, (size_t)nz * 16, s);
+    plane_absmax_kernel<<<592, 256, (size_t)nz * 16, s>>>(nvox, nz, src, dmx);
+    std::vector<unsigned int> hm(4 * (size_t)nz);
+    cudaMemcpyAsync(hm.data(), dmx, (size_t)nz * 16, cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) { cudaFree(dmx); cudaFree(dinv); return -1; }
+    std::vector<float> inv(4 * (size_t)nz);
+    for (size_t k = 0; k < hm.size(); k++) {
         float m;
-        std::memcpy(&m, &hm[c], 4);
-        // power-of-two scale: fp16 maps max|c| to [16384, 32768) (headroom below 65504, full
-        // normal range below); bf16 has the fp32 exponent range and only needs max|c| ~ 1.
+        std::memcpy(&m, &hm[k], 4);
         float sc = 1.f;
         if (m > 0.f) sc = std::ldexp(1.0f, (int)std::ceil(std::log2((double)m)) - (dtype == GRID_F16 ? 15 : 0));
-        scale_out[c] = sc;
-        inv[c] = 1.f / sc;
+        plane_scale_out[k] = sc;
+        inv[k] = 1.f / sc;
     }
-    encode_kernel<<<(unsigned)((nvox + 255) / 256), 256, 0, s>>>(nvox, src, (uint2*)dst, dtype, make_float4(inv[0], inv[1], inv[2], inv[3]));
-    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+    cudaMemcpyAsync(dinv, inv.data(), inv.size() * 4, cudaMemcpyHostToDevice, s);
+    encode_kernel<<<(unsigned)((nvox + 255) / 256), 256, 0, s>>>(nvox, nz, src, (uint2*)dst, dtype, dinv);
+    const bool ok = cudaGetLastError() == cudaSuccess && cudaStreamSynchronize(s) == cudaSuccess;
+    cudaFree(dmx);
+    cudaFree(dinv);
+    return ok ? 0 : -1;
 }
 
-int decode_grid_16(const void* src, float4* dst, size_t nvox, int dtype, const float scale[4], cudaStream_t s) {
-    decode_kernel<<<(unsigned)((nvox + 255) / 256), 256, 0, s>>>(nvox, (const uint2*)src, dst, dtype, make_float4(scale[0], scale[1], scale[2], scale[3]));
+int decode_grid_16(const void* src, float4* dst, size_t nvox, int nz, int dtype, const float4* d_plane_scale, cudaStream_t s) {
+    decode_kernel<<<(unsigned)((nvox + 255) / 256), 256, 0, s>>>(nvox, nz, (const uint2*)src, dst, dtype, d_plane_scale);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

@@ -610,7 +610,10 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
                     // atom prefactors (opencl/UFF.cl:1681-1687) times the stored channel scales
                     const float4 q = S.Q()[i];
                     const float ej = expf(a.alpha_morse * q.x);
-                    const float PLx = ej * ej * q.y * g.scale[0], PLy = ej * q.y * g.scale[1], PLz = q.z * g.scale[2];
+                    float PLx = ej * ej * q.y, PLy = ej * q.y, PLz = q.z;
+                    // stored-value scales: per z plane (this lane reads one plane) or per channel
+                    const float4 zs = g.zscale ? __ldg(g.zscale + (iz - 1 + kz)) : make_float4(g.scale[0], g.scale[1], g.scale[2], 1.f);
+                    PLx *= zs.x; PLy *= zs.y; PLz *= zs.z;
                     const int x0 = imod(ix - 1, g.nx), y0 = imod(iy - 1, g.ny);
                     const size_t zoff = (size_t)(iz - 1 + kz);
                     float sE = 0.f, sX = 0.f, sY = 0.f;

@@ -73,7 +73,8 @@ struct GridView {
     int nx, ny, nz;
     float p0[3];
     float inv_step[3];
-    float scale[4];
+    float scale[4];               // per-channel scale of the stored values (when zscale is null)
+    const float4* zscale;         // 16-bit grids: per z plane and channel scale (null: scale[])
 };
 
 struct FireDev {
@@ -174,7 +175,9 @@ struct GridBuildArgs {
     double alpha; int npbc; double ewald_tol; double morse_rcut;
 };
 int build_grid_device(const GridBuildArgs& a, float4* out_f32, cudaStream_t s, char* err, int errlen);
-int encode_grid_16(const float4* src, void* dst, size_t nvox, int dtype, float scale_out[4], cudaStream_t s);
-int decode_grid_16(const void* src, float4* dst, size_t nvox, int dtype, const float scale[4], cudaStream_t s);
+// 16-bit storage with one power-of-two scale per z plane and channel: plane_scale_out gets nz x 4
+// floats (host); decode takes them as a device table
+int encode_grid_16(const float4* src, void* dst, size_t nvox, int nz, int dtype, float* plane_scale_out, cudaStream_t s);
+int decode_grid_16(const void* src, float4* dst, size_t nvox, int nz, int dtype, const float4* d_plane_scale, cudaStream_t s);
 
 }  // namespace smr

@@ -166,10 +166,16 @@ class RelaxMulti:
         p = N.SmrNbParams(rdamp, alpha_morse, rcut, 0)
         self._chk(self.L.smr_set_nb_params(self.h, C.byref(p)), "smr_set_nb_params")
 
-    def set_grid(self, coef, p0, step, dtype=GRID_F32, scale=(1, 1, 1, 1)):
-        """coef: (nx, ny, nz, 4) float32 (F32) or uint16 (F16/BF16 bit patterns), z-fastest."""
+    def set_grid(self, coef, p0, step, dtype=GRID_F32, scale=(1, 1, 1, 1), plane_scale=None):
+        """coef: (nx, ny, nz, 4) float32 (F32) or uint16 (F16/BF16 bit patterns), z-fastest;
+        16-bit grids take per-channel `scale` or an (nz, 4) per-plane `plane_scale`."""
         coef = np.ascontiguousarray(coef)
         nx, ny, nz, _ = coef.shape
+        if plane_scale is not None:
+            ps = _f(plane_scale)
+            self._chk(self.L.smr_set_grid_planes(self.h, coef.ctypes.data_as(N.VP), dtype, _p(ps, N.FP), nx, ny, nz,
+                                                 _p(_d(p0), N.DP), _p(_d(step), N.DP)), "smr_set_grid_planes")
+            return
         sc = _f(scale)
         self._chk(self.L.smr_set_grid(self.h, coef.ctypes.data_as(N.VP), dtype, _p(sc, N.FP), nx, ny, nz,
                                       _p(_d(p0), N.DP), _p(_d(step), N.DP)), "smr_set_grid")
@@ -184,7 +190,10 @@ class RelaxMulti:
         shape = (dims[0], dims[1], dims[2], 4)
         buf = np.zeros(shape, np.float32 if dt.value == GRID_F32 else np.uint16)
         self._chk(self.L.smr_get_grid(self.h, buf.ctypes.data_as(N.VP), None, None, None, None, None), "smr_get_grid")
-        return dict(coef=buf, dtype=dt.value, scale=np.array(list(sc)), p0=np.array(list(p0)), step=np.array(list(st)))
+        ps = np.zeros((dims[2], 4), np.float32)
+        self._chk(self.L.smr_get_grid_planes(self.h, _p(ps, N.FP)), "smr_get_grid_planes")
+        return dict(coef=buf, dtype=dt.value, scale=np.array(list(sc)), plane_scale=ps, p0=np.array(list(p0)),
+                    step=np.array(list(st)))
 
     def build_grid(self, ions, ion_re, Lx, Ly, nx, ny, nz, p0, step, alpha_morse=1.5, npbc=1, ewald_tol=1e-12,
                    dtype=GRID_F32, morse_rcut=0.0):

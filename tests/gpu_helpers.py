@@ -29,6 +29,9 @@ def decode(g):
         v = c.view(np.float16).astype(np.float64)
     else:
         v = (c.astype(np.uint32) << 16).view(np.float32).astype(np.float64)
+    ps = g.get("plane_scale")
+    if ps is not None:
+        return v * ps.astype(np.float64)[None, None, :, :]
     return v * g["scale"][None, None, None, :]
 
 
