@@ -203,6 +203,10 @@ int  smr_topo_prepare(smr_topo* t, int team);
  * topologies are dropped by an automatic compaction once they outnumber the live ones (long-running
  * servers admit and retire molecules without growing the arenas).  No counterpart in the reference. */
 int  smr_remove_topology(smr_handle* h, int topo_id);
+/* Batch forms (one device upload / one compaction check per batch): attach n host topologies
+ * (ids out), release n topologies.  No counterpart in the reference. */
+int  smr_add_topos(smr_handle* h, int n, const smr_topo* const* topos, int* topo_ids);
+int  smr_remove_topologies(smr_handle* h, int n, const int* topo_ids);
 
 /* Systems: one slot per system; positions are float32 x,y,z concatenated over the systems. */
 int smr_add_systems(smr_handle* h, int nsys, const int* topo_ids, const float* pos, int* slot_ids);

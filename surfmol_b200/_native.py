@@ -81,6 +81,8 @@ SIGNATURES = {
     "smr_add_topo": (C.c_int, [VP, VP, IP]),
     "smr_topo_prepare": (C.c_int, [VP, C.c_int]),
     "smr_remove_topology": (C.c_int, [VP, C.c_int]),
+    "smr_add_topos": (C.c_int, [VP, C.c_int, C.POINTER(VP), IP]),
+    "smr_remove_topologies": (C.c_int, [VP, C.c_int, IP]),
     "smr_add_systems": (C.c_int, [VP, C.c_int, IP, FP, IP]),
     "smr_remove_systems": (C.c_int, [VP, C.c_int, IP]),
     "smr_set_positions": (C.c_int, [VP, C.c_int, IP, FP]),

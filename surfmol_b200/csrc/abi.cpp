@@ -1360,16 +1360,48 @@ int smr_topo_prepare(smr_topo* t, int team) {
     return SMR_OK;
 }
 
-int smr_remove_topology(smr_handle* h, int id) {
-    if (!h || id < 0 || id >= (int)h->topos.size() || !h->topo_alive[id]) return fail(h, SMR_ERR_ARG, "topology %d not live", id);
+int smr_add_topos(smr_handle* h, int n, const smr_topo* const* topos, int* topo_ids) {
+    if (!h || n < 0 || (n && (!topos || !topo_ids))) return SMR_ERR_ARG;
+    for (int i = 0; i < n; i++) if (!topos[i]) return fail(h, SMR_ERR_ARG, "topology %d is null", i);
+    for (int i = 0; i < n; i++) {
+        const smr_topo* t = topos[i];
+        h->topos.push_back(t->T);
+        h->topo_alive.push_back(1);
+        const int team = team_for(h, t->T.n);
+        if (t->prepared && t->prep.team == team) commit_topology(h, h->topos.back(), t->prep);
+        else append_topology(h, h->topos.back());
+        topo_ids[i] = (int)h->topos.size() - 1;
+    }
+    return upload_all(h);
+}
+
+static int remove_one_topology(smr_handle* h, int id) {
+    if (id < 0 || id >= (int)h->topos.size() || !h->topo_alive[id]) return fail(h, SMR_ERR_ARG, "topology %d not live", id);
     for (int s = 0; s < h->max_systems; s++)
         if (h->hs[s].active && h->hs[s].topo == id) return fail(h, SMR_ERR_STATE, "topology %d is used by slot %d", id, s);
     h->topo_alive[id] = 0;
     h->dead_atoms += h->topos[id].n;
     h->topos[id] = HostTopo{};
+    return SMR_OK;
+}
+
+static int maybe_compact(smr_handle* h) {
     const size_t live = h->hreq.size() - h->dead_atoms;
     if (h->dead_atoms > 4096 && h->dead_atoms > live) return compact_topologies(h);
     return SMR_OK;
+}
+
+int smr_remove_topologies(smr_handle* h, int n, const int* ids) {
+    if (!h || n < 0 || (n && !ids)) return SMR_ERR_ARG;
+    for (int i = 0; i < n; i++) { int r = remove_one_topology(h, ids[i]); if (r) return r; }
+    return maybe_compact(h);
+}
+
+int smr_remove_topology(smr_handle* h, int id) {
+    if (!h) return SMR_ERR_ARG;
+    int r = remove_one_topology(h, id);
+    if (r) return r;
+    return maybe_compact(h);
 }
 
 int smr_topo_build(int natoms, const int* Z, const double* pos, const double* charges, double bond_cut, smr_topo** out,

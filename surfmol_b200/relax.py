@@ -289,6 +289,18 @@ class RelaxMulti:
         self.topo_n.append(topo.n)
         return tid.value
 
+    def add_topos(self, topos) -> np.ndarray:
+        """Attach many host topologies with one device upload; returns their ids."""
+        arr = (N.VP * len(topos))(*[t.h.value for t in topos])
+        ids = np.zeros(len(topos), np.int32)
+        self._chk(self.L.smr_add_topos(self.h, len(topos), arr, _p(ids, N.IP)), "smr_add_topos")
+        self.topo_n.extend(t.n for t in topos)
+        return ids
+
+    def remove_topologies(self, tids):
+        t = _i(tids)
+        self._chk(self.L.smr_remove_topologies(self.h, len(t), _p(t, N.IP)), "smr_remove_topologies")
+
     def remove_topology(self, tid):
         self._chk(self.L.smr_remove_topology(self.h, int(tid)), "smr_remove_topology")
 

@@ -66,13 +66,15 @@ class ServeStats:
     launches: int = 0
     max_resident: int = 0
     latencies: list = field(default_factory=list)
+    host_s: dict = field(default_factory=lambda: {"admit": 0.0, "run_call": 0.0, "status": 0.0, "retire": 0.0})
 
     def summary(self):
         lat = np.array(self.latencies) if self.latencies else np.zeros(1)
         return {"requests": self.n, "wall_s": self.wall_s, "throughput_req_s": self.n / max(self.wall_s, 1e-9),
                 "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
                 "gpu_busy": self.gpu_ms * 1e-3 / max(self.wall_s, 1e-9), "chunks": self.chunks,
-                "gpu_launches": self.launches, "max_resident": self.max_resident}
+                "gpu_launches": self.launches, "max_resident": self.max_resident,
+                "wall_split_s": {k: round(v, 3) for k, v in self.host_s.items()}}
 
 
 class Server:
@@ -159,6 +161,7 @@ class Server:
                     if not resident:
                         break
                 # admit in arrival order while slots, atoms and the HBM budget allow
+                t_a = time.perf_counter()
                 adm_t, adm_p, adm_r = [], [], []
                 while waiting:
                     r, topo = waiting[0]
@@ -168,10 +171,9 @@ class Server:
                             or used_bytes + cost > self.budget):
                         break
                     waiting.pop(0)
-                    tid = R.add_topo(topo)
-                    adm_t.append(tid)
+                    adm_t.append(topo)
                     adm_p.append(r.pos)
-                    adm_r.append((r, tid, na))
+                    adm_r.append([r, -1, na])
                     used_bytes += cost
                     used_atoms += na
                 if not resident and not adm_r and waiting:
@@ -181,16 +183,23 @@ class Server:
                     done += 1
                     continue
                 if adm_r:
-                    slots = R.add_systems(adm_t, adm_p)
+                    tids = R.add_topos(adm_t)                  # one upload for the whole batch
+                    for x, tid in zip(adm_r, tids):
+                        x[1] = int(tid)
+                    slots = R.add_systems(tids, adm_p)
                     now = time.perf_counter() - t0
                     for s, (r, tid, na) in zip(slots, adm_r):
                         r.t_admit = now
                         resident[int(s)] = (r, tid, na)
+                st.host_s["admit"] += time.perf_counter() - t_a
                 if not resident:
                     continue
                 st.max_resident = max(st.max_resident, len(resident))
                 # one chunk of FIRE steps over every resident system
+                t_r = time.perf_counter()
                 R.run_fire(self.chunk, step_budget=self.max_steps, **self.fire)
+                t_s = time.perf_counter()
+                st.host_s["run_call"] += t_s - t_r
                 ms, nl = R.last_timing()
                 st.gpu_ms += ms
                 st.launches += nl
@@ -199,6 +208,8 @@ class Server:
                 slots = np.array(sorted(resident), np.int32)
                 stat = R.download(slots, pos=False, forces=False)
                 fin = slots[stat["status"] != ST_RUNNING]
+                t_x = time.perf_counter()
+                st.host_s["status"] += t_x - t_s
                 if len(fin):
                     out = R.download(fin, pos=True, forces=False)
                     p64 = R.download_pos64(fin) if self.keep_pos64 else None
@@ -218,8 +229,8 @@ class Server:
                         tids.append(tid)
                         done += 1
                     R.remove_systems(fin)
-                    for tid in tids:                 # each request has its own topology
-                        R.remove_topology(tid)
+                    R.remove_topologies(tids)        # each request has its own topology
+                    st.host_s["retire"] += time.perf_counter() - t_x
         finally:
             stop.set()
             th.join(timeout=5)
