@@ -440,7 +440,10 @@ std::vector<Seg> group_by(smr_handle* h, std::vector<int>& ids, int form, int re
             const int t = req_team ? req_team : td.team;
             if (team_smem_bytes(n, nf, t, FORM_OWNER) <= h->smem_optin) return Key{FORM_OWNER, t, n, nf};
         }
-        return Key{FORM_ROUNDS, td.team, n, nf};
+        if (team_smem_bytes(n, nf, td.team, FORM_ROUNDS) <= h->smem_optin) return Key{FORM_ROUNDS, td.team, n, nf};
+        // too large for shared memory in any form: the gather form (no per-team packing) with its
+        // team state in global memory
+        return Key{FORM_GATHER, std::max(td.team, n > 1024 ? 512 : 256), n, nf};
     };
     std::vector<Key> keys(h->max_systems);
     for (int s : ids) keys[s] = key_of(s);
@@ -673,6 +676,7 @@ int smr_set_grid(smr_handle* h, const void* coef, int dtype, const float scale[4
     if (!h || !coef || !p0 || !step) return SMR_ERR_ARG;
     if (dtype < 0 || dtype > 2) return fail(h, SMR_ERR_ARG, "unknown grid dtype %d", dtype);
     if (nx < 4 || ny < 4 || nz < 4) return fail(h, SMR_ERR_ARG, "grid must be at least 4x4x4 (got %dx%dx%d)", nx, ny, nz);
+    if ((double)nx * ny * nz >= 2147483648.0) return fail(h, SMR_ERR_ARG, "grid of %dx%dx%d has 2^31 voxels or more", nx, ny, nz);
     if (!(step[0] > 0 && step[1] > 0 && step[2] > 0)) return fail(h, SMR_ERR_ARG, "grid steps must be positive");
     size_t nv = (size_t)nx * ny * nz, bytes = nv * voxel_bytes(dtype);
     void* d = nullptr;
@@ -744,6 +748,7 @@ int smr_build_grid(smr_handle* h, int nions, const double* ions, const double* i
                    int nx, int ny, int nz, const double p0[3], const double step[3], const smr_grid_build_params* p) {
     if (!h || !ions || !ion_re || !p0 || !step || !p || nions <= 0) return SMR_ERR_ARG;
     if (nx < 4 || ny < 4 || nz < 4) return fail(h, SMR_ERR_ARG, "grid must be at least 4x4x4");
+    if ((double)nx * ny * nz >= 2147483648.0) return fail(h, SMR_ERR_ARG, "grid of %dx%dx%d has 2^31 voxels or more", nx, ny, nz);
     if (!(Lx > 0 && Ly > 0)) return fail(h, SMR_ERR_ARG, "cell must be positive");
     if (p->dtype < 0 || p->dtype > 2) return fail(h, SMR_ERR_ARG, "unknown grid dtype");
     double *dions = nullptr, *dre = nullptr;

@@ -33,6 +33,7 @@
 #include <cstdio>
 #include <map>
 #include <tuple>
+#include <type_traits>
 
 #include "smr_internal.h"
 
@@ -136,7 +137,7 @@ template <class Rec> __device__ __forceinline__ Rec load_rec(const Rec* p) {
 }
 
 // ---- grid voxel loads
-template <int GDT> __device__ __forceinline__ float4 load_voxel(const void* g, size_t i);
+template <int GDT> __device__ __forceinline__ float4 load_voxel(const void* g, unsigned i);
 // Grid voxels are read through the non-coherent path without allocating in L1: the stencil
 // lines are used once per atom-step and would otherwise evict the topology records.
 __device__ __forceinline__ float4 ldg_stream(const float4* p) {
@@ -149,16 +150,16 @@ __device__ __forceinline__ uint2 ldg_stream(const uint2* p) {
     asm("ld.global.nc.L1::no_allocate.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "l"(p));
     return v;
 }
-template <> __device__ __forceinline__ float4 load_voxel<GRID_F32>(const void* g, size_t i) {
+template <> __device__ __forceinline__ float4 load_voxel<GRID_F32>(const void* g, unsigned i) {
     return ldg_stream(reinterpret_cast<const float4*>(g) + i);
 }
-template <> __device__ __forceinline__ float4 load_voxel<GRID_F16>(const void* g, size_t i) {
+template <> __device__ __forceinline__ float4 load_voxel<GRID_F16>(const void* g, unsigned i) {
     uint2 u = ldg_stream(reinterpret_cast<const uint2*>(g) + i);
     float2 a = __half22float2(*reinterpret_cast<const __half2*>(&u.x));
     float2 b = __half22float2(*reinterpret_cast<const __half2*>(&u.y));
     return make_float4(a.x, a.y, b.x, b.y);
 }
-template <> __device__ __forceinline__ float4 load_voxel<GRID_BF16>(const void* g, size_t i) {
+template <> __device__ __forceinline__ float4 load_voxel<GRID_BF16>(const void* g, unsigned i) {
     uint2 u = ldg_stream(reinterpret_cast<const uint2*>(g) + i);
     float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.x));
     float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.y));
@@ -192,13 +193,17 @@ __device__ __noinline__ bool beyond_cutoff_fp64(float4 pi, float4 li, float4 pj,
 
 // One LJ + damped-Coulomb pair (getLJQH, opencl/UFF.cl:82-95) added to the force / energy of atom i;
 // excluded pairs and pairs beyond the cutoff are evaluated at r^2 = 1 and weighted 0.
+template <bool CUT>
 __device__ __forceinline__ void nb_pair(const KernelArgs& a, float4 pi, float4 li, float4 qi, float4 pj, float4 lj, float4 qj,
                                         bool excluded, float& fx, float& fy, float& fz, float& E) {
     const float dx = (pj.x - pi.x) + (lj.x - li.x), dy = (pj.y - pi.y) + (lj.y - li.y), dz = (pj.z - pi.z) + (lj.z - li.z);
     float r2 = dx * dx + dy * dy + dz * dz;
-    bool out = r2 > a.rc2;
-    // at the cutoff: decide in FP64, so FP32 rounding never moves a pair across it
-    if (fabsf(r2 - a.rc2) < 1e-4f * a.rc2) out = beyond_cutoff_fp64(pi, li, pj, lj, a.rc2);
+    bool out = false;
+    if (CUT) {
+        out = r2 > a.rc2;
+        // at the cutoff: decide in FP64, so FP32 rounding never moves a pair across it
+        if (fabsf(r2 - a.rc2) < 1e-4f * a.rc2) out = beyond_cutoff_fp64(pi, li, pj, lj, a.rc2);
+    }
     const bool skip = excluded || out;
     r2 = skip ? 1.0f : r2;
     const float R0 = qi.x + qj.x, E0 = qi.y * qj.y, Q = qi.z * qj.z;
@@ -545,6 +550,9 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
         const int L = a.nb_lanes > 0 ? min(a.nb_lanes, min(T, 32)) : nb_lanes(Neff, T), G = T / L;
         const int c = rank & (L - 1);
         const bool small = N <= 64;
+        // the partner loop with the cutoff logic compiled in or out (uniform per launch)
+        auto nb_atoms = [&](auto cut_tag) {
+        constexpr bool CUT = decltype(cut_tag)::value;
         for (int i0 = 0; i0 < N; i0 += G) {
             const int i = i0 + rank / L;
             float fx = 0.f, fy = 0.f, fz = 0.f, E = 0.f;
@@ -557,7 +565,7 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
 #pragma unroll 4
                     for (int e = c; e < cnt; e += L) {
                         const int j = row[e];
-                        nb_pair(a, pi, li, qi, S.P()[j], S.Lo()[j], S.Q()[j], false, fx, fy, fz, E);
+                        nb_pair<CUT>(a, pi, li, qi, S.P()[j], S.Lo()[j], S.Q()[j], false, fx, fy, fz, E);
                     }
                 } else {
                     const short4 ng = S.Ng()[i];
@@ -569,7 +577,7 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
 #pragma unroll 4
                     for (int j = c; j < N; j += L) {
                         const bool excl = small ? (bool)((ex >> j) & 1ull) : (j == i || j == ng.x || j == ng.y || j == ng.z || j == ng.w);
-                        nb_pair(a, pi, li, qi, S.P()[j], S.Lo()[j], S.Q()[j], excl, fx, fy, fz, E);
+                        nb_pair<CUT>(a, pi, li, qi, S.P()[j], S.Lo()[j], S.Q()[j], excl, fx, fy, fz, E);
                     }
                 }
             }
@@ -583,6 +591,9 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
                 acc.add(4, 0.5 * (double)E);
             }
         }
+        };
+        if (a.rc2 < 1e37f) nb_atoms(std::integral_constant<bool, true>{});
+        else nb_atoms(std::integral_constant<bool, false>{});
     }
     team_sync<T>();
 
@@ -614,19 +625,23 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
                     // stored-value scales: per z plane (this lane reads one plane) or per channel
                     const float4 zs = g.zscale ? __ldg(g.zscale + (iz - 1 + kz)) : make_float4(g.scale[0], g.scale[1], g.scale[2], 1.f);
                     PLx *= zs.x; PLy *= zs.y; PLz *= zs.z;
+                    // 32-bit voxel indices (the host keeps grids below 2^31 voxels): column offsets of
+                    // the 4 x and 4 y stencil rows, wrapped periodically, then one add per voxel
                     const int x0 = imod(ix - 1, g.nx), y0 = imod(iy - 1, g.ny);
-                    const size_t zoff = (size_t)(iz - 1 + kz);
+                    const int nyz = g.ny * g.nz;
+                    int yo[4];
+#pragma unroll
+                    for (int b = 0; b < 4; b++) { const int yg = y0 + b; yo[b] = (yg >= g.ny ? yg - g.ny : yg) * g.nz; }
+                    const int zoff = iz - 1 + kz;
                     float sE = 0.f, sX = 0.f, sY = 0.f;
 #pragma unroll
                     for (int ax = 0; ax < 4; ax++) {
-                        int xg = x0 + ax;
-                        if (xg >= g.nx) xg -= g.nx;
+                        const int xg = x0 + ax;
+                        const int xo = (xg >= g.nx ? xg - g.nx : xg) * nyz + zoff;
                         float pE = 0.f, pY = 0.f;
 #pragma unroll
                         for (int b = 0; b < 4; b++) {
-                            int yg = y0 + b;
-                            if (yg >= g.ny) yg -= g.ny;
-                            const float4 v = load_voxel<GDT>(g.data, zoff + (size_t)g.nz * ((size_t)yg + (size_t)g.ny * (size_t)xg));
+                            const float4 v = load_voxel<GDT>(g.data, (unsigned)(xo + yo[b]));
                             const float cs = PLx * v.x + PLy * v.y + PLz * v.z;
                             pE += by[b] * cs; pY += dyw[b] * cs;
                         }
@@ -847,7 +862,11 @@ __device__ void run_system(const KernelArgs& a, const Smem& S, int w, int rank) 
     team_sync<T>();
 }
 
-template <int T, int GDT, bool EVAL, int FORM>
+// GS (global state): the team's state lives in a slot of the global scratch instead of shared
+// memory, for systems too large for it (team syncs order global memory within the block just as
+// shared memory).  A compile-time choice: with the base pointer chosen at run time the compiler
+// could no longer use shared-memory instructions for the state.
+template <int T, int GDT, bool EVAL, int FORM, bool GS>
 // warp teams: 4 per block; a 40-atom system's shared memory allows 7 blocks per SM in the rounds
 // and gather forms and 6 in the owner form (slot pieces), which leaves it 85 registers
 __global__ void __launch_bounds__(T == 32 ? 128 : T, T == 32 ? (FORM == FORM_OWNER ? 6 : 7) : 1)
@@ -856,9 +875,7 @@ relax_kernel(const KernelArgs a) {
     const int team = (T == 32) ? (threadIdx.x >> 5) : 0;
     const int rank = (T == 32) ? (threadIdx.x & 31) : threadIdx.x;
     const size_t tb = team_bytes(a.nmax, a.nfmax, T, FORM);
-    // the team's state: shared memory, or for systems too large for it a slot of the global
-    // scratch (team syncs order global memory within the block just as shared memory)
-    char* tbase = a.gscratch ? a.gscratch + ((size_t)blockIdx.x * (T == 32 ? 4 : 1) + team) * tb : smem + (size_t)team * tb;
+    char* tbase = GS ? a.gscratch + ((size_t)blockIdx.x * (T == 32 ? 4 : 1) + team) * tb : smem + (size_t)team * tb;
     const Smem S = carve(tbase, a.nmax);
     __shared__ int s_w;
     for (;;) {
@@ -877,13 +894,13 @@ relax_kernel(const KernelArgs a) {
     }
 }
 
-template <int T, int GDT, bool EVAL, int FORM>
+template <int T, int GDT, bool EVAL, int FORM, bool GS>
 int launch_t(const KernelArgs& a, cudaStream_t s, int num_sms) {
     const int tpb = (T == 32) ? 4 : 1;           // teams per block
     const int block = T * tpb;
     const size_t state = (size_t)tpb * team_bytes(a.nmax, a.nfmax, T, FORM);
-    const size_t smem = a.gscratch ? 0 : state;   // global-state launches use no dynamic shared memory
-    auto kern = relax_kernel<T, GDT, EVAL, FORM>;
+    const size_t smem = GS ? 0 : state;           // global-state launches use no dynamic shared memory
+    auto kern = relax_kernel<T, GDT, EVAL, FORM, GS>;
     static std::map<size_t, int> occ_cache;
     int occ;
     auto it = occ_cache.find(smem);
@@ -902,7 +919,7 @@ int launch_t(const KernelArgs& a, cudaStream_t s, int num_sms) {
     if (occ < 1) return (int)cudaErrorInvalidConfiguration;
     int blocks_needed = (a.nwork + tpb - 1) / tpb;
     int grid = min(blocks_needed, occ * num_sms);
-    if (a.gscratch) grid = min(grid, (int)(a.gscratch_bytes / state));   // one scratch slot per block
+    if (GS) grid = min(grid, (int)(a.gscratch_bytes / state));   // one scratch slot per block
     if (grid < 1) grid = 1;
     kern<<<grid, block, smem, s>>>(a);
     return (int)cudaGetLastError();
@@ -910,12 +927,24 @@ int launch_t(const KernelArgs& a, cudaStream_t s, int num_sms) {
 
 template <int GDT, bool EVAL, int FORM>
 int launch_team(const KernelArgs& a, int team, cudaStream_t s, int num_sms) {
+    if (a.gscratch) {
+        // global-state launches exist for the gather form with 128-512 threads (the host sends
+        // every system too large for shared memory there)
+        if constexpr (FORM == FORM_GATHER) {
+            switch (team) {
+                case 128: return launch_t<128, GDT, EVAL, FORM, true>(a, s, num_sms);
+                case 256: return launch_t<256, GDT, EVAL, FORM, true>(a, s, num_sms);
+                case 512: return launch_t<512, GDT, EVAL, FORM, true>(a, s, num_sms);
+            }
+        }
+        return (int)cudaErrorInvalidValue;
+    }
     switch (team) {
-        case 32: return launch_t<32, GDT, EVAL, FORM>(a, s, num_sms);
-        case 64: return launch_t<64, GDT, EVAL, FORM>(a, s, num_sms);
-        case 128: return launch_t<128, GDT, EVAL, FORM>(a, s, num_sms);
-        case 256: return launch_t<256, GDT, EVAL, FORM>(a, s, num_sms);
-        case 512: return launch_t<512, GDT, EVAL, FORM>(a, s, num_sms);
+        case 32: return launch_t<32, GDT, EVAL, FORM, false>(a, s, num_sms);
+        case 64: return launch_t<64, GDT, EVAL, FORM, false>(a, s, num_sms);
+        case 128: return launch_t<128, GDT, EVAL, FORM, false>(a, s, num_sms);
+        case 256: return launch_t<256, GDT, EVAL, FORM, false>(a, s, num_sms);
+        case 512: return launch_t<512, GDT, EVAL, FORM, false>(a, s, num_sms);
     }
     return (int)cudaErrorInvalidValue;
 }
