@@ -343,6 +343,13 @@ class RelaxMulti:
     # -- systems
     def add_systems(self, topo_ids, positions) -> np.ndarray:
         topo_ids = _i(topo_ids)
+        if len(positions) != len(topo_ids):
+            raise ValueError(f"{len(topo_ids)} topology ids but {len(positions)} position arrays")
+        for t, p in zip(topo_ids, positions):       # the C call reads natoms x 3 floats per system
+            if 0 <= int(t) < len(self.topo_n) and np.asarray(p).size != 3 * self.topo_n[int(t)]:
+                raise ValueError(f"topology {int(t)} has {self.topo_n[int(t)]} atoms, positions have {np.asarray(p).size // 3}")
+        if len(topo_ids) == 0:
+            return np.zeros(0, np.int32)
         pos = _f(np.concatenate([np.asarray(p, dtype=np.float64).reshape(-1, 3) for p in positions]))
         slots = np.zeros(len(topo_ids), np.int32)
         self._chk(self.L.smr_add_systems(self.h, len(topo_ids), _p(topo_ids, N.IP), _p(pos, N.FP), _p(slots, N.IP)),
@@ -361,6 +368,14 @@ class RelaxMulti:
 
     def set_positions(self, slots, positions):
         slots = _i(slots)
+        if len(positions) != len(slots):
+            raise ValueError(f"{len(slots)} slots but {len(positions)} position arrays")
+        for s, p in zip(slots, positions):           # the C call reads natoms x 3 floats per slot
+            n = self.natoms_of.get(int(s))
+            if n is not None and np.asarray(p).size != 3 * n:
+                raise ValueError(f"slot {int(s)} has {n} atoms, positions have {np.asarray(p).size // 3}")
+        if len(slots) == 0:
+            return
         pos = _f(np.concatenate([np.asarray(p).reshape(-1, 3) for p in positions]))
         self._chk(self.L.smr_set_positions(self.h, len(slots), _p(slots, N.IP), _p(pos, N.FP)), "smr_set_positions")
 
@@ -379,7 +394,7 @@ class RelaxMulti:
     def eval_forces(self, slots):
         """One force evaluation: list of (n, 4) float32 arrays (fx, fy, fz, E_atom), energies (nsys, 8)."""
         slots = _i(slots)
-        tot = sum(self.natoms_of[int(s)] for s in slots)
+        tot = sum(self.natoms_of.get(int(s), 0) for s in slots)
         F = np.zeros((tot, 4), np.float32)
         E = np.zeros((len(slots), 8))
         self._chk(self.L.smr_eval_forces(self.h, len(slots), _p(slots, N.IP), _p(F, N.FP), _p(E, N.DP)),
@@ -397,7 +412,7 @@ class RelaxMulti:
 
     def download(self, slots, pos=True, forces=True):
         slots = _i(slots)
-        tot = sum(self.natoms_of[int(s)] for s in slots)
+        tot = sum(self.natoms_of.get(int(s), 0) for s in slots)
         P = np.zeros((tot, 3), np.float32) if pos else None
         F = np.zeros((tot, 4), np.float32) if forces else None
         E = np.zeros((len(slots), 8))
@@ -411,7 +426,7 @@ class RelaxMulti:
     def download_pos64(self, slots):
         """Positions at full precision (float + its accumulated rounding error), list of (n, 3) float64."""
         slots = _i(slots)
-        tot = sum(self.natoms_of[int(s)] for s in slots)
+        tot = sum(self.natoms_of.get(int(s), 0) for s in slots)
         P = np.zeros((tot, 3), np.float64)
         self._chk(self.L.smr_download_pos64(self.h, len(slots), _p(slots, N.IP), _p(P, N.DP)), "smr_download_pos64")
         return self._split(slots, P, 3)
