@@ -476,7 +476,7 @@ def run_ragged(args, ws, rank, local):
 
 # ---------------------------------------------------------------------------------------- served workload
 SERVE = dict(nmin=20, nmax=2000, rcut=10.0, fconv=1e-4, max_steps=3000, chunk=200, budget_gb=150.0,
-             rates=(2000.0, 10000.0, 50000.0), per_rate=1500, max_systems=2048, plain_sample=8, resident=0)
+             rates=(200.0, 2000.0, 10000.0, 50000.0), per_rate=1500, max_systems=2048, plain_sample=8, resident=0)
 
 
 def run_serve(args, local):

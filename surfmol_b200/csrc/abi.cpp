@@ -4,6 +4,7 @@
 #include <atomic>
 #include <cstdint>
 #include <chrono>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -78,6 +79,7 @@ struct smr_handle {
     double* ecomp = nullptr;
     int* xfer = nullptr;            // 3 * max_systems ints for gather / scatter descriptors
     std::vector<SlotState> hs;      // host mirror of slots
+    std::vector<uint32_t> skey;     // per slot: Morton code of the system's lateral centre in the grid cell
     std::vector<int> free_slots;
     std::map<long long, long long> free_atoms;   // offset -> length
     float4* pinned = nullptr;       // staging for uploads / downloads (max_atoms float4)
@@ -409,6 +411,7 @@ KernelArgs base_args(smr_handle* h) {
     for (int k = 0; k < 3; k++) { a.grid.p0[k] = (float)h->gp0[k]; a.grid.inv_step[k] = (float)(1.0 / h->gstep[k]); }
     for (int k = 0; k < 4; k++) a.grid.scale[k] = h->has_grid ? h->gscale[k] : 1.f;
     a.grid.zscale = (h->has_grid && !h->gzscale.empty()) ? h->dzscale.d : nullptr;
+    a.grid.p0z = h->gp0[2]; a.grid.stepz = h->gstep[2];
     a.R2damp = h->nb.rdamp * h->nb.rdamp;
     a.alpha_morse = h->nb.alpha_morse;
     a.rc2 = h->nb.rcut > 0 ? h->nb.rcut * h->nb.rcut : 3.0e38f;
@@ -451,6 +454,8 @@ std::vector<Seg> group_by(smr_handle* h, std::vector<int>& ids, int form, int re
         const Key &x = keys[a], &y = keys[b];
         if (x.form != y.form) return x.form < y.form;
         if (x.team != y.team) return x.team < y.team;
+        // systems that run at the same time then cover a small patch of the grid (L2 reuse)
+        if (h->skey[a] != h->skey[b]) return h->skey[a] < h->skey[b];
         return x.n < y.n;
     });
     std::vector<Seg> segs;
@@ -471,9 +476,6 @@ std::vector<Seg> group_by(smr_handle* h, std::vector<int>& ids, int form, int re
     return segs;
 }
 
-bool fits(const smr_handle* h, const Seg& g) {
-    return team_smem_bytes(g.nmax, g.nfmax, g.team, g.form) <= h->smem_optin;
-}
 
 // Global-memory team state for the segments that do not fit in shared memory: each such segment
 // gets its own region (segments of one stage run concurrently) of two blocks' state per SM.
@@ -546,6 +548,7 @@ int smr_create(const smr_config* cfg, smr_handle** out) {
         cudaMemsetAsync(h->plo, 0, na * 16, h->stream) || cudaStreamSynchronize(h->stream))
         return bail(SMR_ERR_CUDA);
     h->hs.assign(ns, SlotState{});
+    h->skey.assign(ns, 0u);
     for (int s = (int)ns - 1; s >= 0; s--) h->free_slots.push_back(s);
     h->free_atoms[0] = (long long)na;
     cudaEventCreate(&h->ev0);
@@ -869,6 +872,22 @@ int smr_topology_export(smr_handle* h, int id, int* neighs, int* neighBs, int* b
 
 const char* smr_type_name(int id) { return type_name(id); }
 
+// Launch order key of a system: Morton code (10 + 10 bits) of its lateral centre within the
+// periodic grid cell, so a launch's work list walks the substrate patch by patch.
+static uint32_t locality_key(const smr_handle* h, const float* pos, int n) {
+    if (!h->has_grid || n <= 0) return 0u;
+    double cx = 0, cy = 0;
+    for (int a = 0; a < n; a++) { cx += pos[3 * a]; cy += pos[3 * a + 1]; }
+    cx /= n; cy /= n;
+    const double Lx = h->gdim[0] * h->gstep[0], Ly = h->gdim[1] * h->gstep[1];
+    double fx = (cx - h->gp0[0]) / Lx, fy = (cy - h->gp0[1]) / Ly;
+    fx -= std::floor(fx); fy -= std::floor(fy);
+    const uint32_t qx = std::min<uint32_t>(1023u, (uint32_t)(fx * 1024.0)), qy = std::min<uint32_t>(1023u, (uint32_t)(fy * 1024.0));
+    uint32_t k = 0;
+    for (int b = 0; b < 10; b++) k |= ((qx >> b) & 1u) << (2 * b) | ((qy >> b) & 1u) << (2 * b + 1);
+    return k;
+}
+
 int smr_add_systems(smr_handle* h, int nsys, const int* topo_ids, const float* pos, int* slot_ids) {
     if (!h || nsys < 0 || (nsys && (!topo_ids || !pos || !slot_ids))) return SMR_ERR_ARG;
     if ((int)h->free_slots.size() < nsys) return fail(h, SMR_ERR_CAPACITY, "only %zu free slots for %d systems", h->free_slots.size(), nsys);
@@ -893,6 +912,7 @@ int smr_add_systems(smr_handle* h, int nsys, const int* topo_ids, const float* p
         st = SlotState{};
         st.topo = topo_ids[i]; st.atom_off = (int)off; st.natoms = n; st.active = 1; st.dt = -1.0;
         ids[i] = s; src[i] = (int)p; len[i] = n; dst[i] = (int)off;
+        h->skey[s] = locality_key(h, pos + 3 * p, n);
         for (int a = 0; a < n; a++) h->pinned[p + a] = make_float4(pos[3 * (p + a)], pos[3 * (p + a) + 1], pos[3 * (p + a) + 2], 0.f);
         p += n;
     }
@@ -934,6 +954,7 @@ int smr_set_positions(smr_handle* h, int nsys, const int* slot_ids, const float*
         if (!valid_slot(h, slot_ids[i])) return fail(h, SMR_ERR_ARG, "slot %d not active", slot_ids[i]);
         const SlotState& st = h->hs[slot_ids[i]];
         src[i] = (int)p; len[i] = st.natoms; dst[i] = st.atom_off;
+        h->skey[slot_ids[i]] = locality_key(h, pos + 3 * p, st.natoms);
         for (int a = 0; a < st.natoms; a++) h->pinned[p + a] = make_float4(pos[3 * (p + a)], pos[3 * (p + a) + 1], pos[3 * (p + a) + 2], 0.f);
         p += st.natoms;
     }
@@ -1077,7 +1098,7 @@ static void sig_args(std::vector<long long>& v, const KernelArgs& a) {
     P(a.grid.data); v.push_back(a.grid.dtype); v.push_back(a.grid.nx); v.push_back(a.grid.ny); v.push_back(a.grid.nz);
     for (int k = 0; k < 3; k++) { F(a.grid.p0[k]); F(a.grid.inv_step[k]); }
     for (int k = 0; k < 4; k++) F(a.grid.scale[k]);
-    P(a.grid.zscale);
+    P(a.grid.zscale); D(a.grid.p0z); D(a.grid.stepz);
     v.push_back(a.has_grid); F(a.R2damp); F(a.alpha_morse); F(a.rc2);
     D(a.fire.dt0); D(a.fire.dt_max); D(a.fire.alpha0); D(a.fire.f_inc); D(a.fire.f_dec); D(a.fire.f_alpha);
     D(a.fire.fconv); D(a.fire.flimit); v.push_back(a.fire.n_min);

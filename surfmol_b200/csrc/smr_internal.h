@@ -75,6 +75,7 @@ struct GridView {
     float inv_step[3];
     float scale[4];               // per-channel scale of the stored values (when zscale is null)
     const float4* zscale;         // 16-bit grids: per z plane and channel scale (null: scale[])
+    double p0z, stepz;            // z origin and step in FP64 (cell decisions at the grid's z bounds)
 };
 
 struct FireDev {
