@@ -292,6 +292,11 @@ int smr_set_team_size(smr_handle* h, int max_atoms, int threads);
 #define SMR_TUNE_NBLIST_MIN 2
 #define SMR_TUNE_NBLIST_SKIN_MA 3
 #define SMR_TUNE_NBLIST_CAP 4
+/*   SMR_TUNE_WATCHDOG_MS    the longest a call waits for its device work (default 3600000).  A call
+ *                           that gives up returns SMR_ERR_TIMEOUT with the work still running; the
+ *                           next call on the handle first waits for it (bounded by the same limit)
+ *                           and refreshes its copy of the per-system state, so no result is lost */
+#define SMR_TUNE_WATCHDOG_MS 5
 int smr_set_tuning(smr_handle* h, int key, int value);
 int smr_get_tuning(smr_handle* h, int key, int* value);
 

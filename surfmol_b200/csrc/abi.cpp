@@ -110,6 +110,11 @@ struct smr_handle {
     int eval_form = FORM_ROUNDS;        // form and team (0: by size) of smr_eval_forces
     int eval_team = 0;
     int nb_lanes = 0;                   // tuning: lanes per atom of the NB loop (0: by size)
+    // watchdog: the longest a call waits for its device work; a call that gives up returns
+    // SMR_ERR_TIMEOUT with the work still running and marks the handle pending, and the next call
+    // first waits for it (again bounded) and refreshes the host copy of the slot table
+    double watchdog_s = 3600.0;
+    bool pending = false;
     // NB neighbour lists for systems of at least nbl_min atoms under a cutoff (0: off)
     int nbl_min = 128, nbl_cap = 256, nbl_skin_ma = 1000;
     DArr<unsigned short> nbl; DArr<int> nbl_cnt; DArr<float4> nbl_ref;
@@ -368,7 +373,11 @@ int wait_stream(smr_handle* h, double timeout_s) {
         if (q == cudaSuccess) break;
         if (q != cudaErrorNotReady) { cudaEventDestroy(e); return fail(h, SMR_ERR_CUDA, "stream: %s", cudaGetErrorString(q)); }
         double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-        if (dt > timeout_s) { cudaEventDestroy(e); return fail(h, SMR_ERR_TIMEOUT, "device work not finished after %.0f s", timeout_s); }
+        if (dt > timeout_s) {
+            cudaEventDestroy(e);
+            h->pending = true;
+            return fail(h, SMR_ERR_TIMEOUT, "device work not finished after %.3f s (the handle waits for it on the next call)", timeout_s);
+        }
         std::this_thread::sleep_for(std::chrono::microseconds(dt < 0.01 ? 5 : 200));
     }
     cudaEventDestroy(e);
@@ -377,16 +386,26 @@ int wait_stream(smr_handle* h, double timeout_s) {
 
 int download_slots(smr_handle* h) {
     CU(h, cudaMemcpyAsync(h->hs.data(), h->slots, h->hs.size() * sizeof(SlotState), cudaMemcpyDeviceToHost, h->stream));
-    return wait_stream(h, 3600.0);
+    return wait_stream(h, h->watchdog_s);
 }
+
+// after a watchdog timeout: wait for the abandoned work (bounded), then refresh the slot table
+int settle(smr_handle* h) {
+    if (!h->pending) return 0;
+    int r = wait_stream(h, h->watchdog_s);
+    if (r) return r;
+    h->pending = false;
+    return download_slots(h);
+}
+#define SETTLE(h) do { int r_ = settle(h); if (r_) return r_; } while (0)
 
 int upload_slots(smr_handle* h, const std::vector<int>& ids) {
     if (ids.size() > 32) {   // many slots: one copy of the whole table
         CU(h, cudaMemcpyAsync(h->slots, h->hs.data(), h->hs.size() * sizeof(SlotState), cudaMemcpyHostToDevice, h->stream));
-        return wait_stream(h, 600.0);   // hs is pageable host memory: finish before it can change
+        return wait_stream(h, h->watchdog_s);   // hs is pageable host memory: finish before it can change
     }
     for (int s : ids) CU(h, cudaMemcpyAsync(h->slots + s, &h->hs[s], sizeof(SlotState), cudaMemcpyHostToDevice, h->stream));
-    return wait_stream(h, 600.0);
+    return wait_stream(h, h->watchdog_s);
 }
 
 KernelArgs base_args(smr_handle* h) {
@@ -598,6 +617,11 @@ int smr_set_tuning(smr_handle* h, int key, int value) {
         h->nb_lanes = value;
         return SMR_OK;
     }
+    if (key == SMR_TUNE_WATCHDOG_MS) {
+        if (value < 1) return fail(h, SMR_ERR_ARG, "watchdog must be at least 1 ms");
+        h->watchdog_s = 1e-3 * value;
+        return SMR_OK;
+    }
     if (key == SMR_TUNE_NBLIST_MIN) {
         if (value < 0) return fail(h, SMR_ERR_ARG, "neighbour-list size threshold must be >= 0");
         h->nbl_min = value;
@@ -623,6 +647,7 @@ int smr_get_tuning(smr_handle* h, int key, int* value) {
     if (!h || !value) return SMR_ERR_ARG;
     if (key == SMR_TUNE_NB_LANES) { *value = h->nb_lanes; return SMR_OK; }
     if (key == SMR_TUNE_NBLIST_MIN) { *value = h->nbl_min; return SMR_OK; }
+    if (key == SMR_TUNE_WATCHDOG_MS) { *value = (int)std::min(2.0e9, h->watchdog_s * 1e3); return SMR_OK; }
     if (key == SMR_TUNE_NBLIST_SKIN_MA) { *value = h->nbl_skin_ma; return SMR_OK; }
     if (key == SMR_TUNE_NBLIST_CAP) { *value = h->nbl_cap; return SMR_OK; }
     return fail(h, SMR_ERR_ARG, "unknown tuning key %d", key);
@@ -630,6 +655,7 @@ int smr_get_tuning(smr_handle* h, int key, int* value) {
 
 int smr_set_team_size(smr_handle* h, int max_atoms, int threads) {
     if (!h) return SMR_ERR_ARG;
+    SETTLE(h);
     if (threads != 0 && threads != 32 && threads != 64 && threads != 128 && threads != 256 && threads != 512)
         return fail(h, SMR_ERR_ARG, "team size must be 32, 64, 128, 256 or 512");
     if (threads == 0) h->team_override.erase(max_atoms);
@@ -677,6 +703,7 @@ int smr_get_grid_planes(smr_handle* h, float* plane_scale) {
 int smr_set_grid(smr_handle* h, const void* coef, int dtype, const float scale[4], int nx, int ny, int nz,
                  const double p0[3], const double step[3]) {
     if (!h || !coef || !p0 || !step) return SMR_ERR_ARG;
+    SETTLE(h);
     if (dtype < 0 || dtype > 2) return fail(h, SMR_ERR_ARG, "unknown grid dtype %d", dtype);
     if (nx < 4 || ny < 4 || nz < 4) return fail(h, SMR_ERR_ARG, "grid must be at least 4x4x4 (got %dx%dx%d)", nx, ny, nz);
     if ((double)nx * ny * nz >= 2147483648.0) return fail(h, SMR_ERR_ARG, "grid of %dx%dx%d has 2^31 voxels or more", nx, ny, nz);
@@ -698,6 +725,7 @@ int smr_set_grid(smr_handle* h, const void* coef, int dtype, const float scale[4
 
 int smr_get_grid(smr_handle* h, void* coef_out, int* dtype, float scale[4], int dims[3], double p0[3], double step[3]) {
     if (!h) return SMR_ERR_ARG;
+    SETTLE(h);
     if (!h->has_grid) return fail(h, SMR_ERR_STATE, "no grid set");
     if (dtype) *dtype = h->grid_dtype;
     if (scale) for (int k = 0; k < 4; k++) scale[k] = h->gscale[k];
@@ -714,6 +742,7 @@ int smr_get_grid(smr_handle* h, void* coef_out, int* dtype, float scale[4], int 
 
 int smr_convert_grid(smr_handle* h, int dtype) {
     if (!h) return SMR_ERR_ARG;
+    SETTLE(h);
     if (!h->has_grid) return fail(h, SMR_ERR_STATE, "no grid set");
     if (dtype == h->grid_dtype) return SMR_OK;
     size_t nv = (size_t)h->gdim[0] * h->gdim[1] * h->gdim[2];
@@ -750,6 +779,7 @@ int smr_convert_grid(smr_handle* h, int dtype) {
 int smr_build_grid(smr_handle* h, int nions, const double* ions, const double* ion_re, double Lx, double Ly,
                    int nx, int ny, int nz, const double p0[3], const double step[3], const smr_grid_build_params* p) {
     if (!h || !ions || !ion_re || !p0 || !step || !p || nions <= 0) return SMR_ERR_ARG;
+    SETTLE(h);
     if (nx < 4 || ny < 4 || nz < 4) return fail(h, SMR_ERR_ARG, "grid must be at least 4x4x4");
     if ((double)nx * ny * nz >= 2147483648.0) return fail(h, SMR_ERR_ARG, "grid of %dx%dx%d has 2^31 voxels or more", nx, ny, nz);
     if (!(Lx > 0 && Ly > 0)) return fail(h, SMR_ERR_ARG, "cell must be positive");
@@ -788,6 +818,7 @@ int smr_build_grid(smr_handle* h, int nions, const double* ions, const double* i
 int smr_add_molecule(smr_handle* h, int natoms, const int* Z, const double* pos, const double* charges,
                      double bond_cut, int* topo_id) {
     if (!h || !Z || !pos || !topo_id) return SMR_ERR_ARG;
+    SETTLE(h);
     HostTopo T;
     char msg[300] = {0};
     if (build_molecule_topology(natoms, Z, pos, charges, bond_cut > 0 ? bond_cut : 1.8, T, msg, sizeof(msg)))
@@ -804,6 +835,7 @@ int smr_add_molecule(smr_handle* h, int natoms, const int* Z, const double* pos,
 int smr_add_molecules(smr_handle* h, int nmol, const int* natoms, const int* Z, const double* pos, const double* charges,
                       double bond_cut, int* topo_ids) {
     if (!h || nmol < 0 || (nmol && (!natoms || !Z || !pos || !topo_ids))) return SMR_ERR_ARG;
+    SETTLE(h);
     std::vector<long long> off(nmol + 1, 0);
     for (int i = 0; i < nmol; i++) {
         if (natoms[i] <= 0) return fail(h, SMR_ERR_ARG, "molecule %d has %d atoms", i, natoms[i]);
@@ -831,6 +863,7 @@ int smr_add_molecules(smr_handle* h, int nmol, const int* natoms, const int* Z, 
 
 int smr_add_topology(smr_handle* h, const smr_topology_desc* d, int* topo_id) {
     if (!h || !d || !topo_id || !d->req || !d->neighs || !d->bond_kl) return SMR_ERR_ARG;
+    SETTLE(h);
     if ((d->nang && (!d->angs || !d->angp)) || (d->ndih && (!d->dihs || !d->dihp)) || (d->ninv && (!d->invs || !d->invp)))
         return fail(h, SMR_ERR_ARG, "term arrays missing");
     HostTopo T;
@@ -890,6 +923,7 @@ static uint32_t locality_key(const smr_handle* h, const float* pos, int n) {
 
 int smr_add_systems(smr_handle* h, int nsys, const int* topo_ids, const float* pos, int* slot_ids) {
     if (!h || nsys < 0 || (nsys && (!topo_ids || !pos || !slot_ids))) return SMR_ERR_ARG;
+    SETTLE(h);
     if ((int)h->free_slots.size() < nsys) return fail(h, SMR_ERR_CAPACITY, "only %zu free slots for %d systems", h->free_slots.size(), nsys);
     long long need = 0;
     for (int i = 0; i < nsys; i++) {
@@ -927,7 +961,7 @@ int smr_add_systems(smr_handle* h, int nsys, const int* topo_ids, const float* p
     if (launch_copy_segments(h->xfer, h->xfer + nsys, h->xfer + 2 * nsys, nsys, h->stage, h->plo, s)) return fail(h, SMR_ERR_CUDA, "scatter launch failed");
     int r = upload_slots(h, ids);
     if (r) return r;
-    r = wait_stream(h, 600.0);
+    r = wait_stream(h, h->watchdog_s);
     if (r) return r;
     std::copy(ids.begin(), ids.end(), slot_ids);
     return SMR_OK;
@@ -935,6 +969,7 @@ int smr_add_systems(smr_handle* h, int nsys, const int* topo_ids, const float* p
 
 int smr_remove_systems(smr_handle* h, int nsys, const int* slot_ids) {
     if (!h || nsys < 0 || (nsys && !slot_ids)) return SMR_ERR_ARG;
+    SETTLE(h);
     for (int i = 0; i < nsys; i++) if (!valid_slot(h, slot_ids[i])) return fail(h, SMR_ERR_ARG, "slot %d not active", slot_ids[i]);
     std::vector<int> ids(slot_ids, slot_ids + nsys);
     for (int s : ids) {
@@ -947,6 +982,7 @@ int smr_remove_systems(smr_handle* h, int nsys, const int* slot_ids) {
 
 int smr_set_positions(smr_handle* h, int nsys, const int* slot_ids, const float* pos) {
     if (!h || nsys < 0 || (nsys && (!slot_ids || !pos))) return SMR_ERR_ARG;
+    SETTLE(h);
     { int r = check_batch(h, nsys, slot_ids); if (r) return r; }
     std::vector<int> src(nsys), len(nsys), dst(nsys);
     long long p = 0;
@@ -967,7 +1003,7 @@ int smr_set_positions(smr_handle* h, int nsys, const int* slot_ids, const float*
     // new positions carry no accumulated low part
     CU(h, cudaMemsetAsync(h->stage, 0, (size_t)p * 16, h->stream));
     if (launch_copy_segments(h->xfer, h->xfer + nsys, h->xfer + 2 * nsys, nsys, h->stage, h->plo, h->stream)) return fail(h, SMR_ERR_CUDA, "scatter launch failed");
-    return wait_stream(h, 600.0);
+    return wait_stream(h, h->watchdog_s);
 }
 
 int smr_active_slots(smr_handle* h, int* n, int* ids) {
@@ -980,6 +1016,7 @@ int smr_active_slots(smr_handle* h, int* n, int* ids) {
 
 int smr_reset_fire(smr_handle* h, int nsys, const int* slot_ids) {
     if (!h || nsys < 0 || (nsys && !slot_ids)) return SMR_ERR_ARG;
+    SETTLE(h);
     std::vector<int> ids;
     for (int i = 0; i < nsys; i++) {
         int s = slot_ids[i];
@@ -993,6 +1030,7 @@ int smr_reset_fire(smr_handle* h, int nsys, const int* slot_ids) {
 
 int smr_eval_forces(smr_handle* h, int nsys, const int* slot_ids, float* forces, double* energy) {
     if (!h || nsys < 0 || (nsys && !slot_ids)) return SMR_ERR_ARG;
+    SETTLE(h);
     { int r = check_batch(h, nsys, slot_ids); if (r) return r; }
     if (nsys == 0) return SMR_OK;
     std::vector<int> sorted(slot_ids, slot_ids + nsys);
@@ -1016,7 +1054,7 @@ int smr_eval_forces(smr_handle* h, int nsys, const int* slot_ids, float* forces,
         if (r) return fail(h, SMR_ERR_CUDA, "eval launch: %s", cudaGetErrorString((cudaError_t)r));
     }
     cudaEventRecord(h->ev1, s);
-    int r = wait_stream(h, 600.0);
+    int r = wait_stream(h, h->watchdog_s);
     if (r) return r;
     float ms = 0;
     cudaEventElapsedTime(&ms, h->ev0, h->ev1);
@@ -1122,6 +1160,7 @@ int smr_graph_stats(smr_handle* h, long long* replays) {
 
 int smr_run_fire(smr_handle* h, int max_steps, int step_budget, const smr_fire_params* p, int mode, int* nfinished) {
     if (!h || !p || max_steps < 0) return SMR_ERR_ARG;
+    SETTLE(h);
     if (mode != SMR_MODE_BATCHED && mode != SMR_MODE_PLAIN) return fail(h, SMR_ERR_ARG, "unknown mode %d", mode);
     if (!(p->dt0 > 0 && p->dt_max > 0 && p->f_dec > 0 && p->f_inc > 0)) return fail(h, SMR_ERR_ARG, "invalid FIRE parameters");
     // every running slot may advance to min(steps + max_steps, step_budget) in this call
@@ -1294,7 +1333,7 @@ int smr_run_fire(smr_handle* h, int max_steps, int step_budget, const smr_fire_p
         }
     }
     cudaEventRecord(h->ev1, s);
-    r = wait_stream(h, 3600.0);
+    r = wait_stream(h, h->watchdog_s);
     if (r) return r;
     float ms = 0;
     cudaEventElapsedTime(&ms, h->ev0, h->ev1);
@@ -1311,6 +1350,7 @@ int smr_run_fire(smr_handle* h, int max_steps, int step_budget, const smr_fire_p
 
 int smr_download(smr_handle* h, int nsys, const int* slot_ids, float* pos, float* forces, double* energy, int* steps, int* status) {
     if (!h || nsys < 0 || (nsys && !slot_ids)) return SMR_ERR_ARG;
+    SETTLE(h);
     { int r = check_batch(h, nsys, slot_ids); if (r) return r; }
     for (int i = 0; i < nsys; i++) if (!valid_slot(h, slot_ids[i])) return fail(h, SMR_ERR_ARG, "slot %d not active", slot_ids[i]);
     if (!nsys) return SMR_OK;
@@ -1336,7 +1376,7 @@ int smr_download(smr_handle* h, int nsys, const int* slot_ids, float* pos, float
         if (launch_copy_segments(h->xfer, h->xfer + nsys, h->xfer + 2 * nsys, nsys, which == 0 ? h->pos : h->force, h->stage, s))
             return fail(h, SMR_ERR_CUDA, "gather launch failed");
         CU(h, cudaMemcpyAsync(h->pinned, h->stage, p * 16, cudaMemcpyDeviceToHost, s));
-        r = wait_stream(h, 600.0);
+        r = wait_stream(h, h->watchdog_s);
         if (r) return r;
         if (which == 0) for (long long a = 0; a < p; a++) { out[3 * a] = h->pinned[a].x; out[3 * a + 1] = h->pinned[a].y; out[3 * a + 2] = h->pinned[a].z; }
         else std::memcpy(out, h->pinned, p * 16);
@@ -1346,6 +1386,7 @@ int smr_download(smr_handle* h, int nsys, const int* slot_ids, float* pos, float
 
 int smr_download_pos64(smr_handle* h, int nsys, const int* slot_ids, double* pos) {
     if (!h || nsys < 0 || (nsys && (!slot_ids || !pos))) return SMR_ERR_ARG;
+    SETTLE(h);
     { int r = check_batch(h, nsys, slot_ids); if (r) return r; }
     for (int i = 0; i < nsys; i++) if (!valid_slot(h, slot_ids[i])) return fail(h, SMR_ERR_ARG, "slot %d not active", slot_ids[i]);
     if (!nsys) return SMR_OK;
@@ -1363,7 +1404,7 @@ int smr_download_pos64(smr_handle* h, int nsys, const int* slot_ids, double* pos
         if (launch_copy_segments(h->xfer, h->xfer + nsys, h->xfer + 2 * nsys, nsys, which == 0 ? h->pos : h->plo, h->stage, s))
             return fail(h, SMR_ERR_CUDA, "gather launch failed");
         CU(h, cudaMemcpyAsync(h->pinned, h->stage, p * 16, cudaMemcpyDeviceToHost, s));
-        int r = wait_stream(h, 600.0);
+        int r = wait_stream(h, h->watchdog_s);
         if (r) return r;
         if (which == 0) std::memcpy(hi.data(), h->pinned, p * 16);
     }
@@ -1388,6 +1429,7 @@ int smr_topo_prepare(smr_topo* t, int team) {
 
 int smr_add_topos(smr_handle* h, int n, const smr_topo* const* topos, int* topo_ids) {
     if (!h || n < 0 || (n && (!topos || !topo_ids))) return SMR_ERR_ARG;
+    SETTLE(h);
     for (int i = 0; i < n; i++) if (!topos[i]) return fail(h, SMR_ERR_ARG, "topology %d is null", i);
     for (int i = 0; i < n; i++) {
         const smr_topo* t = topos[i];
@@ -1419,12 +1461,14 @@ static int maybe_compact(smr_handle* h) {
 
 int smr_remove_topologies(smr_handle* h, int n, const int* ids) {
     if (!h || n < 0 || (n && !ids)) return SMR_ERR_ARG;
+    SETTLE(h);
     for (int i = 0; i < n; i++) { int r = remove_one_topology(h, ids[i]); if (r) return r; }
     return maybe_compact(h);
 }
 
 int smr_remove_topology(smr_handle* h, int id) {
     if (!h) return SMR_ERR_ARG;
+    SETTLE(h);
     int r = remove_one_topology(h, id);
     if (r) return r;
     return maybe_compact(h);
@@ -1486,6 +1530,7 @@ int smr_topo_rounds(const smr_topo* t, int team, int rounds[3], short* ang_at, s
 
 int smr_add_topo(smr_handle* h, const smr_topo* t, int* topo_id) {
     if (!h || !t || !topo_id) return SMR_ERR_ARG;
+    SETTLE(h);
     h->topos.push_back(t->T);
     h->topo_alive.push_back(1);
     const int team = team_for(h, t->T.n);

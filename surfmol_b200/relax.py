@@ -234,6 +234,11 @@ class RelaxMulti:
         """Lanes per atom in the NB partner loop (0: chosen from system size and team)."""
         self._chk(self.L.smr_set_tuning(self.h, 1, int(lanes)), "smr_set_tuning")
 
+    def set_watchdog(self, ms):
+        """Longest wait for device work per call (ms); a call that gives up raises SmrError (-6) and the
+        next call waits for the abandoned work first."""
+        self._chk(self.L.smr_set_tuning(self.h, 5, int(ms)), "smr_set_tuning")
+
     def set_nblist(self, min_atoms=None, skin=None, cap=None):
         """NB neighbour lists for systems of >= min_atoms atoms under a cutoff (0: off); skin in A."""
         if min_atoms is not None:

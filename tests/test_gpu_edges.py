@@ -149,3 +149,37 @@ def test_error_paths(env):
     R.remove_topology(tid)
     with pytest.raises(SmrError):
         R.add_systems([tid], [P])                                    # released topology
+
+
+def test_watchdog_timeout_and_recovery():
+    """A call whose device work outlasts the watchdog returns SMR_ERR_TIMEOUT (-6) with the work still
+    running; the next call waits for it and refreshes the per-system state, so the results equal
+    those of a run without the timeout, bit for bit.  Only host waits are bounded here: the kernels
+    have no device-side waits."""
+    from surfmol_b200 import RelaxMulti
+    from surfmol_b200.relax import SmrError
+    slab, dims, p0, step = small_slab_grid()
+    rng = np.random.default_rng(9)
+    mols = [molecule_on_slab(rng, 40, slab) for _ in range(16)]
+    outs = []
+    for watchdog in (None, 1):
+        R = RelaxMulti(max_systems=2048, max_atoms=2048 * 40)
+        try:
+            R.set_nb(1.0, 1.5)
+            build_device_grid(R, slab, dims, p0, step)
+            tids = [R.add_molecule(Z, P, q) for Z, P, q in mols]
+            reps = [k % len(mols) for k in range(2048)]
+            s = R.add_systems([tids[k] for k in reps], [mols[k][1] for k in reps])
+            if watchdog:
+                R.set_watchdog(watchdog)
+                with pytest.raises(SmrError, match=r"\(-6\)"):
+                    R.run_fire(1500, step_budget=1500, fconv=1e-4)
+                R.set_watchdog(600000)
+            else:
+                R.run_fire(1500, step_budget=1500, fconv=1e-4)
+            outs.append(R.download(s))
+        finally:
+            R.finish()
+    a, b = outs
+    assert np.array_equal(a["steps"], b["steps"]) and np.array_equal(a["status"], b["status"])
+    assert all(np.array_equal(x, y) for x, y in zip(a["pos"], b["pos"]))
