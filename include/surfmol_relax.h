@@ -194,6 +194,20 @@ int  smr_topo_export(const smr_topo* t, int* neighs, int* neighBs, int* bonds, d
                      int* invs, int* inv_ngs, double* invp, double* req, int* type_id);
 int  smr_topo_rounds(const smr_topo* t, int team, int rounds[3], short* ang_at, short* dih_at, short* inv_at);
 int  smr_add_topo(smr_handle* h, const smr_topo* t, int* topo_id);
+/* Topologies whose bonds and angle / dihedral / inversion lists come from a file (the reference's
+ * TopologyData JSON, crates/libs/moltopo/src/export.rs:12-74, or UFFTOPO binary,
+ * crates/apps/buildff/src/main.rs:10-28): the lists are used as they are, as Uff::from_topology
+ * does (crates/libs/molff/src/uff.rs:238-240); atoms are typed from Z and the bond graph, or take
+ * the given type ids (smr_type_id maps a UFF type name such as "C_R" to its id, -1 if unknown);
+ * parameters follow the same UFF rules as smr_add_molecule.  bonds: nbonds x 2, angs: nang x 3
+ * (centre in the middle), dihs: ndih x 4, invs: ninv x 4 (centre first); charges may be null. */
+int  smr_topo_build_listed(int natoms, const int* Z, const int* type_ids, const double* charges, int nbonds, const int* bonds,
+                           int nang, const int* angs, int ndih, const int* dihs, int ninv, const int* invs, smr_topo** out,
+                           char* err, int errlen);
+int  smr_add_listed_molecule(smr_handle* h, int natoms, const int* Z, const int* type_ids, const double* charges,
+                             int nbonds, const int* bonds, int nang, const int* angs, int ndih, const int* dihs,
+                             int ninv, const int* invs, int* topo_id);
+int  smr_type_id(const char* name);
 /* Pack a host topology's term records for a team size (0: the default for its size) without a
  * handle; thread-safe, so request topologies can be packed while the GPU works.  smr_add_topo then
  * uploads them as they are when the handle's team for that size matches.  No counterpart in the

@@ -79,6 +79,10 @@ SIGNATURES = {
     "smr_topo_export": (C.c_int, [VP, IP, IP, IP, DP, IP, IP, DP, IP, IP, DP, IP, IP, DP, DP, IP]),
     "smr_topo_rounds": (C.c_int, [VP, C.c_int, IP, SP, SP, SP]),
     "smr_add_topo": (C.c_int, [VP, VP, IP]),
+    "smr_topo_build_listed": (C.c_int, [C.c_int, IP, IP, DP, C.c_int, IP, C.c_int, IP, C.c_int, IP, C.c_int, IP,
+                                        C.POINTER(VP), C.c_char_p, C.c_int]),
+    "smr_add_listed_molecule": (C.c_int, [VP, C.c_int, IP, IP, DP, C.c_int, IP, C.c_int, IP, C.c_int, IP, C.c_int, IP, IP]),
+    "smr_type_id": (C.c_int, [C.c_char_p]),
     "smr_topo_prepare": (C.c_int, [VP, C.c_int]),
     "smr_remove_topology": (C.c_int, [VP, C.c_int]),
     "smr_add_topos": (C.c_int, [VP, C.c_int, C.POINTER(VP), IP]),

@@ -861,6 +861,24 @@ int smr_add_molecules(smr_handle* h, int nmol, const int* natoms, const int* Z, 
     return upload_all(h);
 }
 
+int smr_add_listed_molecule(smr_handle* h, int natoms, const int* Z, const int* type_ids, const double* charges,
+                            int nbonds, const int* bonds, int nang, const int* angs, int ndih, const int* dihs,
+                            int ninv, const int* invs, int* topo_id) {
+    if (!h || !Z || !topo_id || (nbonds && !bonds) || (nang && !angs) || (ndih && !dihs) || (ninv && !invs)) return SMR_ERR_ARG;
+    SETTLE(h);
+    HostTopo T;
+    char msg[300] = {0};
+    if (build_listed_topology(natoms, Z, type_ids, charges, nbonds, bonds, nang, angs, ndih, dihs, ninv, invs, T, msg, sizeof(msg)))
+        return fail(h, SMR_ERR_ARG, "topology: %s", msg);
+    h->topos.push_back(std::move(T));
+    h->topo_alive.push_back(1);
+    append_topology(h, h->topos.back());
+    int r = upload_all(h);
+    if (r) return r;
+    *topo_id = (int)h->topos.size() - 1;
+    return SMR_OK;
+}
+
 int smr_add_topology(smr_handle* h, const smr_topology_desc* d, int* topo_id) {
     if (!h || !d || !topo_id || !d->req || !d->neighs || !d->bond_kl) return SMR_ERR_ARG;
     SETTLE(h);
@@ -1489,6 +1507,25 @@ int smr_topo_build(int natoms, const int* Z, const double* pos, const double* ch
     *out = t;
     return SMR_OK;
 }
+
+int smr_topo_build_listed(int natoms, const int* Z, const int* type_ids, const double* charges, int nbonds, const int* bonds,
+                          int nang, const int* angs, int ndih, const int* dihs, int ninv, const int* invs, smr_topo** out,
+                          char* err, int errlen) {
+    if (!Z || !out || (nbonds && !bonds) || (nang && !angs) || (ndih && !dihs) || (ninv && !invs)) return SMR_ERR_ARG;
+    *out = nullptr;
+    smr_topo* t = new (std::nothrow) smr_topo();
+    if (!t) return SMR_ERR_CAPACITY;
+    char msg[300] = {0};
+    if (build_listed_topology(natoms, Z, type_ids, charges, nbonds, bonds, nang, angs, ndih, dihs, ninv, invs, t->T, msg, sizeof(msg))) {
+        if (err && errlen > 0) std::snprintf(err, errlen, "%s", msg);
+        delete t;
+        return SMR_ERR_ARG;
+    }
+    *out = t;
+    return SMR_OK;
+}
+
+int smr_type_id(const char* name) { return name ? type_id_of(name) : -1; }
 
 void smr_topo_free(smr_topo* t) { delete t; }
 

@@ -163,6 +163,9 @@ void pack_rounds(const HostTopo& T, int team, PackedTerms& out);
 void flat_terms(const HostTopo& T, FlatTerms& out);
 bool owner_terms(const HostTopo& T, OwnerTerms& out);
 const char* type_name(int id);
+int type_id_of(const char* name);
+int build_listed_topology(int n, const int* Z, const int* type_ids, const double* q, int nb, const int* bonds, int na,
+                          const int* angs, int nd, const int* dihs, int ni, const int* invs, HostTopo& T, char* err, int errlen);
 
 // relax.cu
 enum KernelForm { FORM_ROUNDS = 0, FORM_GATHER = 1, FORM_OWNER = 2 };

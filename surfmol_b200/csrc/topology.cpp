@@ -348,6 +348,68 @@ int build_molecule_topology(int n, const int* Z, const double* pos, const double
     return 0;
 }
 
+// A molecule whose bonds and angle / dihedral / inversion lists come from a file (the reference's
+// TopologyData JSON or UFFTOPO binary, crates/libs/moltopo/src/export.rs:12-74,
+// crates/apps/buildff/src/main.rs:10-28): the lists are taken as they are, as Uff::from_topology
+// does (crates/libs/molff/src/uff.rs:238-240); atoms are typed from Z and the bond graph unless
+// type ids are given; parameters follow the same UFF rules as build_molecule_topology.
+int build_listed_topology(int n, const int* Z, const int* type_ids, const double* q, int nb, const int* bonds, int na,
+                          const int* angs, int nd, const int* dihs, int ni, const int* invs, HostTopo& T, char* err, int errlen) {
+    if (n <= 0 || n > 8191) { std::snprintf(err, errlen, "natoms=%d outside [1, 8191]", n); return -1; }
+    std::vector<El> el(n);
+    for (int a = 0; a < n; a++) {
+        el[a] = el_of_Z(Z[a]);
+        if (el[a] == EL_X || !kElem[el[a]].known) { std::snprintf(err, errlen, "atom %d: element Z=%d has no UFF parameters here", a, Z[a]); return -1; }
+    }
+    auto in_range = [&](const int* p, int m) { for (int r = 0; r < m; r++) if (p[r] < 0 || p[r] >= n) return false; return true; };
+    T = HostTopo();
+    T.n = n;
+    std::vector<int> deg(n, 0);
+    for (int b = 0; b < nb; b++) {
+        if (!in_range(bonds + 2 * b, 2) || bonds[2 * b] == bonds[2 * b + 1]) { std::snprintf(err, errlen, "bond %d: invalid atoms", b); return -1; }
+        T.bonds.push_back(bonds[2 * b]); T.bonds.push_back(bonds[2 * b + 1]);
+        deg[bonds[2 * b]]++; deg[bonds[2 * b + 1]]++;
+    }
+    for (int a = 0; a < n; a++) if (deg[a] > 4) { std::snprintf(err, errlen, "atom %d has %d bonds (max 4)", a, deg[a]); return -1; }
+    neighbour_slots(T);
+    if (type_ids) {
+        T.type_id.assign(type_ids, type_ids + n);
+        for (int a = 0; a < n; a++)
+            if (T.type_id[a] < 0 || T.type_id[a] >= kNType) { std::snprintf(err, errlen, "atom %d: unknown type id %d", a, T.type_id[a]); return -1; }
+    } else {
+        assign_types(n, el, T.neighs, T.type_id);
+    }
+    for (int t = 0; t < na; t++) {
+        const int* a = angs + 3 * t;
+        if (!in_range(a, 3)) { std::snprintf(err, errlen, "angle %d: atom index out of range", t); return -1; }
+        T.angs.insert(T.angs.end(), {a[0], a[1], a[2]});
+        T.ang_ngs.insert(T.ang_ngs.end(), {slot_of(T, a[1], a[0], 4), slot_of(T, a[1], a[2], 4)});
+    }
+    for (int t = 0; t < nd; t++) {
+        const int* q4 = dihs + 4 * t;
+        if (!in_range(q4, 4)) { std::snprintf(err, errlen, "dihedral %d: atom index out of range", t); return -1; }
+        T.dihs.insert(T.dihs.end(), {q4[0], q4[1], q4[2], q4[3]});
+        T.dih_ngs.insert(T.dih_ngs.end(), {slot_of(T, q4[1], q4[0], 4), slot_of(T, q4[1], q4[2], 4), slot_of(T, q4[2], q4[3], 4)});
+        T.dih_kj.push_back(slot_of(T, q4[2], q4[1], 4));
+    }
+    for (int t = 0; t < ni; t++) {
+        const int* q4 = invs + 4 * t;
+        if (!in_range(q4, 4)) { std::snprintf(err, errlen, "inversion %d: atom index out of range", t); return -1; }
+        T.invs.insert(T.invs.end(), {q4[0], q4[1], q4[2], q4[3]});
+        T.inv_ngs.insert(T.inv_ngs.end(), {slot_of(T, q4[0], q4[1], 3), slot_of(T, q4[0], q4[2], 3), slot_of(T, q4[0], q4[3], 3)});
+    }
+    if (!check_slots(T, err, errlen)) return -1;
+    uff_parameters(T);
+    if (q) for (int a = 0; a < n; a++) T.req[4 * a + 2] = q[a];
+    fill_bond_kl(T);
+    return 0;
+}
+
+int type_id_of(const char* name) {
+    for (int t = 0; t < kNType; t++) if (std::strcmp(kType[t].name, name) == 0) return t;
+    return -1;
+}
+
 int build_desc_topology(int natoms, const double* req, const int* neighs, const double* bond_kl,
                         int nang, const int* angs, const double* angp, int ndih, const int* dihs, const double* dihp,
                         int ninv, const int* invs, const double* invp, HostTopo& T, char* err, int errlen) {

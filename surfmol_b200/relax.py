@@ -108,6 +108,33 @@ class Topology:
         except Exception:
             pass
 
+    @classmethod
+    def from_lists(cls, Z, bonds, angles, dihedrals, inversions, charges=None, types=None):
+        """Host topology from explicit bond / term lists (a topology file): lists used as given;
+        types: UFF type names (None: typed from Z and the bond graph)."""
+        L = N.lib()
+        Z = _i(Z)
+        b, a, d, v = (_i(np.asarray(x).reshape(-1, w)) for x, w in ((bonds, 2), (angles, 3), (dihedrals, 4), (inversions, 4)))
+        tid = None
+        if types is not None:
+            tid = _i([L.smr_type_id(t.encode()) for t in types])
+            if (tid < 0).any():
+                raise SmrError(f"unknown UFF type {types[int(np.argmin(tid))]!r}")
+        q = _d(charges) if charges is not None else None
+        h = N.VP()
+        err = C.create_string_buffer(300)
+        r_ = L.smr_topo_build_listed(len(Z), _p(Z, N.IP), _p(tid, N.IP), _p(q, N.DP), len(b), _p(b, N.IP), len(a), _p(a, N.IP),
+                                     len(d), _p(d, N.IP), len(v), _p(v, N.IP), C.byref(h), err, 300)
+        if r_ != 0:
+            raise SmrError(f"smr_topo_build_listed: {err.value.decode()}")
+        t = cls.__new__(cls)
+        t.h = h
+        c = (C.c_int * 5)()
+        L.smr_topo_counts(t.h, c)
+        t.counts = list(c)
+        t.n = t.counts[0]
+        return t
+
     def export(self):
         out = _export_arrays(self.counts)
         N.lib().smr_topo_export(self.h, *_export_ptrs(out))
@@ -287,6 +314,31 @@ class RelaxMulti:
                                            _p(ids, N.IP)), "smr_add_molecules")
         self.topo_n.extend(int(k) for k in n)
         return ids
+
+    def add_listed_molecule(self, Z, bonds, angles, dihedrals, inversions, charges=None, types=None) -> int:
+        """A molecule from explicit bond / term lists (a topology file); see topo_io."""
+        Z = _i(Z)
+        b, a, d, v = (_i(np.asarray(x).reshape(-1, w)) for x, w in ((bonds, 2), (angles, 3), (dihedrals, 4), (inversions, 4)))
+        tid = None
+        if types is not None:
+            tid = _i([self.L.smr_type_id(t.encode()) for t in types])
+            if (tid < 0).any():
+                raise SmrError(f"unknown UFF type {types[int(np.argmin(tid))]!r}")
+        q = _d(charges) if charges is not None else None
+        out = C.c_int()
+        self._chk(self.L.smr_add_listed_molecule(self.h, len(Z), _p(Z, N.IP), _p(tid, N.IP), _p(q, N.DP), len(b), _p(b, N.IP),
+                                                 len(a), _p(a, N.IP), len(d), _p(d, N.IP), len(v), _p(v, N.IP), C.byref(out)),
+                  "smr_add_listed_molecule")
+        self.topo_n.append(len(Z))
+        return out.value
+
+    def add_topology_file(self, path, charges=None):
+        """Add the molecule of a TopologyData JSON or UFFTOPO file; returns (topology id, positions)."""
+        from .topo_io import read
+        d = read(path)
+        tid = self.add_listed_molecule(d["Z"], d["bonds"], d["angles"], d["dihedrals"], d["inversions"], charges,
+                                       d["types"])
+        return tid, d["positions"]
 
     def add_topo(self, topo: Topology) -> int:
         tid = C.c_int()

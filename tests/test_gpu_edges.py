@@ -183,3 +183,22 @@ def test_watchdog_timeout_and_recovery():
     a, b = outs
     assert np.array_equal(a["steps"], b["steps"]) and np.array_equal(a["status"], b["status"])
     assert all(np.array_equal(x, y) for x, y in zip(a["pos"], b["pos"]))
+
+
+def test_topology_file_relaxes_like_pipeline(env, tmp_path):
+    """A molecule loaded from a UFFTOPO file relaxes bit for bit like the same molecule added from
+    elements and positions (same lists, types and parameters)."""
+    from surfmol_b200.relax import Topology
+    from surfmol_b200.topo_io import write_ufftopo
+    R, slab, _ = env
+    rng = np.random.default_rng(8)
+    Z, P, q = molecule_on_slab(rng, 60, slab)
+    ref = Topology(Z, P, q).export()
+    write_ufftopo(tmp_path / "m.bin", ref["types"], P, ref["bonds"], ref["angs"], ref["dihs"], ref["invs"])
+    t1 = R.add_molecule(Z, P, q)
+    t2, P2 = R.add_topology_file(tmp_path / "m.bin", charges=q)
+    s = R.add_systems([t1, t2], [P, P2])
+    R.run_fire(200, step_budget=200, fconv=1e-6)
+    out = R.download(s)
+    assert np.array_equal(out["pos"][0], out["pos"][1]) and out["steps"][0] == out["steps"][1] == 200
+    R.remove_systems(s)
