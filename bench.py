@@ -137,10 +137,20 @@ def make_workload(seed, nsys):
     return synth.config1(seed, nsys)
 
 
-def workload_desc(w, nsys):
+def workload_desc(w, nsys, substrate="grid"):
     g = w.grid
+    if substrate == "folded":
+        return (f"config1 on the folded surface: {nsys} replicas of a 40-atom polyaromatic (24 C, 12 H, 2 N, 2 O) "
+                f"over the NaCl-like SurfaceFolded basis (2x2 harmonics x 3 z decays, a=5.66 A, plane at the slab top), "
+                f"forces clamped at 100 eV/A; FIRE to max|F|<1e-3 or {MAX_STEPS} steps")
     return (f"config1: {nsys} replicas of a 40-atom polyaromatic (24 C, 12 H, 2 N, 2 O) over NaCl(100) "
             f"2 layers 4x4 cells, fp32 B-spline grid {g.nx}x{g.ny}x{g.nz} at 0.1 A; FIRE to max|F|<1e-3 or {MAX_STEPS} steps")
+
+
+def folded_surface(slab):
+    """The NaCl-like folded surface of the reference's editor, its plane at the slab's top layer."""
+    from surfmol_b200.folded import nacl
+    return nacl(z0=slab.z_top)
 
 
 # ---------------------------------------------------------------------------------------- reference arm
@@ -151,9 +161,12 @@ def run_reference(args, ws, rank):
     w = make_workload(SEED, args.nsys)
     slab, g = w.slab, w.grid
     t0 = time.perf_counter()
-    coef = O.build_grid_fast(slab.ions, slab.req(), slab.Lx, slab.Ly, g.nx, g.ny, g.nz, g.p0, g.step)
+    if args.substrate == "folded":
+        grid = O.Folded(**folded_surface(slab).as_dict())
+    else:
+        coef = O.build_grid_fast(slab.ions, slab.req(), slab.Lx, slab.Ly, g.nx, g.ny, g.nz, g.p0, g.step)
+        grid = O.Grid(coef.astype(np.float32), g.p0, g.step)
     tgrid = time.perf_counter() - t0
-    grid = O.Grid(coef.astype(np.float32), g.p0, g.step)
     sys0 = O.System.from_molecule(w.Z[0], w.pos[0], w.q[0])
     threads = os.cpu_count() or 1
     sample = max(threads, args.ref_sample)
@@ -177,7 +190,7 @@ def run_reference(args, ws, rank):
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "systems/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * tt / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": workload_desc(w, args.nsys), "sample_per_step": sample,
+            "config": {"workload": workload_desc(w, args.nsys, args.substrate), "sample_per_step": sample,
                        "grid_build_s": round(tgrid, 2), "converged_fraction": conv / (sample * args.steps),
                        "fire_steps_p50": float(np.percentile(steps, 50)), "fire_steps_p99": float(np.percentile(steps, 99))},
             "cpu_baseline": {"value": v, "unit": "systems/s", "cores": threads, "kind": "port",
@@ -189,9 +202,9 @@ def run_reference(args, ws, rank):
 
 
 # ---------------------------------------------------------------------------------------- our arm
-def cpu_baseline(w, coef, p0, step, budget_s=15.0):
+def cpu_baseline(w, grid, budget_s=15.0):
+    """grid: the oracle's substrate (oracle.Grid or oracle.Folded)."""
     from oracle import oracle as O
-    grid = O.Grid(coef, p0, step)
     sys0 = O.System.from_molecule(w.Z[0], w.pos[0], w.q[0])
     threads = os.cpu_count() or 1
     chunk = max(threads, 16)
@@ -220,7 +233,10 @@ def run_ours(args, ws, rank, local):
     R = RelaxMulti(max_systems=args.nsys, max_atoms=natoms, device=dev)
     R.set_nb(rdamp=1.0, alpha_morse=1.5)
     t0 = time.perf_counter()
-    R.build_grid(slab.ions, slab.req()[:, :2], slab.Lx, slab.Ly, g.nx, g.ny, g.nz, g.p0, g.step, alpha_morse=1.5, npbc=1)
+    if args.substrate == "folded":
+        R.set_surface_folded(folded_surface(slab))
+    else:
+        R.build_grid(slab.ions, slab.req()[:, :2], slab.Lx, slab.Ly, g.nx, g.ny, g.nz, g.p0, g.step, alpha_morse=1.5, npbc=1)
     torch.cuda.synchronize()
     tgrid = time.perf_counter() - t0
     tid = R.add_molecule(w.Z[0], w.pos[0], w.q[0])
@@ -297,7 +313,7 @@ def run_ours(args, ws, rank, local):
     line = {"metric": METRIC, "value": value, "unit": "systems/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": workload_desc(w, args.nsys), "nsys_per_gpu": args.nsys, "atoms_per_system": 40,
+            "config": {"workload": workload_desc(w, args.nsys, args.substrate), "nsys_per_gpu": args.nsys, "atoms_per_system": 40,
                        "parallelism": f"systems sharded over {ws} GPU(s), no collective",
                        "l2": "flushed (256 MB write) before every timed step", "grid_build_s": round(tgrid, 3),
                        "converged_fraction": conv / (args.nsys * args.steps),
@@ -308,9 +324,19 @@ def run_ours(args, ws, rank, local):
                          "traffic": traffic, "peak_source": peak_kind,
                          "algorithmic_bytes": "1024 B per atom-step (64 float4 grid voxels), state resident in shared memory"},
             "e2e": e2e, "gpu_launches": launches, "clocks": clocks}
+    if args.substrate == "folded":
+        # no grid stream: the basis (12 float4 coefficients) stays in L1; the kernel is bound by
+        # its FP32 / SFU issue rate, which the ncu summary of this workload shows
+        line["roofline"] = None
+        line["roofline_note"] = "folded surface: no HBM stream to bound the kernel (basis in L1); issue-bound"
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        gd = R.get_grid()
-        line["cpu_baseline"] = cpu_baseline(w, gd["coef"], gd["p0"], gd["step"], budget_s=args.cpu_budget)
+        from oracle import oracle as O
+        if args.substrate == "folded":
+            og = O.Folded(**folded_surface(slab).as_dict())
+        else:
+            gd = R.get_grid()
+            og = O.Grid(gd["coef"], gd["p0"], gd["step"])
+        line["cpu_baseline"] = cpu_baseline(w, og, budget_s=args.cpu_budget)
     R.finish()
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -642,6 +668,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="uniform", choices=["uniform", "ragged", "serve", "precision"],
                     help="uniform: 4096 replicas of the 40-atom molecule (default); ragged: 16384 molecules of 20-400 atoms")
+    ap.add_argument("--substrate", default="grid", choices=["grid", "folded"],
+                    help="uniform workload: B-spline grid (default) or the reference's folded surface")
     ap.add_argument("--nsys", type=int, default=0, help="systems per GPU (0: the workload's default)")
     ap.add_argument("--no-tune", action="store_true", help="ragged: skip the autotuner (library defaults)")
     ap.add_argument("--resident", type=int, default=0, help="serve: cap on resident systems (0: the handle's slots)")

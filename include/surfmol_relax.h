@@ -130,6 +130,25 @@ int smr_get_grid(smr_handle* h, void* coef_out, int* dtype, float scale[4], int 
 int smr_set_grid_planes(smr_handle* h, const void* coef, int dtype, const float* plane_scale, int nx, int ny, int nz,
                         const double p0[3], const double step[3]);
 int smr_get_grid_planes(smr_handle* h, float* plane_scale);
+/* Folded-surface substrate, the reference's SurfaceFolded (crates/libs/surfff/src/lib.rs:126-351)
+ * as MolWorld::eval_forces applies it (crates/libs/surfmol/src/mol_world.rs:80-83).  While set it
+ * replaces the grid for every system: each atom gets
+ *   E = sum_b (cq[b] Q + cp[b] P + cl[b] L) cos(2 pi kx[ix] u) cos(2 pi ky[iy] v) exp(-kz[iz] (z - z0[iz]))
+ * over the basis b = ix + nx (iy + ny iz), (u, v) its fractional coordinates in the lattice
+ * a = (ax, ay), b = (bx, by), and the atom's P = e L, L = e sqrt(req1), e = exp(-alpha R)
+ * (NonBondedFF::make_plqs, req1 = sqrt(E_vdW) as the reference stores it); the force is clamped
+ * to fmax per atom (eval_all_clamped; the reference passes 100 eV/A).  One coefficient set for all
+ * atoms (the reference evaluates type 0 only).  Arrays are copied; evaluation is FP32.
+ * smr_set_surface_folded(h, NULL) returns to the grid.  1 <= nx, ny, nz <= 64. */
+typedef struct {
+    double ax, bx, ay, by;
+    int nx, ny, nz;
+    const double *kx, *ky, *kz, *z0;      /* nx, ny, nz, nz */
+    const double *cq, *cp, *cl;           /* nx * ny * nz each */
+    double alpha;                         /* make_plqs exponent (the reference uses 2.0) */
+    double fmax;                          /* per-atom force clamp */
+} smr_folded_surface;
+int smr_set_surface_folded(smr_handle* h, const smr_folded_surface* f);
 /* Build on the device from ions (x, y, z, q) and their Morse (R, sqrt(E)); the slab is periodic
  * in an orthogonal Lx x Ly cell and lies entirely below p0[2]. */
 int smr_build_grid(smr_handle* h, int nions, const double* ions, const double* ion_re, double Lx, double Ly,

@@ -194,12 +194,25 @@ struct orc_sys {
     std::vector<int> type_id;
 };
 
+// Folded surface (crates/libs/surfff/src/lib.rs:126-351, SurfaceFolded): separable basis of
+// lattice harmonics cos(2 pi k u), cos(2 pi k v) and z decays exp(-kz (z - z0)), one coefficient
+// per basis function and channel (charge, Pauli, London), basis index ix + nx (iy + ny iz).
+struct orc_folded {
+    double inv[4];          // inv_ax, inv_bx, inv_ay, inv_by (inverse of the 2D lattice)
+    int nx, ny, nz;
+    const double *kx, *ky, *kz, *z0;
+    const double *cq, *cp, *cl;
+    double alpha;           // make_plqs exponent (molengine uses 2.0)
+    double fmax;            // per-atom force clamp of eval_all_clamped (mol_world.rs:82: 100 eV/A)
+};
+
 struct orc_grid {
     int nx, ny, nz;
     double p0[3], step[3];
     const float* cf32;      // z-fastest (nx*ny*nz*4) float B-spline coefficients, or
     const double* cf64;     // the same in double (exactly one is non-null)
     double scale[4];        // per-channel scale folded into the atom prefactor (1 for fp32/f64 data)
+    const orc_folded* folded;   // non-null: the substrate is this folded surface, not the grid
 };
 
 namespace {
@@ -395,6 +408,38 @@ inline void dbasis(double u, double d[4]) {   // UFF.cl:1422-1432
 inline int modulo(int i, int m) { int r = i % m; if (r < 0) r += m; return r; }
 
 // fe3d_pbc_comb (UFF.cl:1459-1511): returns (dE/du_x, dE/du_y, dE/du_z, E) in grid units.
+// One atom on the folded surface: energy and force (surfff/src/lib.rs:277-320), force clamped to
+// fmax as eval_all_clamped does (lib.rs:245-253, 340-351).  plq as NonBondedFF::make_plqs
+// (molff/src/nonbonded.rs:98-108): e = exp(-alpha R), L = e sqrt(req[1]), P = e L, with req[1]
+// holding sqrt(E_vdW) (moltopo/src/params.rs:595-597), so L carries E_vdW^(1/4) as the code does.
+double folded_atom(const orc_folded& f, const double req[4], V3 p, V3& force) {
+    const double e = std::exp(-f.alpha * req[0]);
+    const double L = e * std::sqrt(req[1]), P = e * L, Q = req[2];
+    double u = f.inv[0] * p.x + f.inv[2] * p.y, v = f.inv[1] * p.x + f.inv[3] * p.y;
+    u -= std::floor(u); v -= std::floor(v);
+    const double tau = 2.0 * 3.14159265358979323846;
+    double E = 0, dEdu = 0, dEdv = 0, dEdz = 0;
+    int ic = 0;
+    for (int iz = 0; iz < f.nz; iz++) {
+        const double bz = std::exp(-f.kz[iz] * (p.z - f.z0[iz])), dbz = -f.kz[iz] * bz;
+        for (int iy = 0; iy < f.ny; iy++) {
+            const double by = std::cos(tau * f.ky[iy] * v), dby = -tau * f.ky[iy] * std::sin(tau * f.ky[iy] * v);
+            for (int ix = 0; ix < f.nx; ix++, ic++) {
+                const double bx = std::cos(tau * f.kx[ix] * u), dbx = -tau * f.kx[ix] * std::sin(tau * f.kx[ix] * u);
+                const double c = f.cq[ic] * Q + f.cp[ic] * P + f.cl[ic] * L;
+                E += c * bx * by * bz;
+                dEdu += c * dbx * by * bz;
+                dEdv += c * bx * dby * bz;
+                dEdz += c * bx * by * dbz;
+            }
+        }
+    }
+    force = {-(dEdu * f.inv[0] + dEdv * f.inv[1]), -(dEdu * f.inv[2] + dEdv * f.inv[3]), -dEdz};
+    const double f2 = dot(force, force);
+    if (f2 > f.fmax * f.fmax) force = force * (f.fmax / std::sqrt(f2));
+    return E;
+}
+
 void sample_grid(const orc_grid& g, const double PLQH[4], V3 u, double out[4]) {
     int ix = (int)u.x, iy = (int)u.y, iz = (int)u.z;
     if (u.x < 0) ix--;
@@ -558,7 +603,13 @@ void eval_forces(const orc_sys& S, const V3* P, const orc_grid* g, const NBParam
             fe = fe + f;
         }
         enb += 0.5 * E;
-        if (g) {
+        if (g && g->folded) {
+            V3 fs;
+            const double E1 = folded_atom(*g->folded, ri.data(), P[a], fs);
+            fe = fe + fs;
+            E += E1;
+            eg += E1;
+        } else if (g) {
             double ej = std::exp(nb.alpha * ri[0]);
             double PLQH[4] = {ej * ej * ri[1], ej * ri[1], ri[2], 0.0};
             V3 u = {(P[a].x - g->p0[0]) / g->step[0], (P[a].y - g->p0[1]) / g->step[1], (P[a].z - g->p0[2]) / g->step[2]};
@@ -801,6 +852,16 @@ const char* orc_type_name(int id) { return (id >= 0 && id < N_ATYPES) ? ATYPES[i
 static NBParams nbp_of(const double* p) { return NBParams{p[0], p[1], p[2], (int)p[3]}; }
 // fp = (dt0, dt_max, alpha0, f_inc, f_dec, f_alpha, n_min, fconv, flimit)
 static FireParams fp_of(const double* p) { return FireParams{p[0], p[1], p[2], p[3], p[4], p[5], (int)p[6], p[7], p[8]}; }
+
+// Folded-surface energy and (clamped) force of isolated atoms: n x (x, y, z), n x req -> E[n], F[n x 3]
+int orc_folded_points(const orc_folded* f, int n, const double* pos, const double* req, double* E, double* F) {
+    for (int a = 0; a < n; a++) {
+        V3 fo;
+        E[a] = folded_atom(*f, req + 4 * a, V3{pos[3 * a], pos[3 * a + 1], pos[3 * a + 2]}, fo);
+        F[3 * a] = fo.x; F[3 * a + 1] = fo.y; F[3 * a + 2] = fo.z;
+    }
+    return 0;
+}
 
 int orc_eval(const orc_sys* S, const double* pos, const orc_grid* g, const double* nbp, double* F, double* Ea, double* Ec) {
     std::vector<V3> P(S->n), FF(S->n);

@@ -19,10 +19,17 @@ DP = C.POINTER(C.c_double)
 IP = C.POINTER(C.c_int)
 
 
+class OrcFolded(C.Structure):
+    _fields_ = [("inv", C.c_double * 4), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                ("kx", DP), ("ky", DP), ("kz", DP), ("z0", DP), ("cq", DP), ("cp", DP), ("cl", DP),
+                ("alpha", C.c_double), ("fmax", C.c_double)]
+
+
 class OrcGrid(C.Structure):
     _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
                 ("p0", C.c_double * 3), ("step", C.c_double * 3),
-                ("cf32", C.POINTER(C.c_float)), ("cf64", DP), ("scale", C.c_double * 4)]
+                ("cf32", C.POINTER(C.c_float)), ("cf64", DP), ("scale", C.c_double * 4),
+                ("folded", C.POINTER(OrcFolded))]
 
 
 def build() -> str:
@@ -47,6 +54,7 @@ def lib():
         L.orc_type_name.restype = C.c_char_p
         L.orc_type_name.argtypes = [C.c_int]
         L.orc_eval.argtypes = [C.c_void_p, DP, C.POINTER(OrcGrid), DP, DP, DP, DP]
+        L.orc_folded_points.argtypes = [C.POINTER(OrcFolded), C.c_int, DP, DP, DP, DP]
         L.orc_relax.restype = C.c_int
         L.orc_relax.argtypes = [C.c_void_p, DP, C.POINTER(OrcGrid), DP, DP, C.c_int, DP, DP, DP, DP, IP]
         L.orc_relax_batch.argtypes = [C.c_int, C.POINTER(C.c_void_p), C.POINTER(DP), C.POINTER(OrcGrid), DP, DP,
@@ -128,6 +136,44 @@ class Grid:
 
     def ptr(self):
         return C.byref(self.s)
+
+
+class Folded:
+    """Oracle view of a folded surface (SurfaceFolded, crates/libs/surfff/src/lib.rs:126-351):
+    lattice (ax, bx, ay, by), harmonics kx, ky, z decays kz, z0, coefficients cq / cp / cl of
+    length nx*ny*nz (index ix + nx*(iy + ny*iz)), make_plqs exponent alpha, force clamp fmax.
+    Passed where a Grid goes (System.eval / relax / relax_batch)."""
+
+    def __init__(self, ax, bx, ay, by, kx, ky, kz, z0, cq, cp, cl, alpha=2.0, fmax=100.0):
+        det = ax * by - bx * ay
+        if abs(det) < 1e-12:
+            raise ValueError("degenerate 2D lattice")
+        self.arrs = [_d(x) for x in (kx, ky, kz, z0, cq, cp, cl)]
+        kx, ky, kz, z0, cq, cp, cl = self.arrs
+        nb = len(kx) * len(ky) * len(kz)
+        if len(z0) != len(kz) or not (len(cq) == len(cp) == len(cl) == nb):
+            raise ValueError("folded surface arrays do not match nx*ny*nz")
+        self.f = OrcFolded()
+        idet = 1.0 / det
+        for k, v in enumerate((by * idet, -bx * idet, -ay * idet, ax * idet)):
+            self.f.inv[k] = v
+        self.f.nx, self.f.ny, self.f.nz = len(kx), len(ky), len(kz)
+        for name, a in zip(("kx", "ky", "kz", "z0", "cq", "cp", "cl"), self.arrs):
+            setattr(self.f, name, a.ctypes.data_as(DP))
+        self.f.alpha, self.f.fmax = float(alpha), float(fmax)
+        self.s = OrcGrid()
+        self.s.folded = C.pointer(self.f)
+
+    def ptr(self):
+        return C.byref(self.s)
+
+    def points(self, pos, req):
+        """Energy and clamped force of isolated atoms at pos (n, 3) with req (n, 4) = (R, sqrt E, Q, H)."""
+        pos, req = _d(pos).reshape(-1, 3), _d(req).reshape(-1, 4)
+        E = np.zeros(len(pos))
+        F = np.zeros((len(pos), 3))
+        lib().orc_folded_points(C.byref(self.f), len(pos), _dp(pos), _dp(req), _dp(E), _dp(F))
+        return E, F
 
 
 class System:

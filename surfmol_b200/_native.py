@@ -34,6 +34,13 @@ class SmrNbParams(C.Structure):
     _fields_ = [("rdamp", C.c_float), ("alpha_morse", C.c_float), ("rcut", C.c_float), ("reserved", C.c_int)]
 
 
+class SmrFoldedSurface(C.Structure):
+    _fields_ = [("ax", C.c_double), ("bx", C.c_double), ("ay", C.c_double), ("by", C.c_double),
+                ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                ("kx", DP), ("ky", DP), ("kz", DP), ("z0", DP), ("cq", DP), ("cp", DP), ("cl", DP),
+                ("alpha", C.c_double), ("fmax", C.c_double)]
+
+
 class SmrGridBuildParams(C.Structure):
     _fields_ = [("alpha_morse", C.c_double), ("npbc", C.c_int), ("ewald_tol", C.c_double), ("dtype", C.c_int),
                 ("morse_rcut", C.c_double), ("reserved", C.c_int * 4)]
@@ -62,6 +69,7 @@ SIGNATURES = {
     "smr_get_grid": (C.c_int, [VP, VP, IP, FP, IP, DP, DP]),
     "smr_set_grid_planes": (C.c_int, [VP, VP, C.c_int, FP, C.c_int, C.c_int, C.c_int, DP, DP]),
     "smr_get_grid_planes": (C.c_int, [VP, FP]),
+    "smr_set_surface_folded": (C.c_int, [VP, VP]),
     "smr_build_grid": (C.c_int, [VP, C.c_int, DP, DP, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, DP, DP,
                                  C.POINTER(SmrGridBuildParams)]),
     "smr_convert_grid": (C.c_int, [VP, C.c_int]),

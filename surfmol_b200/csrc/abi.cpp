@@ -129,6 +129,13 @@ struct smr_handle {
     std::vector<float> gzscale;         // 16-bit grids: nz x 4 per-plane channel scales (empty: gscale)
     DArr<float4> dzscale;
     bool has_grid = false;
+    // folded surface: while set it is the substrate in place of the grid
+    bool fold_on = false;
+    int fold_n[3] = {0, 0, 0};
+    float fold_inv[4] = {0, 0, 0, 0};
+    float fold_alpha = 2.f, fold_fmax = 100.f;
+    DArr<float> dfold_k;                // kx, ky, kz, z0
+    DArr<float4> dfold_coef;            // (cq, cp, cl, 0) per basis function
 
     smr_nb_params nb{1.0f, 1.5f, 0.0f, 0};
 
@@ -431,6 +438,13 @@ KernelArgs base_args(smr_handle* h) {
     for (int k = 0; k < 4; k++) a.grid.scale[k] = h->has_grid ? h->gscale[k] : 1.f;
     a.grid.zscale = (h->has_grid && !h->gzscale.empty()) ? h->dzscale.d : nullptr;
     a.grid.p0z = h->gp0[2]; a.grid.stepz = h->gstep[2];
+    if (h->fold_on) {
+        a.fold.on = 1;
+        a.fold.nx = h->fold_n[0]; a.fold.ny = h->fold_n[1]; a.fold.nz = h->fold_n[2];
+        for (int k = 0; k < 4; k++) a.fold.inv[k] = h->fold_inv[k];
+        a.fold.alpha = h->fold_alpha; a.fold.fmax = h->fold_fmax;
+        a.fold.k = h->dfold_k.d; a.fold.coef = h->dfold_coef.d;
+    }
     a.R2damp = h->nb.rdamp * h->nb.rdamp;
     a.alpha_morse = h->nb.alpha_morse;
     a.rc2 = h->nb.rcut > 0 ? h->nb.rcut * h->nb.rcut : 3.0e38f;
@@ -678,6 +692,39 @@ static int set_plane_scales(smr_handle* h, const float* ps, int nz) {
         for (int z = 0; z < nz; z++) m = std::max(m, h->gzscale[4 * (size_t)z + c]);
         h->gscale[c] = m;
     }
+    return SMR_OK;
+}
+
+int smr_set_surface_folded(smr_handle* h, const smr_folded_surface* f) {
+    if (!h) return SMR_ERR_ARG;
+    SETTLE(h);
+    if (!f) { h->fold_on = false; return SMR_OK; }
+    if (f->nx < 1 || f->ny < 1 || f->nz < 1 || f->nx > 64 || f->ny > 64 || f->nz > 64)
+        return fail(h, SMR_ERR_ARG, "folded surface: nx, ny, nz must be 1..64 (got %d, %d, %d)", f->nx, f->ny, f->nz);
+    if (!f->kx || !f->ky || !f->kz || !f->z0 || !f->cq || !f->cp || !f->cl) return fail(h, SMR_ERR_ARG, "folded surface: null array");
+    const double det = f->ax * f->by - f->bx * f->ay;
+    if (!(std::fabs(det) > 1e-12)) return fail(h, SMR_ERR_ARG, "folded surface: degenerate 2D lattice");
+    if (!(f->fmax > 0) || !std::isfinite(f->alpha)) return fail(h, SMR_ERR_ARG, "folded surface: fmax must be positive, alpha finite");
+    const int nx = f->nx, ny = f->ny, nz = f->nz, nb = nx * ny * nz;
+    std::vector<float> k;
+    for (int i = 0; i < nx; i++) k.push_back((float)f->kx[i]);
+    for (int i = 0; i < ny; i++) k.push_back((float)f->ky[i]);
+    for (int i = 0; i < nz; i++) k.push_back((float)f->kz[i]);
+    for (int i = 0; i < nz; i++) k.push_back((float)f->z0[i]);
+    std::vector<float4> c(nb);
+    for (int i = 0; i < nb; i++) c[i] = make_float4((float)f->cq[i], (float)f->cp[i], (float)f->cl[i], 0.f);
+    cudaError_t e = h->dfold_k.reserve(k.size(), 0, h->stream);
+    if (e == cudaSuccess) e = h->dfold_coef.reserve((size_t)nb, 0, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h->dfold_k.d, k.data(), k.size() * 4, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h->dfold_coef.d, c.data(), (size_t)nb * 16, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);      // the host vectors are freed on return
+    if (e != cudaSuccess) { h->fold_on = false; return fail(h, SMR_ERR_CUDA, "folded surface upload: %s", cudaGetErrorString(e)); }
+    h->fold_n[0] = nx; h->fold_n[1] = ny; h->fold_n[2] = nz;
+    const double idet = 1.0 / det;
+    h->fold_inv[0] = (float)(f->by * idet); h->fold_inv[1] = (float)(-f->bx * idet);
+    h->fold_inv[2] = (float)(-f->ay * idet); h->fold_inv[3] = (float)(f->ax * idet);
+    h->fold_alpha = (float)f->alpha; h->fold_fmax = (float)f->fmax;
+    h->fold_on = true;
     return SMR_OK;
 }
 
@@ -1161,6 +1208,10 @@ static void sig_args(std::vector<long long>& v, const KernelArgs& a) {
     v.push_back(a.phase_limit); v.push_back(a.step_budget); P(a.ecomp); v.push_back(a.nmax); v.push_back(a.nfmax);
     P(a.a2f); P(a.a2f_idx); P(a.own_geo); P(a.own_par); P(a.own_meta); v.push_back(a.nb_lanes);
     P(a.gscratch); v.push_back((long long)a.gscratch_bytes);
+    P(a.nbl); P(a.nbl_cnt); P(a.nbl_ref); v.push_back(a.nbl_cap); v.push_back(a.nbl_min); F(a.nbl_skin);
+    v.push_back(a.fold.on); v.push_back(a.fold.nx); v.push_back(a.fold.ny); v.push_back(a.fold.nz);
+    for (int k = 0; k < 4; k++) F(a.fold.inv[k]);
+    F(a.fold.alpha); F(a.fold.fmax); P(a.fold.k); P(a.fold.coef);
 }
 
 int smr_set_graph(smr_handle* h, int on) {

@@ -197,6 +197,45 @@ __device__ __noinline__ int grid_cell_z_fp64(float pz, float lz, const GridView&
     return (int)((((double)pz + (double)lz) - g.p0z) / g.stepz);
 }
 
+// Folded surface, one lane's share of an atom: the z-decay terms iz = lane, lane + 4, ... of
+// SurfaceFolded::eval_atom_scratch (crates/libs/surfff/src/lib.rs:277-320) with the atom's
+// prefactors of NonBondedFF::make_plqs (crates/libs/molff/src/nonbonded.rs:98-108: e = exp(-alpha R),
+// L = e sqrt(req1), P = e L).  Returns E and dE/du, dE/dv, dE/dz.  Not inlined: its registers stay
+// out of the kernels' other phases.
+__device__ __noinline__ float4 folded_part(const FoldedView f, float4 p, float4 lo, float4 q, int lane) {
+    const float e = expf(-f.alpha * q.x);
+    const float L = e * sqrtf(q.y), P = e * L, Q = q.z;
+    const float x = p.x + lo.x, y = p.y + lo.y, z = p.z + lo.z;
+    float u = f.inv[0] * x + f.inv[2] * y, v = f.inv[1] * x + f.inv[3] * y;
+    u -= floorf(u); v -= floorf(v);
+    const float* kx = f.k;
+    const float* ky = kx + f.nx;
+    const float* kz = ky + f.ny;
+    const float* z0 = kz + f.nz;
+    const float tau = 6.28318530717958647692f;
+    float E = 0.f, du = 0.f, dv = 0.f, dz = 0.f;
+    for (int iz = lane; iz < f.nz; iz += 4) {
+        const float bz = expf(-__ldg(kz + iz) * (z - __ldg(z0 + iz))), dbz = -__ldg(kz + iz) * bz;
+        for (int iy = 0; iy < f.ny; iy++) {
+            float sy, cy;
+            sincospif(2.0f * __ldg(ky + iy) * v, &sy, &cy);
+            const float dby = -tau * __ldg(ky + iy) * sy;
+            for (int ix = 0; ix < f.nx; ix++) {
+                float sx, cx;
+                sincospif(2.0f * __ldg(kx + ix) * u, &sx, &cx);
+                const float dbx = -tau * __ldg(kx + ix) * sx;
+                const float4 c4 = __ldg(f.coef + ix + f.nx * (iy + f.ny * iz));
+                const float c = c4.x * Q + c4.y * P + c4.z * L;
+                E += c * cx * cy * bz;
+                du += c * dbx * cy * bz;
+                dv += c * cx * dby * bz;
+                dz += c * cx * cy * dbz;
+            }
+        }
+    }
+    return make_float4(E, du, dv, dz);
+}
+
 // One LJ + damped-Coulomb pair (getLJQH, opencl/UFF.cl:82-95) added to the force / energy of atom i;
 // excluded pairs and pairs beyond the cutoff are evaluated at r^2 = 1 and weighted 0.
 template <bool CUT>
@@ -607,9 +646,30 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
     }
     team_sync<T>();
 
+    // D': folded surface instead of the grid, 4 lanes per atom splitting the z-decay terms
+    if (a.fold.on) {
+        const FoldedView& f = a.fold;
+        const int lane = rank & 3;
+        for (int i0 = 0; i0 < N; i0 += T / 4) {
+            const int i = i0 + (rank >> 2);
+            float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (i < N) r = folded_part(f, S.P()[i], S.Lo()[i], S.Q()[i], lane);
+            for (int o = 1; o < 4; o <<= 1) {
+                r.x += __shfl_xor_sync(FULL, r.x, o); r.y += __shfl_xor_sync(FULL, r.y, o);
+                r.z += __shfl_xor_sync(FULL, r.z, o); r.w += __shfl_xor_sync(FULL, r.w, o);
+            }
+            if (lane == 0 && i < N) {
+                float fx = -(r.y * f.inv[0] + r.z * f.inv[1]), fy = -(r.y * f.inv[2] + r.z * f.inv[3]), fz = -r.w;
+                const float f2 = fx * fx + fy * fy + fz * fz;
+                if (f2 > f.fmax * f.fmax) { const float sc = f.fmax / sqrtf(f2); fx *= sc; fy *= sc; fz *= sc; }   // eval_all_clamped
+                add4(S.F()[i], fx, fy, fz, r.x);
+                acc.add(5, (double)r.x);
+            }
+        }
+    }
     // D: substrate grid, 4 lanes per atom; lane kz reads the voxels at z offset kz of the 16 (x, y)
     // columns of the stencil, so the 4 lanes of an atom read each column as one 64 B run
-    if (a.has_grid) {
+    else if (a.has_grid) {
         const GridView& g = a.grid;
         const int kz = rank & 3;
         for (int i0 = 0; i0 < N; i0 += T / 4) {
@@ -964,7 +1024,7 @@ int launch_team(const KernelArgs& a, int team, cudaStream_t s, int num_sms) {
 
 template <bool EVAL, int FORM>
 int launch_dtype(const KernelArgs& a, int team, cudaStream_t s, int num_sms) {
-    const int gdt = a.has_grid ? a.grid.dtype : GRID_F32;
+    const int gdt = a.has_grid && !a.fold.on ? a.grid.dtype : GRID_F32;
     if (gdt == GRID_F16) return launch_team<GRID_F16, EVAL, FORM>(a, team, s, num_sms);
     if (gdt == GRID_BF16) return launch_team<GRID_BF16, EVAL, FORM>(a, team, s, num_sms);
     return launch_team<GRID_F32, EVAL, FORM>(a, team, s, num_sms);

@@ -78,6 +78,16 @@ struct GridView {
     double p0z, stepz;            // z origin and step in FP64 (cell decisions at the grid's z bounds)
 };
 
+// folded-surface substrate (SurfaceFolded, crates/libs/surfff/src/lib.rs:126-351)
+struct FoldedView {
+    int on;
+    int nx, ny, nz;
+    float inv[4];                 // inv_ax, inv_bx, inv_ay, inv_by
+    float alpha, fmax;            // make_plqs exponent, per-atom force clamp
+    const float* k;               // kx[nx], ky[ny], kz[nz], z0[nz]
+    const float4* coef;           // per basis function (cq, cp, cl, 0), index ix + nx (iy + ny iz)
+};
+
 struct FireDev {
     double dt0, dt_max, alpha0, f_inc, f_dec, f_alpha, fconv, flimit;
     int n_min;
@@ -91,6 +101,7 @@ struct KernelArgs {
     const AngRec* angs; const DihRec* dihs; const InvRec* invs;
     float4* pos; float4* plo; float4* vel; float4* force;
     GridView grid; int has_grid;
+    FoldedView fold;              // fold.on: the substrate is the folded surface, not the grid
     float R2damp, alpha_morse, rc2;
     FireDev fire;
     int phase_limit;              // this launch runs a system until SlotState::steps reaches min(target, phase_limit)

@@ -233,6 +233,20 @@ class RelaxMulti:
     def convert_grid(self, dtype):
         self._chk(self.L.smr_convert_grid(self.h, dtype), "smr_convert_grid")
 
+    def set_surface_folded(self, surf):
+        """Folded-surface substrate in place of the grid (a ``folded.FoldedSurface``, or None to go
+        back to the grid): MolWorld's SurfaceFolded with its per-atom force clamp."""
+        if surf is None:
+            self._chk(self.L.smr_set_surface_folded(self.h, None), "smr_set_surface_folded")
+            return
+        arrs = [_d(np.ravel(getattr(surf, k))) for k in ("kx", "ky", "kz", "z0", "cq", "cp", "cl")]
+        kx, ky, kz, z0, cq, cp, cl = arrs
+        if len(z0) != len(kz) or not (len(cq) == len(cp) == len(cl) == len(kx) * len(ky) * len(kz)):
+            raise ValueError("folded surface arrays do not match nx*ny*nz")
+        f = N.SmrFoldedSurface(surf.ax, surf.bx, surf.ay, surf.by, len(kx), len(ky), len(kz),
+                               *[_p(a, N.DP) for a in arrs], surf.alpha, surf.fmax)
+        self._chk(self.L.smr_set_surface_folded(self.h, C.byref(f)), "smr_set_surface_folded")
+
     def set_schedule(self, switch_step=0, latency_team=0, eval_form=0):
         self._chk(self.L.smr_set_schedule(self.h, switch_step, latency_team, eval_form), "smr_set_schedule")
 
