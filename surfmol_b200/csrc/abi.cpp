@@ -132,7 +132,7 @@ struct smr_handle {
     // folded surface: while set it is the substrate in place of the grid
     bool fold_on = false;
     int fold_n[3] = {0, 0, 0};
-    float fold_inv[4] = {0, 0, 0, 0};
+    float fold_inv[4] = {0, 0, 0, 0}, fold_inv_lo[4] = {0, 0, 0, 0};
     float fold_alpha = 2.f, fold_fmax = 100.f;
     DArr<float> dfold_k;                // kx, ky, kz, z0
     DArr<float4> dfold_coef;            // (cq, cp, cl, 0) per basis function
@@ -441,7 +441,7 @@ KernelArgs base_args(smr_handle* h) {
     if (h->fold_on) {
         a.fold.on = 1;
         a.fold.nx = h->fold_n[0]; a.fold.ny = h->fold_n[1]; a.fold.nz = h->fold_n[2];
-        for (int k = 0; k < 4; k++) a.fold.inv[k] = h->fold_inv[k];
+        for (int k = 0; k < 4; k++) { a.fold.inv[k] = h->fold_inv[k]; a.fold.inv_lo[k] = h->fold_inv_lo[k]; }
         a.fold.alpha = h->fold_alpha; a.fold.fmax = h->fold_fmax;
         a.fold.k = h->dfold_k.d; a.fold.coef = h->dfold_coef.d;
     }
@@ -721,8 +721,8 @@ int smr_set_surface_folded(smr_handle* h, const smr_folded_surface* f) {
     if (e != cudaSuccess) { h->fold_on = false; return fail(h, SMR_ERR_CUDA, "folded surface upload: %s", cudaGetErrorString(e)); }
     h->fold_n[0] = nx; h->fold_n[1] = ny; h->fold_n[2] = nz;
     const double idet = 1.0 / det;
-    h->fold_inv[0] = (float)(f->by * idet); h->fold_inv[1] = (float)(-f->bx * idet);
-    h->fold_inv[2] = (float)(-f->ay * idet); h->fold_inv[3] = (float)(f->ax * idet);
+    const double inv[4] = {f->by * idet, -f->bx * idet, -f->ay * idet, f->ax * idet};
+    for (int k = 0; k < 4; k++) { h->fold_inv[k] = (float)inv[k]; h->fold_inv_lo[k] = (float)(inv[k] - (double)h->fold_inv[k]); }
     h->fold_alpha = (float)f->alpha; h->fold_fmax = (float)f->fmax;
     h->fold_on = true;
     return SMR_OK;
@@ -1210,7 +1210,7 @@ static void sig_args(std::vector<long long>& v, const KernelArgs& a) {
     P(a.gscratch); v.push_back((long long)a.gscratch_bytes);
     P(a.nbl); P(a.nbl_cnt); P(a.nbl_ref); v.push_back(a.nbl_cap); v.push_back(a.nbl_min); F(a.nbl_skin);
     v.push_back(a.fold.on); v.push_back(a.fold.nx); v.push_back(a.fold.ny); v.push_back(a.fold.nz);
-    for (int k = 0; k < 4; k++) F(a.fold.inv[k]);
+    for (int k = 0; k < 4; k++) { F(a.fold.inv[k]); F(a.fold.inv_lo[k]); }
     F(a.fold.alpha); F(a.fold.fmax); P(a.fold.k); P(a.fold.coef);
 }
 

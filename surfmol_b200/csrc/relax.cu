@@ -205,8 +205,16 @@ __device__ __noinline__ int grid_cell_z_fp64(float pz, float lz, const GridView&
 __device__ __noinline__ float4 folded_part(const FoldedView f, float4 p, float4 lo, float4 q, int lane) {
     const float e = expf(-f.alpha * q.x);
     const float L = e * sqrtf(q.y), P = e * L, Q = q.z;
-    const float x = p.x + lo.x, y = p.y + lo.y, z = p.z + lo.z;
-    float u = f.inv[0] * x + f.inv[2] * y, v = f.inv[1] * x + f.inv[3] * y;
+    const float z = p.z + lo.z;
+    // fractional coordinates to ~1e-7 of a cell: the whole cells n are taken off inside the first
+    // fma, so the products are rounded only once they are small, and the inverse's rounding
+    // remainder and the positions' low words enter as corrections (one product rounding at |u| ~ 4
+    // would already cost 2.4e-7, or 1.5e-6 rad of phase)
+    const float nu = floorf(f.inv[0] * p.x + f.inv[2] * p.y), nv = floorf(f.inv[1] * p.x + f.inv[3] * p.y);
+    float u = fmaf(f.inv[0], p.x, -nu), v = fmaf(f.inv[1], p.x, -nv);
+    u = fmaf(f.inv[2], p.y, u); v = fmaf(f.inv[3], p.y, v);
+    u = fmaf(f.inv_lo[0], p.x, fmaf(f.inv_lo[2], p.y, u)); v = fmaf(f.inv_lo[1], p.x, fmaf(f.inv_lo[3], p.y, v));
+    u = fmaf(f.inv[0], lo.x, fmaf(f.inv[2], lo.y, u)); v = fmaf(f.inv[1], lo.x, fmaf(f.inv[3], lo.y, v));
     u -= floorf(u); v -= floorf(v);
     const float* kx = f.k;
     const float* ky = kx + f.nx;

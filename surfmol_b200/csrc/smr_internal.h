@@ -82,7 +82,8 @@ struct GridView {
 struct FoldedView {
     int on;
     int nx, ny, nz;
-    float inv[4];                 // inv_ax, inv_bx, inv_ay, inv_by
+    float inv[4];                 // inv_ax, inv_bx, inv_ay, inv_by (rounded to float)
+    float inv_lo[4];              // their rounding remainders: inverse = inv + inv_lo
     float alpha, fmax;            // make_plqs exponent, per-atom force clamp
     const float* k;               // kx[nx], ky[ny], kz[nz], z0[nz]
     const float4* coef;           // per basis function (cq, cp, cl, 0), index ix + nx (iy + ny iz)
