@@ -189,6 +189,26 @@ int smr_add_molecule(smr_handle* h, int natoms, const int* Z, const double* pos,
 int smr_add_molecules(smr_handle* h, int nmol, const int* natoms, const int* Z, const double* pos, const double* charges,
                       double bond_cut, int* topo_ids);
 int smr_add_topology(smr_handle* h, const smr_topology_desc* d, int* topo_id);
+/* Periodic molecules and PBC images: the bond shifts (neighCell / pbc_shifts) of
+ * evalBondsAndHNeigh_UFF (opencl/UFF.cl:141-236) and the NB image sums of
+ * getNonBond_GridFF_Bspline (UFF.cl:1592-1650), with the lattice per system as lvecs[iS].
+ * smr_add_molecule_pbc: bonds by cutoff to every image within one cell along each nonzero lattice
+ * vector (lvec = a, b, c, 9 values; a zero vector is a non-periodic axis), each bond slot recording
+ * its partner's cell.  Refused (SMR_ERR_ARG) when the cell is too small for index-based terms: an
+ * atom bonding to its own image, a pair bonding in two images, or a 3-bond path closing through
+ * the images.  npbc (may be null: one image each side along the periodic axes, 0 along the others)
+ * is the default of the systems made from it: the NB sum runs over the (2 npbc + 1) images per axis,
+ * excluding a bonded pair only in its bond's image and an atom's own images always.
+ * smr_set_pbc: per slot lattice (nsys x 9) and images (nsys x 3, each 0..7); images on any
+ * topology (an isolated molecule then meets its periodic copies); all-zero npbc on a molecule
+ * without periodic bonds turns PBC off for the slot.  Systems with images use the all-pairs NB
+ * loop (no neighbour lists).  smr_get_pbc reads a slot's setting back.  smr_topology_cells: the
+ * cell code of each neighbour slot (natoms x 4): 4-bit two's-complement offsets x | y << 4 | z << 8. */
+int smr_add_molecule_pbc(smr_handle* h, int natoms, const int* Z, const double* pos, const double* charges,
+                         double bond_cut, const double lvec[9], const int npbc[3], int* topo_id);
+int smr_set_pbc(smr_handle* h, int nsys, const int* slot_ids, const double* lvec, const int* npbc);
+int smr_get_pbc(smr_handle* h, int slot, double lvec[9], int npbc[3]);
+int smr_topology_cells(smr_handle* h, int topo_id, int* cells);
 /* counts[6] = natoms, nbonds, nang, ndih, ninv, type-rounds (schedule length) */
 int smr_topology_counts(smr_handle* h, int topo_id, int counts[6]);
 /* Any output pointer may be null.  Layouts as the arrays of smr_topology_desc plus

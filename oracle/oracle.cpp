@@ -192,7 +192,15 @@ struct orc_sys {
     std::vector<std::array<int,4>> invs; std::vector<std::array<int,3>> inv_ngs; std::vector<std::array<double,4>> invp; // (K,c0,c1,c2)
     std::vector<std::array<double,4>> req;               // (R, sqrt(E), Q, H)
     std::vector<int> type_id;
+    // periodic molecules: per neighbour slot the lattice offset of the bonded image (neighCell,
+    // opencl/UFF.cl:152, 229-236), as a cell code; empty for molecules without periodic bonds
+    std::vector<std::array<int,4>> ngc;
+    std::vector<std::array<int,3>> bond_off;             // per bond: offset of atom 1's image seen from atom 0
 };
+
+// Cell code of a lattice offset (ox, oy, oz), each in [-8, 7]: one 4-bit two's-complement field per axis.
+inline int cell_code(int ox, int oy, int oz) { return (ox & 15) | ((oy & 15) << 4) | ((oz & 15) << 8); }
+inline int cell_field(int c, int k) { int v = (c >> (4 * k)) & 15; return v >= 8 ? v - 16 : v; }
 
 // Folded surface (crates/libs/surfff/src/lib.rs:126-351, SurfaceFolded): separable basis of
 // lattice harmonics cos(2 pi k u), cos(2 pi k v) and z decays exp(-kz (z - z0)), one coefficient
@@ -475,7 +483,13 @@ void sample_grid(const orc_grid& g, const double PLQH[4], V3 u, double out[4]) {
     out[3] = bx[0] * Ez[0] + bx[1] * Ez[1] + bx[2] * Ez[2] + bx[3] * Ez[3];
 }
 
-struct NBParams { double rdamp, alpha, rcut; int excl13; };
+// lvec: lattice vectors a, b, c of the system (lvecs[iS], opencl/UFF.cl:1532-1574); npbc: image
+// counts per axis (nPBC); with all npbc 0 the NB sum has no images, as for an isolated molecule.
+struct NBParams { double rdamp, alpha, rcut; int excl13; double lvec[9]; int npbc[3]; };
+inline V3 lattice_shift(const NBParams& nb, int ox, int oy, int oz) {
+    return V3{ox * nb.lvec[0] + oy * nb.lvec[3] + oz * nb.lvec[6], ox * nb.lvec[1] + oy * nb.lvec[4] + oz * nb.lvec[7],
+              ox * nb.lvec[2] + oy * nb.lvec[5] + oz * nb.lvec[8]};
+}
 enum { E_TOT = 0, E_BOND, E_ANG, E_DIH, E_INV, E_NB, E_GRID, E_NCOMP = 8 };
 
 // One force evaluation; forces F (n), per-atom energy Ea (n, the reference's fapos.w),
@@ -491,6 +505,11 @@ void eval_forces(const orc_sys& S, const V3* P, const orc_grid* g, const NBParam
             int g2 = S.neighs[a][s];
             if (g2 < 0) { hn[4 * a + s] = {{0, 0, 0}, 1e6}; continue; }
             V3 dp = P[g2] - P[a];
+            // a bond to a neighbour's image in another cell (UFF.cl:229-236: dp += pbc_shifts[ngC])
+            if (!S.ngc.empty() && S.ngc[a][s]) {
+                const int c = S.ngc[a][s];
+                dp = dp + lattice_shift(nb, cell_field(c, 0), cell_field(c, 1), cell_field(c, 2));
+            }
             double l2 = dot(dp, dp); if (l2 < 1e-16) l2 = 1e-16;
             double l = std::sqrt(l2), il = 1.0 / l;
             V3 h = dp * il;
@@ -578,14 +597,36 @@ void eval_forces(const orc_sys& S, const V3* P, const orc_grid* g, const NBParam
         for (int r = 0; r < 4; r++) Ea[v[r]] += 0.25 * E;
         ei += E;
     }
-    // non-bonded + grid (UFF.cl:1524-1718, no PBC images for isolated molecules)
+    // non-bonded + grid (UFF.cl:1524-1718)
     const double R2damp = nb.rdamp * nb.rdamp;
     const double rc2 = nb.rcut > 0 ? nb.rcut * nb.rcut : 1e300;
+    const bool pbc = nb.npbc[0] > 0 || nb.npbc[1] > 0 || nb.npbc[2] > 0;
     for (int a = 0; a < n; a++) {
         V3 fe{0, 0, 0}; double E = 0;
         const auto& ri = S.req[a];
         const auto& ng = S.neighs[a];
-        for (int j = 0; j < n; j++) {
+        // PBC images (UFF.cl:1592-1650): every partner j != a in every image of the (2 npbc + 1)^3
+        // block, iz outer and ix inner; a bonded pair is excluded only in the image of its bond
+        // (neighbour index and cell both match); an atom never meets its own images
+        for (int j = 0; pbc && j < n; j++) {
+            if (j == a) continue;
+            const auto& rj = S.req[j];
+            for (int iz = -nb.npbc[2]; iz <= nb.npbc[2]; iz++)
+                for (int iy = -nb.npbc[1]; iy <= nb.npbc[1]; iy++)
+                    for (int ix = -nb.npbc[0]; ix <= nb.npbc[0]; ix++) {
+                        const int code = cell_code(ix, iy, iz);
+                        bool bonded = false;
+                        for (int s = 0; s < 4; s++)
+                            if (ng[s] == j && (S.ngc.empty() ? 0 : S.ngc[a][s]) == code) bonded = true;
+                        if (bonded) continue;
+                        V3 dp = P[j] - P[a] + lattice_shift(nb, ix, iy, iz);
+                        if (dot(dp, dp) > rc2) continue;
+                        V3 f;
+                        E += getLJQH(dp, ri[0] + rj[0], ri[1] * rj[1], ri[2] * rj[2], R2damp, f);
+                        fe = fe + f;
+                    }
+        }
+        for (int j = 0; !pbc && j < n; j++) {
             if (j == a) continue;
             if (j == ng[0] || j == ng[1] || j == ng[2] || j == ng[3]) continue;
             if (nb.excl13) {   // 1-3 exclusion: j bonded to a neighbour of a (getNonBond_ex2 semantics)
@@ -807,6 +848,72 @@ orc_sys* orc_sys_from_molecule(int n, const int* Z, const double* pos, const dou
     return S;
 }
 
+// Periodic molecule: bonds by cutoff to every image within one cell along each nonzero lattice
+// vector (lvec = a, b, c; a zero vector is a non-periodic axis), each bond remembering the cell of
+// its partner (neighCell).  Terms are enumerated over atom indices, so a cell in which a pair bonds
+// in two images, an atom bonds to its own image, or a 3-bond path returns to its first atom
+// through the images is too small and is refused (null, message in err).
+orc_sys* orc_sys_from_molecule_pbc(int n, const int* Z, const double* pos, const double* q, double bond_cut,
+                                   const double* lvec, char* err, int errlen) {
+    int range[3];
+    for (int k = 0; k < 3; k++) range[k] = (lvec[3 * k] != 0 || lvec[3 * k + 1] != 0 || lvec[3 * k + 2] != 0) ? 1 : 0;
+    NBParams L{}; for (int k = 0; k < 9; k++) L.lvec[k] = lvec[k];
+    orc_sys* S = new orc_sys();
+    S->n = n;
+    const double rc2 = bond_cut * bond_cut;
+    for (int i = 0; i < n; i++)
+        for (int j = i; j < n; j++) {
+            int found = 0;
+            for (int oz = -range[2]; oz <= range[2]; oz++)
+                for (int oy = -range[1]; oy <= range[1]; oy++)
+                    for (int ox = -range[0]; ox <= range[0]; ox++) {
+                        if (i == j && ox == 0 && oy == 0 && oz == 0) continue;
+                        V3 d = V3{pos[3 * j] - pos[3 * i], pos[3 * j + 1] - pos[3 * i + 1], pos[3 * j + 2] - pos[3 * i + 2]} +
+                               lattice_shift(L, ox, oy, oz);
+                        if (dot(d, d) >= rc2) continue;
+                        if (i == j) { std::snprintf(err, errlen, "atom %d bonds to its own image: cell too small", i); delete S; return nullptr; }
+                        if (found++) { std::snprintf(err, errlen, "atoms %d and %d bond in two images: cell too small", i, j); delete S; return nullptr; }
+                        S->bonds.push_back({i, j});
+                        S->bond_off.push_back({ox, oy, oz});
+                    }
+        }
+    fill_neighs(*S);
+    S->ngc.assign(n, {0, 0, 0, 0});
+    for (int a = 0; a < n; a++)
+        for (int s = 0; s < 4; s++) {
+            const int ib = S->neighBs[a][s];
+            if (ib < 0) continue;
+            const auto& o = S->bond_off[ib];
+            const int sg = S->bonds[ib][0] == a ? 1 : -1;   // offsets are seen from the bond's first atom
+            S->ngc[a][s] = cell_code(sg * o[0], sg * o[1], sg * o[2]);
+        }
+    // 3-bond paths i-j-k-l with l == i through the images
+    for (int j = 0; j < n; j++)
+        for (int sj = 0; sj < 4; sj++) {
+            const int k = S->neighs[j][sj]; if (k < 0) continue;
+            for (int si = 0; si < 4; si++) {
+                const int i = S->neighs[j][si]; if (i < 0 || si == sj) continue;
+                for (int sk = 0; sk < 4; sk++) {
+                    const int l = S->neighs[k][sk]; if (l != i) continue;
+                    int c[3];
+                    for (int ax = 0; ax < 3; ax++)
+                        c[ax] = -cell_field(S->ngc[j][si], ax) + cell_field(S->ngc[j][sj], ax) + cell_field(S->ngc[k][sk], ax);
+                    if (c[0] || c[1] || c[2]) { std::snprintf(err, errlen, "bond path %d-%d-%d-%d closes through the images: cell too small", i, j, k, l); delete S; return nullptr; }
+                }
+            }
+        }
+    std::vector<std::string> el(n);
+    for (int i = 0; i < n; i++) { const Elem* e = elem_by_Z(Z[i]); el[i] = e ? e->name : "X"; }
+    std::vector<std::string> T = assign_types(el, S->neighs);
+    finish_sys(S, &T);
+    if (q) for (int i = 0; i < n; i++) S->req[i][2] = q[i];
+    return S;
+}
+
+void orc_sys_cells(const orc_sys* S, int* ngc) {
+    for (int a = 0; a < S->n; a++) for (int s = 0; s < 4; s++) ngc[4 * a + s] = S->ngc.empty() ? 0 : S->ngc[a][s];
+}
+
 // Explicit bonds and parameters (angles/dihedrals/inversions enumerated from the
 // bonds with zero parameters unless set later).
 orc_sys* orc_sys_from_bonds(int n, int nbonds, const int* bonds, const double* bparams, const double* req) {
@@ -848,8 +955,13 @@ void orc_sys_set_params(orc_sys* S, const double* angp, const double* dihp, cons
 
 const char* orc_type_name(int id) { return (id >= 0 && id < N_ATYPES) ? ATYPES[id].name : "?"; }
 
-// nbp = (rdamp, alpha_morse, rcut (<=0: none), excl13 (0/1))
-static NBParams nbp_of(const double* p) { return NBParams{p[0], p[1], p[2], (int)p[3]}; }
+// nbp = (rdamp, alpha_morse, rcut (<=0: none), excl13 (0/1), lvec (9: a, b, c), npbc (3))
+static NBParams nbp_of(const double* p) {
+    NBParams nb{p[0], p[1], p[2], (int)p[3], {}, {}};
+    for (int k = 0; k < 9; k++) nb.lvec[k] = p[4 + k];
+    for (int k = 0; k < 3; k++) nb.npbc[k] = (int)p[13 + k];
+    return nb;
+}
 // fp = (dt0, dt_max, alpha0, f_inc, f_dec, f_alpha, n_min, fconv, flimit)
 static FireParams fp_of(const double* p) { return FireParams{p[0], p[1], p[2], p[3], p[4], p[5], (int)p[6], p[7], p[8]}; }
 

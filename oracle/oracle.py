@@ -45,6 +45,9 @@ def lib():
         L = C.CDLL(_LIB_PATH)
         L.orc_sys_from_molecule.restype = C.c_void_p
         L.orc_sys_from_molecule.argtypes = [C.c_int, IP, DP, DP, C.c_double]
+        L.orc_sys_from_molecule_pbc.restype = C.c_void_p
+        L.orc_sys_from_molecule_pbc.argtypes = [C.c_int, IP, DP, DP, C.c_double, DP, C.c_char_p, C.c_int]
+        L.orc_sys_cells.argtypes = [C.c_void_p, IP]
         L.orc_sys_from_bonds.restype = C.c_void_p
         L.orc_sys_from_bonds.argtypes = [C.c_int, C.c_int, IP, DP, DP]
         L.orc_sys_free.argtypes = [C.c_void_p]
@@ -97,7 +100,7 @@ def _ip(a):
 # the pentacene relaxation uses (crates/libs/surfmol/tests/relax_pentacene_uff.rs:259).
 FIRE_DEFAULT = dict(dt0=0.001, dt_max=0.05, alpha0=0.1, f_inc=1.1, f_dec=0.5, f_alpha=0.99, n_min=5,
                     fconv=1e-3, flimit=0.0)
-NB_DEFAULT = dict(rdamp=1.0, alpha=1.5, rcut=0.0, excl13=0)
+NB_DEFAULT = dict(rdamp=1.0, alpha=1.5, rcut=0.0, excl13=0, lvec=None, npbc=(0, 0, 0))
 
 
 def fire_vec(**kw):
@@ -110,7 +113,8 @@ def fire_vec(**kw):
 def nb_vec(**kw):
     p = dict(NB_DEFAULT)
     p.update(kw)
-    return _d([p["rdamp"], p["alpha"], p["rcut"], p["excl13"]])
+    lv = np.zeros(9) if p["lvec"] is None else _d(p["lvec"]).reshape(9)
+    return _d([p["rdamp"], p["alpha"], p["rcut"], p["excl13"], *lv, *p["npbc"]])
 
 
 class Grid:
@@ -186,11 +190,25 @@ class System:
         self.n, self.nbonds, self.nang, self.ndih, self.ninv = list(c)
 
     @classmethod
-    def from_molecule(cls, Z, pos, q=None, bond_cut=1.8):
+    def from_molecule(cls, Z, pos, q=None, bond_cut=1.8, lattice=None):
+        """lattice: (3, 3) lattice vectors a, b, c (zero rows: non-periodic axes) for a periodic
+        molecule whose bonds may cross the cell; None for an isolated molecule."""
         Z = _i(Z)
         pos = _d(pos)
         q = _d(q) if q is not None else None
-        return cls(lib().orc_sys_from_molecule(len(Z), _ip(Z), _dp(pos), _dp(q), bond_cut))
+        if lattice is None:
+            return cls(lib().orc_sys_from_molecule(len(Z), _ip(Z), _dp(pos), _dp(q), bond_cut))
+        err = C.create_string_buffer(300)
+        h = lib().orc_sys_from_molecule_pbc(len(Z), _ip(Z), _dp(pos), _dp(q), bond_cut, _dp(_d(lattice).reshape(9)), err, 300)
+        if not h:
+            raise ValueError(err.value.decode())
+        return cls(h)
+
+    def cells(self):
+        """Cell codes of the neighbour slots (n, 4): 4-bit two's-complement lattice offsets x | y << 4 | z << 8."""
+        out = np.zeros((self.n, 4), np.int32)
+        lib().orc_sys_cells(self.h, _ip(out))
+        return out
 
     @classmethod
     def from_bonds(cls, n, bonds, bparams, req=None):

@@ -76,6 +76,10 @@ SIGNATURES = {
     "smr_build_grid_static": (C.c_int, [C.c_int, DP, DP, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, DP, DP,
                                         C.POINTER(SmrGridBuildParamsStatic), VP, VP, C.c_char_p, C.c_int]),
     "smr_add_molecule": (C.c_int, [VP, C.c_int, IP, DP, DP, C.c_double, IP]),
+    "smr_add_molecule_pbc": (C.c_int, [VP, C.c_int, IP, DP, DP, C.c_double, DP, IP, IP]),
+    "smr_set_pbc": (C.c_int, [VP, C.c_int, IP, DP, IP]),
+    "smr_get_pbc": (C.c_int, [VP, C.c_int, DP, IP]),
+    "smr_topology_cells": (C.c_int, [VP, C.c_int, IP]),
     "smr_add_molecules": (C.c_int, [VP, C.c_int, IP, IP, DP, DP, C.c_double, IP]),
     "smr_add_topology": (C.c_int, [VP, C.POINTER(SmrTopologyDesc), IP]),
     "smr_topology_counts": (C.c_int, [VP, C.c_int, IP]),

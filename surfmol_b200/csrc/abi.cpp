@@ -92,9 +92,12 @@ struct smr_handle {
     std::vector<TopoDev> htd;
     DArr<TopoDev> dtd;
     std::vector<float4> hreq, hbk, hbl;
-    std::vector<short4> hneigh;
+    std::vector<short4> hneigh, hneighc;              // neighbour slots, their cell codes
     std::vector<AngRec> hang; std::vector<DihRec> hdih; std::vector<InvRec> hinv;
-    DArr<float4> dreq, dbk, dbl; DArr<short4> dneigh;
+    DArr<float4> dreq, dbk, dbl; DArr<short4> dneigh, dneighc;
+    // per slot: lattice vectors with the images each side in w (3 float4), for slots with pbc set
+    std::vector<float4> hlat;
+    DArr<float4> dlat;
     DArr<AngRec> dang; DArr<DihRec> ddih; DArr<InvRec> dinv;
     std::vector<int2> ha2f; std::vector<int> hidx;      // gather form: per atom (start, count), piece indices
     DArr<int2> da2f; DArr<int> didx;
@@ -213,10 +216,14 @@ void commit_topology(smr_handle* h, const HostTopo& T, const PreparedTopo& pt) {
     td.natoms = T.n;
     td.atom_off = (int)h->hreq.size();
     td.team = pt.team;
+    td.pbc_bonds = 0;
+    for (int c : T.neighc) if (c) td.pbc_bonds = 1;
     for (int a = 0; a < T.n; a++) {
         const double* r = &T.req[4 * a];
         h->hreq.push_back(make_float4((float)r[0], (float)r[1], (float)r[2], (float)r[3]));
         h->hneigh.push_back(make_short4((short)T.neighs[4 * a], (short)T.neighs[4 * a + 1], (short)T.neighs[4 * a + 2], (short)T.neighs[4 * a + 3]));
+        if (T.neighc.empty()) h->hneighc.push_back(make_short4(0, 0, 0, 0));
+        else h->hneighc.push_back(make_short4((short)T.neighc[4 * a], (short)T.neighc[4 * a + 1], (short)T.neighc[4 * a + 2], (short)T.neighc[4 * a + 3]));
         const double* kl = &T.bond_kl[8 * a];
         h->hbk.push_back(make_float4((float)kl[0], (float)kl[2], (float)kl[4], (float)kl[6]));
         h->hbl.push_back(make_float4((float)kl[1], (float)kl[3], (float)kl[5], (float)kl[7]));
@@ -274,6 +281,7 @@ int upload_all(smr_handle* h) {
     size_t t;
     t = ua; CU(h, sync_arr(h->dreq, h->hreq, t, s));
     t = ua; CU(h, sync_arr(h->dneigh, h->hneigh, t, s));
+    t = ua; CU(h, sync_arr(h->dneighc, h->hneighc, t, s));
     t = ua; CU(h, sync_arr(h->dbk, h->hbk, t, s));
     t = ua; CU(h, sync_arr(h->dbl, h->hbl, t, s));
     t = ua; CU(h, sync_arr(h->da2f, h->ha2f, t, s));
@@ -292,7 +300,7 @@ int upload_all(smr_handle* h) {
 
 // repack every topology for the current team mapping (after smr_set_team_size)
 int repack_all(smr_handle* h) {
-    h->htd.clear(); h->hreq.clear(); h->hneigh.clear(); h->hbk.clear(); h->hbl.clear();
+    h->htd.clear(); h->hreq.clear(); h->hneigh.clear(); h->hneighc.clear(); h->hbk.clear(); h->hbl.clear();
     h->hang.clear(); h->hdih.clear(); h->hinv.clear(); h->ha2f.clear(); h->hidx.clear();
     h->hown_geo.clear(); h->hown_par.clear(); h->hown_meta.clear();
     h->up_atoms = h->up_ang = h->up_dih = h->up_inv = h->up_topo = h->up_idx = h->up_own = 0;
@@ -313,7 +321,7 @@ int repack_all(smr_handle* h) {
 // copied in id order into fresh host mirrors, its offsets updated, and everything re-uploaded.
 int compact_topologies(smr_handle* h) {
     smr_handle& o = *h;
-    std::vector<float4> req, bk, bl; std::vector<short4> neigh; std::vector<int2> a2f; std::vector<int> meta, idx;
+    std::vector<float4> req, bk, bl; std::vector<short4> neigh, neighc; std::vector<int2> a2f; std::vector<int> meta, idx;
     std::vector<AngRec> ang; std::vector<DihRec> dih; std::vector<InvRec> inv;
     std::vector<short4> geo; std::vector<float4> par;
     auto cp = [](auto& dst, const auto& src, size_t off, size_t n) { dst.insert(dst.end(), src.begin() + off, src.begin() + off + n); };
@@ -322,7 +330,7 @@ int compact_topologies(smr_handle* h) {
         if (!o.topo_alive[id]) { td = TopoDev{}; td.atom_off = (int)req.size(); td.team = 32; o.own_len[id] = 0; continue; }
         const size_t n = td.natoms, a0 = td.atom_off;
         td.atom_off = (int)req.size();
-        cp(req, o.hreq, a0, n); cp(neigh, o.hneigh, a0, n); cp(bk, o.hbk, a0, n); cp(bl, o.hbl, a0, n);
+        cp(req, o.hreq, a0, n); cp(neigh, o.hneigh, a0, n); cp(neighc, o.hneighc, a0, n); cp(bk, o.hbk, a0, n); cp(bl, o.hbl, a0, n);
         cp(a2f, o.ha2f, a0, n); cp(meta, o.hown_meta, a0, n);
         const size_t T = td.team;
         size_t x;
@@ -339,7 +347,7 @@ int compact_topologies(smr_handle* h) {
             td.own_a_off += shift; td.own_i_off += shift; td.own_d_off += shift;
         }
     }
-    o.hreq.swap(req); o.hneigh.swap(neigh); o.hbk.swap(bk); o.hbl.swap(bl); o.ha2f.swap(a2f); o.hown_meta.swap(meta);
+    o.hreq.swap(req); o.hneigh.swap(neigh); o.hneighc.swap(neighc); o.hbk.swap(bk); o.hbl.swap(bl); o.ha2f.swap(a2f); o.hown_meta.swap(meta);
     o.hang.swap(ang); o.hdih.swap(dih); o.hinv.swap(inv); o.hidx.swap(idx); o.hown_geo.swap(geo); o.hown_par.swap(par);
     o.up_atoms = o.up_ang = o.up_dih = o.up_inv = o.up_topo = o.up_idx = o.up_own = 0;
     o.dead_atoms = 0;
@@ -421,6 +429,7 @@ KernelArgs base_args(smr_handle* h) {
     a.slots = h->slots;
     a.topos = h->dtd.d;
     a.req = h->dreq.d; a.neigh = h->dneigh.d; a.bk = h->dbk.d; a.bl = h->dbl.d;
+    a.neighc = h->dneighc.d; a.lat = h->dlat.d;
     a.angs = h->dang.d; a.dihs = h->ddih.d; a.invs = h->dinv.d;
     a.a2f = h->da2f.d; a.a2f_idx = h->didx.d;
     a.own_geo = h->down_geo.d; a.own_par = h->down_par.d; a.own_meta = h->down_meta.d;
@@ -461,7 +470,8 @@ int latency_team_for(int requested, int n) {
 
 // Launch segments for a list of slots.  The form of every system is decided from the system
 // alone (the requested form when the topology supports it and its own shared memory fits, else
-// the rounds form with its topology's team), never from what it is batched with; segments group
+// the rounds form with its topology's team; systems with a lattice always the gather form with
+// the periodic code), never from what it is batched with; segments group
 // equal (form, team) and are split wherever the segment's largest system would no longer fit.
 std::vector<Seg> group_by(smr_handle* h, std::vector<int>& ids, int form, int req_team = 0) {
     struct Key { int form, team, n, nf; };
@@ -469,6 +479,12 @@ std::vector<Seg> group_by(smr_handle* h, std::vector<int>& ids, int form, int re
         const SlotState& st = h->hs[s];
         const TopoDev& td = h->htd[st.topo];
         const int n = st.natoms, nf = td.npieces;
+        if (st.pbc) {
+            // periodic systems: the gather form with the PBC code, whatever the stage's form
+            const int t = req_team ? req_team : td.team;
+            if (team_smem_bytes(n, nf, t, FORM_GATHER_PBC) <= h->smem_optin) return Key{FORM_GATHER_PBC, t, n, nf};
+            return Key{FORM_GATHER_PBC, std::max(td.team, n > 1024 ? 512 : 256), n, nf};
+        }
         if (form == FORM_GATHER) {
             const int t = latency_team_for(req_team, n);
             if (team_smem_bytes(n, nf, t, FORM_GATHER) <= h->smem_optin) return Key{FORM_GATHER, t, n, nf};
@@ -582,6 +598,7 @@ int smr_create(const smr_config* cfg, smr_handle** out) {
         return bail(SMR_ERR_CUDA);
     h->hs.assign(ns, SlotState{});
     h->skey.assign(ns, 0u);
+    h->hlat.assign(3 * (size_t)ns, make_float4(0.f, 0.f, 0.f, 0.f));
     for (int s = (int)ns - 1; s >= 0; s--) h->free_slots.push_back(s);
     h->free_atoms[0] = (long long)na;
     cudaEventCreate(&h->ev0);
@@ -879,6 +896,80 @@ int smr_add_molecule(smr_handle* h, int natoms, const int* Z, const double* pos,
     return SMR_OK;
 }
 
+int smr_add_molecule_pbc(smr_handle* h, int natoms, const int* Z, const double* pos, const double* charges,
+                         double bond_cut, const double lvec[9], const int npbc[3], int* topo_id) {
+    if (!h || !Z || !pos || !lvec || !topo_id) return SMR_ERR_ARG;
+    SETTLE(h);
+    if (npbc) for (int k = 0; k < 3; k++)
+        if (npbc[k] < 0 || npbc[k] > 7) return fail(h, SMR_ERR_ARG, "npbc[%d]=%d outside [0, 7]", k, npbc[k]);
+    HostTopo T;
+    char msg[300] = {0};
+    if (build_molecule_topology_pbc(natoms, Z, pos, charges, bond_cut > 0 ? bond_cut : 1.8, lvec, T, msg, sizeof(msg)))
+        return fail(h, SMR_ERR_ARG, "periodic molecule: %s", msg);
+    if (npbc) for (int k = 0; k < 3; k++) T.npbc[k] = npbc[k];
+    h->topos.push_back(std::move(T));
+    h->topo_alive.push_back(1);
+    append_topology(h, h->topos.back());
+    int r = upload_all(h);
+    if (r) return r;
+    *topo_id = (int)h->topos.size() - 1;
+    return SMR_OK;
+}
+
+// write the lattice rows of the given slots to the device (the per-slot table is allocated on first use)
+static int upload_lat(smr_handle* h, const std::vector<int>& ids) {
+    if (ids.empty()) return SMR_OK;
+    CU(h, h->dlat.reserve(h->hlat.size(), 0, h->stream));
+    for (int s : ids) CU(h, cudaMemcpyAsync(h->dlat.d + 3 * (size_t)s, &h->hlat[3 * (size_t)s], 48, cudaMemcpyHostToDevice, h->stream));
+    return wait_stream(h, h->watchdog_s);
+}
+
+// a slot's lattice and images: the rows of hlat and the slot flag (no flag without images or periodic bonds)
+static void set_slot_lattice(smr_handle* h, int s, const double* lvec, const int* npbc) {
+    const HostTopo& T = h->topos[h->hs[s].topo];
+    bool on = !T.neighc.empty();
+    for (int k = 0; k < 3; k++) {
+        h->hlat[3 * (size_t)s + k] = make_float4((float)lvec[3 * k], (float)lvec[3 * k + 1], (float)lvec[3 * k + 2], (float)npbc[k]);
+        on = on || npbc[k] > 0;
+    }
+    h->hs[s].pbc = on ? 1 : 0;
+}
+
+int smr_set_pbc(smr_handle* h, int nsys, const int* slot_ids, const double* lvec, const int* npbc) {
+    if (!h || nsys < 0 || (nsys && (!slot_ids || !lvec || !npbc))) return SMR_ERR_ARG;
+    SETTLE(h);
+    for (int i = 0; i < nsys; i++) {
+        if (!valid_slot(h, slot_ids[i])) return fail(h, SMR_ERR_ARG, "slot %d not active", slot_ids[i]);
+        for (int k = 0; k < 3; k++)
+            if (npbc[3 * i + k] < 0 || npbc[3 * i + k] > 7) return fail(h, SMR_ERR_ARG, "system %d: npbc[%d]=%d outside [0, 7]", i, k, npbc[3 * i + k]);
+        const HostTopo& T = h->topos[h->hs[slot_ids[i]].topo];
+        for (int k = 0; k < 3; k++) {
+            const bool crosses = [&] { for (size_t c = 0; c < T.neighc.size(); c++) if (cell_field(T.neighc[c], k)) return true; return false; }();
+            const double* v = lvec + 9 * (size_t)i + 3 * k;
+            if (crosses && v[0] == 0 && v[1] == 0 && v[2] == 0)
+                return fail(h, SMR_ERR_ARG, "system %d: bonds cross lattice axis %d but its vector is zero", i, k);
+        }
+    }
+    std::vector<int> ids(slot_ids, slot_ids + nsys);
+    for (int i = 0; i < nsys; i++) set_slot_lattice(h, slot_ids[i], lvec + 9 * (size_t)i, npbc + 3 * (size_t)i);
+    int r = upload_lat(h, ids);
+    if (r) return r;
+    return upload_slots(h, ids);
+}
+
+int smr_get_pbc(smr_handle* h, int slot, double lvec[9], int npbc[3]) {
+    if (!h || !lvec || !npbc) return SMR_ERR_ARG;
+    SETTLE(h);
+    if (!valid_slot(h, slot)) return fail(h, SMR_ERR_ARG, "slot %d not active", slot);
+    for (int k = 0; k < 3; k++) {
+        const float4 v = h->hlat[3 * (size_t)slot + k];
+        const bool on = h->hs[slot].pbc != 0;
+        lvec[3 * k] = on ? v.x : 0.0; lvec[3 * k + 1] = on ? v.y : 0.0; lvec[3 * k + 2] = on ? v.z : 0.0;
+        npbc[k] = on ? (int)v.w : 0;
+    }
+    return SMR_OK;
+}
+
 int smr_add_molecules(smr_handle* h, int nmol, const int* natoms, const int* Z, const double* pos, const double* charges,
                       double bond_cut, int* topo_ids) {
     if (!h || nmol < 0 || (nmol && (!natoms || !Z || !pos || !topo_ids))) return SMR_ERR_ARG;
@@ -954,6 +1045,14 @@ int smr_topology_counts(smr_handle* h, int id, int c[6]) {
     return SMR_OK;
 }
 
+int smr_topology_cells(smr_handle* h, int topo_id, int* cells) {
+    if (!h || !cells) return SMR_ERR_ARG;
+    if (topo_id < 0 || topo_id >= (int)h->topos.size() || !h->topo_alive[topo_id]) return fail(h, SMR_ERR_ARG, "unknown topology %d", topo_id);
+    const HostTopo& T = h->topos[topo_id];
+    for (int k = 0; k < 4 * T.n; k++) cells[k] = T.neighc.empty() ? 0 : T.neighc[k];
+    return SMR_OK;
+}
+
 int smr_topology_export(smr_handle* h, int id, int* neighs, int* neighBs, int* bonds, double* bparams,
                         int* angs, int* ang_ngs, double* angp, int* dihs, int* dih_ngs, double* dihp,
                         int* invs, int* inv_ngs, double* invp, double* req, int* type_id) {
@@ -996,7 +1095,7 @@ int smr_add_systems(smr_handle* h, int nsys, const int* topo_ids, const float* p
             return fail(h, SMR_ERR_ARG, "system %d: unknown topology %d", i, topo_ids[i]);
         need += h->topos[topo_ids[i]].n;
     }
-    std::vector<int> ids(nsys), src(nsys), len(nsys), dst(nsys);
+    std::vector<int> ids(nsys), src(nsys), len(nsys), dst(nsys), lat_ids;
     long long p = 0;
     for (int i = 0; i < nsys; i++) {
         int n = h->topos[topo_ids[i]].n;
@@ -1010,6 +1109,8 @@ int smr_add_systems(smr_handle* h, int nsys, const int* topo_ids, const float* p
         SlotState& st = h->hs[s];
         st = SlotState{};
         st.topo = topo_ids[i]; st.atom_off = (int)off; st.natoms = n; st.active = 1; st.dt = -1.0;
+        const HostTopo& T = h->topos[topo_ids[i]];
+        if (!T.neighc.empty() || T.npbc[0] || T.npbc[1] || T.npbc[2]) { set_slot_lattice(h, s, T.lattice, T.npbc); lat_ids.push_back(s); }
         ids[i] = s; src[i] = (int)p; len[i] = n; dst[i] = (int)off;
         h->skey[s] = locality_key(h, pos + 3 * p, n);
         for (int a = 0; a < n; a++) h->pinned[p + a] = make_float4(pos[3 * (p + a)], pos[3 * (p + a) + 1], pos[3 * (p + a) + 2], 0.f);
@@ -1024,7 +1125,9 @@ int smr_add_systems(smr_handle* h, int nsys, const int* topo_ids, const float* p
     if (launch_copy_segments(h->xfer, h->xfer + nsys, h->xfer + 2 * nsys, nsys, h->stage, h->pos, s)) return fail(h, SMR_ERR_CUDA, "scatter launch failed");
     CU(h, cudaMemsetAsync(h->stage, 0, (size_t)p * 16, s));
     if (launch_copy_segments(h->xfer, h->xfer + nsys, h->xfer + 2 * nsys, nsys, h->stage, h->plo, s)) return fail(h, SMR_ERR_CUDA, "scatter launch failed");
-    int r = upload_slots(h, ids);
+    int r = upload_lat(h, lat_ids);
+    if (r) return r;
+    r = upload_slots(h, ids);
     if (r) return r;
     r = wait_stream(h, h->watchdog_s);
     if (r) return r;
@@ -1208,6 +1311,7 @@ static void sig_args(std::vector<long long>& v, const KernelArgs& a) {
     v.push_back(a.phase_limit); v.push_back(a.step_budget); P(a.ecomp); v.push_back(a.nmax); v.push_back(a.nfmax);
     P(a.a2f); P(a.a2f_idx); P(a.own_geo); P(a.own_par); P(a.own_meta); v.push_back(a.nb_lanes);
     P(a.gscratch); v.push_back((long long)a.gscratch_bytes);
+    P(a.neighc); P(a.lat);
     P(a.nbl); P(a.nbl_cnt); P(a.nbl_ref); v.push_back(a.nbl_cap); v.push_back(a.nbl_min); F(a.nbl_skin);
     v.push_back(a.fold.on); v.push_back(a.fold.nx); v.push_back(a.fold.ny); v.push_back(a.fold.nz);
     for (int k = 0; k < 4; k++) { F(a.fold.inv[k]); F(a.fold.inv_lo[k]); }

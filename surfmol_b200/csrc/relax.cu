@@ -53,7 +53,7 @@ __host__ __device__ inline size_t red_bytes(int T) { return T > 32 ? size_t(T / 
 __host__ __device__ inline size_t team_bytes(int nmax, int nfmax, int T, int form) {
     size_t n = (size_t)nmax;
     return n * 16 * 5 + n * 64 + align16(n * 4) + align16(n * 8) + red_bytes(T) +
-           (form == FORM_GATHER ? (size_t)nfmax * 16 : 0) + (form == FORM_OWNER ? n * 64 : 0);
+           (form == FORM_GATHER || form == FORM_GATHER_PBC ? (size_t)nfmax * 16 : 0) + (form == FORM_OWNER ? n * 64 : 0);
 }
 
 // Shared memory of one team: one base pointer and the capacity; every array's address is
@@ -244,23 +244,14 @@ __device__ __noinline__ float4 folded_part(const FoldedView f, float4 p, float4 
     return make_float4(E, du, dv, dz);
 }
 
-// One LJ + damped-Coulomb pair (getLJQH, opencl/UFF.cl:82-95) added to the force / energy of atom i;
-// excluded pairs and pairs beyond the cutoff are evaluated at r^2 = 1 and weighted 0.
-template <bool CUT>
-__device__ __forceinline__ void nb_pair(const KernelArgs& a, float4 pi, float4 li, float4 qi, float4 pj, float4 lj, float4 qj,
-                                        bool excluded, float& fx, float& fy, float& fz, float& E) {
-    const float dx = (pj.x - pi.x) + (lj.x - li.x), dy = (pj.y - pi.y) + (lj.y - li.y), dz = (pj.z - pi.z) + (lj.z - li.z);
+// One LJ + damped-Coulomb pair (getLJQH, opencl/UFF.cl:82-95) at separation (dx, dy, dz) added to
+// the force / energy of atom i; skipped pairs are evaluated at r^2 = 1 and weighted 0.
+__device__ __forceinline__ void ljq_pair(float dx, float dy, float dz, bool skip, float4 qi, float4 qj, float R2damp,
+                                         float& fx, float& fy, float& fz, float& E) {
     float r2 = dx * dx + dy * dy + dz * dz;
-    bool out = false;
-    if (CUT) {
-        out = r2 > a.rc2;
-        // at the cutoff: decide in FP64, so FP32 rounding never moves a pair across it
-        if (fabsf(r2 - a.rc2) < 1e-4f * a.rc2) out = beyond_cutoff_fp64(pi, li, pj, lj, a.rc2);
-    }
-    const bool skip = excluded || out;
     r2 = skip ? 1.0f : r2;
     const float R0 = qi.x + qj.x, E0 = qi.y * qj.y, Q = qi.z * qj.z;
-    const float rs = rsqrtf(r2 + a.R2damp);          // 1/sqrt(r^2 + Rdamp^2)
+    const float rs = rsqrtf(r2 + R2damp);            // 1/sqrt(r^2 + Rdamp^2)
     const float Ec = kCoulomb * Q * rs;
     const float ir2 = 1.0f / r2;
     const float u2 = R0 * R0 * ir2, u6 = u2 * u2 * u2, vdW = u6 * E0;
@@ -268,6 +259,122 @@ __device__ __forceinline__ void nb_pair(const KernelArgs& a, float4 pi, float4 l
     E += w * ((u6 - 2.0f) * vdW + Ec);
     const float fr = w * (-12.0f * (u6 - 1.0f) * vdW * ir2 - Ec * (rs * rs));
     fx += dx * fr; fy += dy * fr; fz += dz * fr;
+}
+
+// One pair of the team's atoms i, j (compensated positions); excluded pairs and, under a cutoff,
+// pairs beyond it weigh 0.
+template <bool CUT>
+__device__ __forceinline__ void nb_pair(const KernelArgs& a, float4 pi, float4 li, float4 qi, float4 pj, float4 lj, float4 qj,
+                                        bool excluded, float& fx, float& fy, float& fz, float& E) {
+    const float dx = (pj.x - pi.x) + (lj.x - li.x), dy = (pj.y - pi.y) + (lj.y - li.y), dz = (pj.z - pi.z) + (lj.z - li.z);
+    bool out = false;
+    if (CUT) {
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        out = r2 > a.rc2;
+        // at the cutoff: decide in FP64, so FP32 rounding never moves a pair across it
+        if (fabsf(r2 - a.rc2) < 1e-4f * a.rc2) out = beyond_cutoff_fp64(pi, li, pj, lj, a.rc2);
+    }
+    ljq_pair(dx, dy, dz, excluded || out, qi, qj, a.R2damp, fx, fy, fz, E);
+}
+
+// ------------------------------------------------------------------ periodic systems
+__device__ __forceinline__ int cell_f(int c, int k) { const int v = (c >> (4 * k)) & 15; return v >= 8 ? v - 16 : v; }
+
+// Lattice shift of cell code c (4-bit offsets x | y << 4 | z << 8) for the lattice rows lat[0..2].
+__device__ __forceinline__ float3 cell_shift(const float4* lat, int c) {
+    const float4 A = __ldg(lat), B = __ldg(lat + 1), C = __ldg(lat + 2);
+    const float ox = (float)cell_f(c, 0), oy = (float)cell_f(c, 1), oz = (float)cell_f(c, 2);
+    return make_float3(ox * A.x + oy * B.x + oz * C.x, ox * A.y + oy * B.y + oz * C.y, ox * A.z + oy * B.z + oz * C.z);
+}
+
+// (pj + lj) - (pi + li) + s for a bond whose partner sits in another cell: the two coordinates
+// differ by about a lattice vector, so the roundings of pj - pi and of adding s are recovered
+// (TwoSum) and added back; the bond vector keeps the accuracy of an in-cell bond.
+__device__ __forceinline__ float shifted_diff(float pj, float pi, float lj, float li, float s) {
+    const float t = pj - pi, tb = t - pj, e1 = (pj - (t - tb)) + (-pi - tb);
+    const float u = t + s, ub = u - t, e2 = (t - (u - ub)) + (s - ub);
+    return u + ((e1 + e2) + (lj - li));
+}
+
+// Phase A for one atom of a system with periodic bonds: bond vectors (hneigh) and bond forces, a
+// slot whose partner sits in another cell shifted by its lattice vector (UFF.cl:229-236).  Writes
+// the atom's hneigh, force and bond energy; returns the bond energy.  Not inlined.
+__device__ __forceinline__ float bonds_atom_pbc(Smem S, const float4* bk_, const float4* bl_, const short4* ngc_, const float4* lat, int i) {
+    const float4 pi = S.P()[i], li = S.Lo()[i];
+    const short4 ng = S.Ng()[i], gc = __ldg(ngc_ + i);
+    const float4 bk = __ldg(bk_ + i), bl = __ldg(bl_ + i);
+    float fx = 0.f, fy = 0.f, fz = 0.f, E = 0.f;
+    for (int s = 0; s < 4; s++) {
+        const int g = comp(ng, s);
+        if (g < 0) { S.H()[s * S.n + i] = make_float4(0.f, 0.f, 0.f, 1e6f); continue; }
+        const float4 pj = S.P()[g], lj = S.Lo()[g];
+        const int cc = comp(gc, s);
+        float dx, dy, dz;
+        if (cc) {
+            const float3 sh = cell_shift(lat, cc);
+            dx = shifted_diff(pj.x, pi.x, lj.x, li.x, sh.x);
+            dy = shifted_diff(pj.y, pi.y, lj.y, li.y, sh.y);
+            dz = shifted_diff(pj.z, pi.z, lj.z, li.z, sh.z);
+        } else {
+            dx = (pj.x - pi.x) + (lj.x - li.x); dy = (pj.y - pi.y) + (lj.y - li.y); dz = (pj.z - pi.z) + (lj.z - li.z);
+        }
+        const float l2 = fmaxf(dx * dx + dy * dy + dz * dz, 1e-16f);
+        const float l = sqrtf(l2), il = 1.0f / l;
+        const float hx = dx * il, hy = dy * il, hz = dz * il;
+        S.H()[s * S.n + i] = make_float4(hx, hy, hz, il);
+        const float k = comp(bk, s), dl = l - comp(bl, s), fr = 2.0f * k * dl;
+        fx += hx * fr; fy += hy * fr; fz += hz * fr;
+        E += k * dl * dl;
+    }
+    S.F()[i] = make_float4(fx, fy, fz, E);
+    S.Eh()[i] = E;
+    return E;
+}
+
+// beyond_cutoff_fp64 for a partner image shifted by s
+__device__ __noinline__ bool beyond_cutoff_fp64_shift(float4 pi, float4 li, float4 pj, float4 lj, float sx, float sy, float sz, float rc2) {
+    const double dx = ((double)pj.x - (double)pi.x) + ((double)lj.x - (double)li.x) + (double)sx;
+    const double dy = ((double)pj.y - (double)pi.y) + ((double)lj.y - (double)li.y) + (double)sy;
+    const double dz = ((double)pj.z - (double)pi.z) + ((double)lj.z - (double)li.z) + (double)sz;
+    return dx * dx + dy * dy + dz * dz > (double)rc2;
+}
+
+// NB sum of atom i over the partners j = c, c + L, ... < N in every image of the system's
+// (2 nx + 1)(2 ny + 1)(2 nz + 1) block (getNonBond_GridFF_Bspline with PBC, opencl/UFF.cl:1592-1650):
+// an atom never meets its own images, a bonded pair is excluded only in the image of its bond
+// (neighbour index and cell code both match).  Returns (F, E) of atom i.  Not inlined: the
+// kernels' other phases keep their registers.
+__device__ __forceinline__ float4 nb_atom_images(Smem S, float rc2, float R2damp, const float4* lat, int N, int i, int c,
+                                              int L, short4 ng, short4 gc) {
+    const float4 A = __ldg(lat), B = __ldg(lat + 1), C = __ldg(lat + 2);
+    const int nx = (int)A.w, ny = (int)B.w, nz = (int)C.w;
+    const bool cut = rc2 < 1e37f;
+    const float4 pi = S.P()[i], li = S.Lo()[i], qi = S.Q()[i];
+    float fx = 0.f, fy = 0.f, fz = 0.f, E = 0.f;
+    for (int j = c; j < N; j += L) {
+        if (j == i) continue;
+        const float4 pj = S.P()[j], lj = S.Lo()[j], qj = S.Q()[j];
+        const float dx0 = (pj.x - pi.x) + (lj.x - li.x), dy0 = (pj.y - pi.y) + (lj.y - li.y), dz0 = (pj.z - pi.z) + (lj.z - li.z);
+        for (int iz = -nz; iz <= nz; iz++)
+            for (int iy = -ny; iy <= ny; iy++)
+                for (int ix = -nx; ix <= nx; ix++) {
+                    const int code = (ix & 15) | ((iy & 15) << 4) | ((iz & 15) << 8);
+                    const bool bonded = (j == ng.x && code == gc.x) || (j == ng.y && code == gc.y) ||
+                                        (j == ng.z && code == gc.z) || (j == ng.w && code == gc.w);
+                    const float fxi = (float)ix, fyi = (float)iy, fzi = (float)iz;
+                    const float sx = fxi * A.x + fyi * B.x + fzi * C.x, sy = fxi * A.y + fyi * B.y + fzi * C.y,
+                                sz = fxi * A.z + fyi * B.z + fzi * C.z;
+                    const float dx = dx0 + sx, dy = dy0 + sy, dz = dz0 + sz;
+                    bool out = false;
+                    if (cut) {
+                        const float r2 = dx * dx + dy * dy + dz * dz;
+                        out = r2 > rc2;
+                        if (fabsf(r2 - rc2) < 1e-4f * rc2) out = beyond_cutoff_fp64_shift(pi, li, pj, lj, sx, sy, sz, rc2);
+                    }
+                    ljq_pair(dx, dy, dz, bonded || out, qi, qj, R2damp, fx, fy, fz, E);
+                }
+    }
+    return make_float4(fx, fy, fz, E);
 }
 
 // lanes per atom for the NB partner loop: minimise passes x (partners per lane + the shuffle
@@ -377,38 +484,50 @@ template <> struct EAcc<true> {
 // ------------------------------------------------------------------ force evaluation
 template <int T, int GDT, bool EVAL, int FORM>
 __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* __restrict__ tpp, int N, int rank, EAcc<EVAL>& acc,
-                            bool use_list = false, size_t ga0 = 0) {
+                            const float4* lat, bool use_list = false, size_t ga0 = 0) {
 #define TP(f) __ldg(&tpp->f)
+    // periodic systems (lat: the slot's lattice rows) run in FORM_GATHER_PBC, the gather form plus
+    // bonds to a partner's image in another cell (neighCell, UFF.cl:229-236) and NB image sums
+    constexpr bool PBC = FORM == FORM_GATHER_PBC;
+    constexpr int BF = PBC ? FORM_GATHER : FORM;
+    const bool pbc_bonds = PBC && lat != nullptr && TP(pbc_bonds) != 0;
     // A: bonds and hneigh, one atom per rank (opencl/UFF.cl:141-322)
-    for (int i = rank; i < N; i += T) {
-        const float4 pi = S.P()[i], li = S.Lo()[i];
-        const short4 ng = S.Ng()[i];
-        const float4 bk = __ldg(a.bk + TP(atom_off) + i), bl = __ldg(a.bl + TP(atom_off) + i);
-        float fx = 0.f, fy = 0.f, fz = 0.f, E = 0.f;
-#pragma unroll
-        for (int s = 0; s < 4; s++) {
-            const int g = comp(ng, s);
-            if (g < 0) { S.H()[s * S.n + i] = make_float4(0.f, 0.f, 0.f, 1e6f); continue; }
-            const float4 pj = S.P()[g], lj = S.Lo()[g];
-            // difference of the compensated positions: its error is relative to the bond length,
-            // not to the absolute coordinate (float positions alone would put ~1e-6 A of rounding
-            // into every stiff bond and make the force field rough at the 1e-4 eV/A level)
-            const float dx = (pj.x - pi.x) + (lj.x - li.x), dy = (pj.y - pi.y) + (lj.y - li.y), dz = (pj.z - pi.z) + (lj.z - li.z);
-            const float l2 = fmaxf(dx * dx + dy * dy + dz * dz, 1e-16f);
-            const float l = sqrtf(l2), il = 1.0f / l;
-            const float hx = dx * il, hy = dy * il, hz = dz * il;
-            S.H()[s * S.n + i] = make_float4(hx, hy, hz, il);
-            const float k = comp(bk, s), dl = l - comp(bl, s), fr = 2.0f * k * dl;
-            fx += hx * fr; fy += hy * fr; fz += hz * fr;
-            E += k * dl * dl;
+    if (pbc_bonds) {
+        for (int i = rank; i < N; i += T) {
+            const float E = bonds_atom_pbc(S, a.bk + TP(atom_off), a.bl + TP(atom_off), a.neighc + TP(atom_off), lat, i);
+            acc.add(0, 0.5 * (double)E);
         }
-        S.F()[i] = make_float4(fx, fy, fz, E);
-        S.Eh()[i] = E;
-        acc.add(0, 0.5 * (double)E);
+    } else {
+        for (int i = rank; i < N; i += T) {
+            const float4 pi = S.P()[i], li = S.Lo()[i];
+            const short4 ng = S.Ng()[i];
+            const float4 bk = __ldg(a.bk + TP(atom_off) + i), bl = __ldg(a.bl + TP(atom_off) + i);
+            float fx = 0.f, fy = 0.f, fz = 0.f, E = 0.f;
+    #pragma unroll
+            for (int s = 0; s < 4; s++) {
+                const int g = comp(ng, s);
+                if (g < 0) { S.H()[s * S.n + i] = make_float4(0.f, 0.f, 0.f, 1e6f); continue; }
+                const float4 pj = S.P()[g], lj = S.Lo()[g];
+                // difference of the compensated positions: its error is relative to the bond length,
+                // not to the absolute coordinate (float positions alone would put ~1e-6 A of rounding
+                // into every stiff bond and make the force field rough at the 1e-4 eV/A level)
+                const float dx = (pj.x - pi.x) + (lj.x - li.x), dy = (pj.y - pi.y) + (lj.y - li.y), dz = (pj.z - pi.z) + (lj.z - li.z);
+                const float l2 = fmaxf(dx * dx + dy * dy + dz * dz, 1e-16f);
+                const float l = sqrtf(l2), il = 1.0f / l;
+                const float hx = dx * il, hy = dy * il, hz = dz * il;
+                S.H()[s * S.n + i] = make_float4(hx, hy, hz, il);
+                const float k = comp(bk, s), dl = l - comp(bl, s), fr = 2.0f * k * dl;
+                fx += hx * fr; fy += hy * fr; fz += hz * fr;
+                E += k * dl * dl;
+            }
+            S.F()[i] = make_float4(fx, fy, fz, E);
+            S.Eh()[i] = E;
+            acc.add(0, 0.5 * (double)E);
+        }
     }
     team_sync<T>();
 
-    if (FORM == FORM_ROUNDS) {
+    if (BF == FORM_ROUNDS) {
         // B (rounds): in one round the atoms of each role are distinct, so each role's pieces
         // are added with plain read-modify-writes separated by team syncs
         for (int r = 0; r < TP(ang_rounds); r++) {
@@ -457,7 +576,7 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
             if (ok) addf(S.F()[rec.at.w], f4, e4);
             team_sync<T>();
         }
-    } else if (FORM == FORM_OWNER) {
+    } else if (BF == FORM_OWNER) {
         // B (owner): lane o evaluates the terms atom o owns and keeps every piece in registers: its
         // own, and those of its neighbours by bond slot (angles: apex j, pieces on i and k;
         // inversions: centre i, pieces on j, k, l; a dihedral i-j-k-l once at j, keeping the
@@ -607,6 +726,8 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
         const int L = a.nb_lanes > 0 ? min(a.nb_lanes, min(T, 32)) : nb_lanes(Neff, T), G = T / L;
         const int c = rank & (L - 1);
         const bool small = N <= 64;
+        // PBC images: uniform per system
+        const bool images = PBC && lat != nullptr && __ldg(&lat[0].w) + __ldg(&lat[1].w) + __ldg(&lat[2].w) > 0.f;
         // the partner loop with the cutoff logic compiled in or out (uniform per launch)
         auto nb_atoms = [&](auto cut_tag) {
         constexpr bool CUT = decltype(cut_tag)::value;
@@ -649,7 +770,24 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
             }
         }
         };
-        if (a.rc2 < 1e37f) nb_atoms(std::integral_constant<bool, true>{});
+        if (images) {
+            // periodic system: the same lanes-per-atom split over the image sums
+            for (int i0 = 0; i0 < N; i0 += G) {
+                const int i = i0 + rank / L;
+                float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (i < N) r = nb_atom_images(S, a.rc2, a.R2damp, lat, N, i, c, L, S.Ng()[i], __ldg(a.neighc + TP(atom_off) + i));
+                for (int o = 1; o < L; o <<= 1) {
+                    r.x += __shfl_xor_sync(FULL, r.x, o); r.y += __shfl_xor_sync(FULL, r.y, o);
+                    r.z += __shfl_xor_sync(FULL, r.z, o); r.w += __shfl_xor_sync(FULL, r.w, o);
+                }
+                if (c == 0 && i < N) {
+                    add4(S.F()[i], r.x, r.y, r.z, r.w);
+                    S.Eh()[i] += r.w;
+                    acc.add(4, 0.5 * (double)r.w);
+                }
+            }
+        }
+        else if (a.rc2 < 1e37f) nb_atoms(std::integral_constant<bool, true>{});
         else nb_atoms(std::integral_constant<bool, false>{});
     }
     team_sync<T>();
@@ -831,8 +969,9 @@ __device__ void run_system(const KernelArgs& a, const Smem& S, int w, int rank) 
     team_sync<T>();
 
     EAcc<EVAL> acc;
+    const float4* lat = st.pbc ? a.lat + 3 * (size_t)slot : nullptr;
     if (EVAL) {
-        eval_forces<T, GDT, EVAL, FORM>(a, S, tpp, N, rank, acc);
+        eval_forces<T, GDT, EVAL, FORM>(a, S, tpp, N, rank, acc, lat);
         for (int i = rank; i < N; i += T) a.force[st.atom_off + i] = S.F()[i];
         if constexpr (EVAL) {
             double tot = 0, e[6];
@@ -850,7 +989,7 @@ __device__ void run_system(const KernelArgs& a, const Smem& S, int w, int rank) 
 
     // neighbour list: rebuilt on the first step after positions were set (fresh FIRE state) and
     // whenever an atom has moved more than skin / 2; both depend only on this system's trajectory
-    const bool use_list = a.nbl != nullptr && N >= a.nbl_min && a.rc2 < 1e37f;
+    const bool use_list = a.nbl != nullptr && N >= a.nbl_min && a.rc2 < 1e37f && FORM != FORM_GATHER_PBC;
     const size_t ga0 = (size_t)st.atom_off;
     bool need_build = use_list && fresh;
     double dt = fresh ? a.fire.dt0 : st.dt, alpha = fresh ? a.fire.alpha0 : st.alpha;
@@ -863,7 +1002,7 @@ __device__ void run_system(const KernelArgs& a, const Smem& S, int w, int rank) 
             if (need_build || nblist_stale<T>(a, S, N, ga0, rank)) build_nblist<T>(a, S, N, ga0, rank);
             need_build = false;
         }
-        eval_forces<T, GDT, EVAL, FORM>(a, S, tpp, N, rank, acc, use_list, ga0);
+        eval_forces<T, GDT, EVAL, FORM>(a, S, tpp, N, rank, acc, lat, use_list, ga0);
         ran = 1;
         const double dt_old = dt;
         const float dtf = (float)dt_old;
@@ -1011,7 +1150,7 @@ int launch_team(const KernelArgs& a, int team, cudaStream_t s, int num_sms) {
     if (a.gscratch) {
         // global-state launches exist for the gather form with 128-512 threads (the host sends
         // every system too large for shared memory there)
-        if constexpr (FORM == FORM_GATHER) {
+        if constexpr (FORM == FORM_GATHER || FORM == FORM_GATHER_PBC) {
             switch (team) {
                 case 128: return launch_t<128, GDT, EVAL, FORM, true>(a, s, num_sms);
                 case 256: return launch_t<256, GDT, EVAL, FORM, true>(a, s, num_sms);
@@ -1066,9 +1205,11 @@ int launch_relax(const KernelArgs& a, int team, int form, int eval_only, cudaStr
     int r;
     if (eval_only) r = form == FORM_GATHER ? launch_dtype<true, FORM_GATHER>(a, team, s, num_sms)
                      : form == FORM_OWNER ? launch_dtype<true, FORM_OWNER>(a, team, s, num_sms)
+                     : form == FORM_GATHER_PBC ? launch_dtype<true, FORM_GATHER_PBC>(a, team, s, num_sms)
                                           : launch_dtype<true, FORM_ROUNDS>(a, team, s, num_sms);
     else r = form == FORM_GATHER ? launch_dtype<false, FORM_GATHER>(a, team, s, num_sms)
            : form == FORM_OWNER ? launch_dtype<false, FORM_OWNER>(a, team, s, num_sms)
+           : form == FORM_GATHER_PBC ? launch_dtype<false, FORM_GATHER_PBC>(a, team, s, num_sms)
                                 : launch_dtype<false, FORM_ROUNDS>(a, team, s, num_sms);
     if (launches && r == 0) (*launches)++;
     return r;

@@ -46,7 +46,8 @@ struct TopoDev {
     // off + r * natoms + o, so a warp's lanes read consecutive records.
     int own_a_off, own_i_off, own_d_off;   // into the owner record arenas (geo + par)
     int own_ok;                   // 0: the topology cannot run the owner form (rounds instead)
-    int pad[3];
+    int pbc_bonds;                // 1: some bonds reach a neighbour's image in another cell (cell codes in neighc)
+    int pad[2];
 };
 static_assert(sizeof(TopoDev) == 96, "TopoDev size");
 
@@ -62,7 +63,7 @@ struct SlotState {
     double dt, alpha;             // FIRE adaptive state
     double energy;                // total physical energy at the last force evaluation
     float fmax;                   // max |F| at the last force evaluation
-    float pad1;
+    int pbc;                      // 1: the slot has a lattice (KernelArgs::lat) for bond shifts / NB images
 };
 
 enum GridDtype { GRID_F32 = 0, GRID_F16 = 1, GRID_BF16 = 2 };
@@ -99,6 +100,10 @@ struct KernelArgs {
     SlotState* slots;
     const TopoDev* topos;
     const float4* req; const short4* neigh; const float4* bk; const float4* bl;
+    // periodic molecules: per atom the cell code of each bond slot's partner image (4-bit
+    // two's-complement lattice offsets x | y << 4 | z << 8; 0 = same cell), and per slot the
+    // lattice: lat[3 s + k] = (vector k, number of images each side along it)
+    const short4* neighc; const float4* lat;
     const AngRec* angs; const DihRec* dihs; const InvRec* invs;
     float4* pos; float4* plo; float4* vel; float4* force;
     GridView grid; int has_grid;
@@ -143,7 +148,16 @@ struct HostTopo {
     std::vector<double> req;                          // 4n
     std::vector<double> bond_kl;                      // 8n: (k, l0) per neighbour slot
     std::vector<int> type_id;                         // n
+    // periodic molecules: per neighbour slot the cell code of the partner's image (4n, empty for
+    // molecules without periodic bonds), the lattice the molecule was built in and its images
+    std::vector<int> neighc;
+    double lattice[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    int npbc[3] = {0, 0, 0};
 };
+
+// cell code of a lattice offset (each component in [-8, 7]) and its components
+inline int cell_code(int ox, int oy, int oz) { return (ox & 15) | ((oy & 15) << 4) | ((oz & 15) << 8); }
+inline int cell_field(int c, int k) { int v = (c >> (4 * k)) & 15; return v >= 8 ? v - 16 : v; }
 
 struct PackedTerms {
     std::vector<AngRec> ang; std::vector<DihRec> dih; std::vector<InvRec> inv;
@@ -176,11 +190,15 @@ void flat_terms(const HostTopo& T, FlatTerms& out);
 bool owner_terms(const HostTopo& T, OwnerTerms& out);
 const char* type_name(int id);
 int type_id_of(const char* name);
+int build_molecule_topology_pbc(int n, const int* Z, const double* pos, const double* q, double bond_cut,
+                                const double lvec[9], HostTopo& T, char* err, int errlen);
 int build_listed_topology(int n, const int* Z, const int* type_ids, const double* q, int nb, const int* bonds, int na,
                           const int* angs, int nd, const int* dihs, int ni, const int* invs, HostTopo& T, char* err, int errlen);
 
 // relax.cu
-enum KernelForm { FORM_ROUNDS = 0, FORM_GATHER = 1, FORM_OWNER = 2 };
+// FORM_GATHER_PBC: the gather form with the periodic-system code (bond shifts, NB image sums)
+// compiled in; the host sends every system with a lattice there, so the other forms carry none of it
+enum KernelForm { FORM_ROUNDS = 0, FORM_GATHER = 1, FORM_OWNER = 2, FORM_GATHER_PBC = 3 };
 int launch_relax(const KernelArgs& a, int team, int form, int eval_only, cudaStream_t s, int num_sms, long long* launches);
 size_t team_smem_bytes(int nmax, int nfmax, int team, int form);
 

@@ -348,6 +348,84 @@ int build_molecule_topology(int n, const int* Z, const double* pos, const double
     return 0;
 }
 
+// A periodic molecule: bonds by cutoff to every image of a partner within one cell along each
+// nonzero lattice vector (lvec = a, b, c), each bond slot recording the cell of its partner's image
+// (the neighCell of opencl/UFF.cl:152, 229-236).  Typing and terms follow the bond graph as for an
+// isolated molecule; since terms are enumerated over atom indices, a cell in which an atom bonds
+// to its own image, a pair bonds in two images, or a 3-bond path returns to its first atom through
+// the images is too small and is refused.  The molecule's default images are one cell each side
+// along its periodic axes.
+int build_molecule_topology_pbc(int n, const int* Z, const double* pos, const double* q, double bond_cut,
+                                const double lvec[9], HostTopo& T, char* err, int errlen) {
+    if (n <= 0 || n > 8191) { std::snprintf(err, errlen, "natoms=%d outside [1, 8191]", n); return -1; }
+    std::vector<El> el(n);
+    for (int a = 0; a < n; a++) {
+        el[a] = el_of_Z(Z[a]);
+        if (el[a] == EL_X || !kElem[el[a]].known) { std::snprintf(err, errlen, "atom %d: element Z=%d has no UFF parameters here", a, Z[a]); return -1; }
+    }
+    int range[3];
+    for (int k = 0; k < 3; k++) range[k] = (lvec[3 * k] != 0 || lvec[3 * k + 1] != 0 || lvec[3 * k + 2] != 0) ? 1 : 0;
+    if (!range[0] && !range[1] && !range[2]) { std::snprintf(err, errlen, "all three lattice vectors are zero"); return -1; }
+    T = HostTopo();
+    T.n = n;
+    for (int k = 0; k < 9; k++) T.lattice[k] = lvec[k];
+    for (int k = 0; k < 3; k++) T.npbc[k] = range[k];
+    const double rc2 = bond_cut * bond_cut;
+    std::vector<int> off;                              // per bond: cell code of atom 1's image seen from atom 0
+    for (int i = 0; i < n; i++)
+        for (int j = i; j < n; j++) {
+            int found = 0;
+            for (int oz = -range[2]; oz <= range[2]; oz++)
+                for (int oy = -range[1]; oy <= range[1]; oy++)
+                    for (int ox = -range[0]; ox <= range[0]; ox++) {
+                        if (i == j && !ox && !oy && !oz) continue;
+                        double d[3];
+                        for (int c = 0; c < 3; c++) d[c] = pos[3 * j + c] - pos[3 * i + c] + ox * lvec[c] + oy * lvec[3 + c] + oz * lvec[6 + c];
+                        if (d[0] * d[0] + d[1] * d[1] + d[2] * d[2] >= rc2) continue;
+                        if (i == j) { std::snprintf(err, errlen, "atom %d bonds to its own image: cell too small", i); return -1; }
+                        if (found++) { std::snprintf(err, errlen, "atoms %d and %d bond in two images: cell too small", i, j); return -1; }
+                        T.bonds.push_back(i); T.bonds.push_back(j);
+                        off.push_back(cell_code(ox, oy, oz));
+                    }
+        }
+    std::vector<int> deg(n, 0);
+    for (size_t k = 0; k < T.bonds.size(); k++) deg[T.bonds[k]]++;
+    for (int a = 0; a < n; a++) if (deg[a] > 4) { std::snprintf(err, errlen, "atom %d has %d bonds within the cutoff (max 4)", a, deg[a]); return -1; }
+    neighbour_slots(T);
+    T.neighc.assign(4 * (size_t)n, 0);
+    for (int a = 0; a < n; a++)
+        for (int s = 0; s < 4; s++) {
+            const int b = T.neighBs[4 * a + s];
+            if (b < 0) continue;
+            const int c = off[b], sg = T.bonds[2 * b] == a ? 1 : -1;   // offsets are seen from the bond's first atom
+            T.neighc[4 * a + s] = cell_code(sg * cell_field(c, 0), sg * cell_field(c, 1), sg * cell_field(c, 2));
+        }
+    for (int j = 0; j < n; j++)                        // 3-bond paths i-j-k-i through the images
+        for (int sj = 0; sj < 4; sj++) {
+            const int k = T.neighs[4 * j + sj];
+            if (k < 0) continue;
+            for (int si = 0; si < 4; si++) {
+                const int i = T.neighs[4 * j + si];
+                if (i < 0 || si == sj) continue;
+                for (int sk = 0; sk < 4; sk++) {
+                    if (T.neighs[4 * k + sk] != i) continue;
+                    for (int ax = 0; ax < 3; ax++)
+                        if (cell_field(T.neighc[4 * j + sj], ax) - cell_field(T.neighc[4 * j + si], ax) + cell_field(T.neighc[4 * k + sk], ax)) {
+                            std::snprintf(err, errlen, "bond path %d-%d-%d-%d closes through the images: cell too small", i, j, k, i);
+                            return -1;
+                        }
+                }
+            }
+        }
+    assign_types(n, el, T.neighs, T.type_id);
+    enumerate_terms(T);
+    if (!check_slots(T, err, errlen)) return -1;
+    uff_parameters(T);
+    if (q) for (int a = 0; a < n; a++) T.req[4 * a + 2] = q[a];
+    fill_bond_kl(T);
+    return 0;
+}
+
 // A molecule whose bonds and angle / dihedral / inversion lists come from a file (the reference's
 // TopologyData JSON or UFFTOPO binary, crates/libs/moltopo/src/export.rs:12-74,
 // crates/apps/buildff/src/main.rs:10-28): the lists are taken as they are, as Uff::from_topology

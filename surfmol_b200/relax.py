@@ -317,6 +317,53 @@ class RelaxMulti:
         self.topo_n.append(len(Z))
         return tid.value
 
+    def add_molecule_pbc(self, Z, pos, lattice, charges=None, bond_cut=1.8, npbc=None) -> int:
+        """A periodic molecule: ``lattice`` (3, 3) rows a, b, c (zero rows: non-periodic axes); bonds
+        may reach a partner's image in the next cell.  ``npbc``: NB images each side per axis for the
+        systems made from it (default 1 along the periodic axes)."""
+        Z = _i(Z)
+        pos = _d(pos)
+        q = _d(charges) if charges is not None else None
+        lat = _d(np.asarray(lattice, float).reshape(9))
+        nimg = _i(npbc) if npbc is not None else None
+        tid = C.c_int()
+        self._chk(self.L.smr_add_molecule_pbc(self.h, len(Z), _p(Z, N.IP), _p(pos, N.DP), _p(q, N.DP), bond_cut,
+                                              _p(lat, N.DP), _p(nimg, N.IP), C.byref(tid)), "smr_add_molecule_pbc")
+        self.topo_n.append(len(Z))
+        return tid.value
+
+    def set_pbc(self, slots, lattice, npbc):
+        """Per-system lattice ((3, 3) or one per slot) and NB images each side ((3,) or one per slot)."""
+        slots = _i(slots)
+        n = len(slots)
+        lat = _d(np.broadcast_to(np.asarray(lattice, float).reshape(-1, 9), (n, 9)))
+        nimg = _i(np.broadcast_to(np.asarray(npbc).reshape(-1, 3), (n, 3)))
+        self._chk(self.L.smr_set_pbc(self.h, n, _p(slots, N.IP), _p(lat, N.DP), _p(nimg, N.IP)), "smr_set_pbc")
+
+    def get_pbc(self, slot):
+        lat = np.zeros(9)
+        nimg = np.zeros(3, np.int32)
+        self._chk(self.L.smr_get_pbc(self.h, int(slot), _p(lat, N.DP), _p(nimg, N.IP)), "smr_get_pbc")
+        return lat.reshape(3, 3), nimg
+
+    def topology_counts(self, topo_id):
+        """(natoms, nbonds, nang, ndih, ninv, type-rounds) of a topology on the handle."""
+        c = (C.c_int * 6)()
+        self._chk(self.L.smr_topology_counts(self.h, int(topo_id), c), "smr_topology_counts")
+        return list(c)
+
+    def topology_export(self, topo_id):
+        """The topology's lists and parameters, as Topology.export."""
+        out = _export_arrays(self.topology_counts(topo_id)[:5])
+        self._chk(self.L.smr_topology_export(self.h, int(topo_id), *_export_ptrs(out)), "smr_topology_export")
+        return out
+
+    def topology_cells(self, topo_id):
+        """Cell code of each neighbour slot (natoms, 4)."""
+        out = np.zeros((self.topo_n[topo_id], 4), np.int32)
+        self._chk(self.L.smr_topology_cells(self.h, int(topo_id), _p(out, N.IP)), "smr_topology_cells")
+        return out
+
     def add_molecules(self, Zs, poss, charges=None, bond_cut=1.8):
         """Many molecules at once (typing and packing on all host cores); returns their topology ids."""
         n = _i([len(z) for z in Zs])

@@ -159,6 +159,24 @@ def ragged_molecule(rng, target: int) -> Molecule:
     raise RuntimeError("could not generate a ragged molecule")
 
 
+def polyacene_ribbon(ncell: int, cc: float = 1.40, ch: float = 1.08):
+    """A periodic polyacene ribbon along x: ``ncell`` repeats of C4H2 (a rung of two carbons and
+    the two apex CH of the next ring), period ``cc * sqrt(3)``.  Returns (Molecule, lattice (3, 3))
+    with lattice a = (ncell * period, 0, 0) and b = c = 0 (non-periodic)."""
+    per = cc * math.sqrt(3.0)
+    Z, P = [], []
+    for k in range(ncell):
+        x0 = k * per
+        Z += [6, 6, 6, 6, 1, 1]
+        P += [(x0, 0.5 * cc, 0.0), (x0, -0.5 * cc, 0.0), (x0 + 0.5 * per, cc, 0.0), (x0 + 0.5 * per, -cc, 0.0),
+              (x0 + 0.5 * per, cc + ch, 0.0), (x0 + 0.5 * per, -cc - ch, 0.0)]
+    P = np.array(P)
+    P -= P.mean(0)
+    lat = np.zeros((3, 3))
+    lat[0, 0] = ncell * per
+    return Molecule(np.array(Z, np.int32), P), lat
+
+
 def charges(rng, n: int, sigma: float = 0.15) -> np.ndarray:
     q = rng.normal(0.0, sigma, n)
     return q - q.mean()
