@@ -209,6 +209,14 @@ int smr_add_molecule_pbc(smr_handle* h, int natoms, const int* Z, const double* 
 int smr_set_pbc(smr_handle* h, int nsys, const int* slot_ids, const double* lvec, const int* npbc);
 int smr_get_pbc(smr_handle* h, int slot, double lvec[9], int npbc[3]);
 int smr_topology_cells(smr_handle* h, int topo_id, int* cells);
+/* Position constraints: the constr / constrK springs of updateAtomsMMFFf4 (opencl/UFF.cl:974-982).
+ * For n listed atoms (indices within the system) a target (x, y, z) and per-axis stiffness
+ * (kx, ky, kz in eV/A^2; negative counts as 0): the force (target - position) * k is added after
+ * the force limit and drives FIRE (its power, norms and the max|F| convergence test), but is not
+ * part of the returned forces or energies, as the reference stores the force before it.  A call
+ * replaces the system's constraints; n = 0 removes them.  Constrained systems run in the
+ * extended gather form. */
+int smr_set_constraints(smr_handle* h, int slot, int n, const int* atoms, const double* target, const double* k);
 /* counts[6] = natoms, nbonds, nang, ndih, ninv, type-rounds (schedule length) */
 int smr_topology_counts(smr_handle* h, int topo_id, int counts[6]);
 /* Any output pointer may be null.  Layouts as the arrays of smr_topology_desc plus

@@ -98,6 +98,7 @@ struct smr_handle {
     // per slot: lattice vectors with the images each side in w (3 float4), for slots with pbc set
     std::vector<float4> hlat;
     DArr<float4> dlat;
+    DArr<float4> dcons;                 // per state atom 2 float4: constraint target (+ on) and stiffness
     DArr<AngRec> dang; DArr<DihRec> ddih; DArr<InvRec> dinv;
     std::vector<int2> ha2f; std::vector<int> hidx;      // gather form: per atom (start, count), piece indices
     DArr<int2> da2f; DArr<int> didx;
@@ -429,7 +430,7 @@ KernelArgs base_args(smr_handle* h) {
     a.slots = h->slots;
     a.topos = h->dtd.d;
     a.req = h->dreq.d; a.neigh = h->dneigh.d; a.bk = h->dbk.d; a.bl = h->dbl.d;
-    a.neighc = h->dneighc.d; a.lat = h->dlat.d;
+    a.neighc = h->dneighc.d; a.lat = h->dlat.d; a.cons = h->dcons.d;
     a.angs = h->dang.d; a.dihs = h->ddih.d; a.invs = h->dinv.d;
     a.a2f = h->da2f.d; a.a2f_idx = h->didx.d;
     a.own_geo = h->down_geo.d; a.own_par = h->down_par.d; a.own_meta = h->down_meta.d;
@@ -470,8 +471,8 @@ int latency_team_for(int requested, int n) {
 
 // Launch segments for a list of slots.  The form of every system is decided from the system
 // alone (the requested form when the topology supports it and its own shared memory fits, else
-// the rounds form with its topology's team; systems with a lattice always the gather form with
-// the periodic code), never from what it is batched with; segments group
+// the rounds form with its topology's team; periodic or constrained systems always the extended
+// gather form), never from what it is batched with; segments group
 // equal (form, team) and are split wherever the segment's largest system would no longer fit.
 std::vector<Seg> group_by(smr_handle* h, std::vector<int>& ids, int form, int req_team = 0) {
     struct Key { int form, team, n, nf; };
@@ -479,11 +480,11 @@ std::vector<Seg> group_by(smr_handle* h, std::vector<int>& ids, int form, int re
         const SlotState& st = h->hs[s];
         const TopoDev& td = h->htd[st.topo];
         const int n = st.natoms, nf = td.npieces;
-        if (st.pbc) {
-            // periodic systems: the gather form with the PBC code, whatever the stage's form
+        if (st.flags) {
+            // periodic or constrained systems: the extended gather form, whatever the stage's form
             const int t = req_team ? req_team : td.team;
-            if (team_smem_bytes(n, nf, t, FORM_GATHER_PBC) <= h->smem_optin) return Key{FORM_GATHER_PBC, t, n, nf};
-            return Key{FORM_GATHER_PBC, std::max(td.team, n > 1024 ? 512 : 256), n, nf};
+            if (team_smem_bytes(n, nf, t, FORM_GATHER_EXT) <= h->smem_optin) return Key{FORM_GATHER_EXT, t, n, nf};
+            return Key{FORM_GATHER_EXT, std::max(td.team, n > 1024 ? 512 : 256), n, nf};
         }
         if (form == FORM_GATHER) {
             const int t = latency_team_for(req_team, n);
@@ -932,7 +933,7 @@ static void set_slot_lattice(smr_handle* h, int s, const double* lvec, const int
         h->hlat[3 * (size_t)s + k] = make_float4((float)lvec[3 * k], (float)lvec[3 * k + 1], (float)lvec[3 * k + 2], (float)npbc[k]);
         on = on || npbc[k] > 0;
     }
-    h->hs[s].pbc = on ? 1 : 0;
+    h->hs[s].flags = on ? (h->hs[s].flags | SLOT_PBC) : (h->hs[s].flags & ~SLOT_PBC);
 }
 
 int smr_set_pbc(smr_handle* h, int nsys, const int* slot_ids, const double* lvec, const int* npbc) {
@@ -957,13 +958,40 @@ int smr_set_pbc(smr_handle* h, int nsys, const int* slot_ids, const double* lvec
     return upload_slots(h, ids);
 }
 
+int smr_set_constraints(smr_handle* h, int slot, int n, const int* atoms, const double* target, const double* k) {
+    if (!h || n < 0 || (n && (!atoms || !target || !k))) return SMR_ERR_ARG;
+    SETTLE(h);
+    if (!valid_slot(h, slot)) return fail(h, SMR_ERR_ARG, "slot %d not active", slot);
+    SlotState& st = h->hs[slot];
+    std::vector<float4> c(2 * (size_t)st.natoms, make_float4(0.f, 0.f, 0.f, 0.f));
+    for (int i = 0; i < n; i++) {
+        const int a = atoms[i];
+        if (a < 0 || a >= st.natoms) return fail(h, SMR_ERR_ARG, "constraint %d: atom %d outside [0, %d)", i, a, st.natoms);
+        for (int d = 0; d < 3; d++)
+            if (!std::isfinite(target[3 * i + d]) || !std::isfinite(k[3 * i + d])) return fail(h, SMR_ERR_ARG, "constraint %d: non-finite value", i);
+        c[2 * a] = make_float4((float)target[3 * i], (float)target[3 * i + 1], (float)target[3 * i + 2], 1.f);
+        c[2 * a + 1] = make_float4((float)k[3 * i], (float)k[3 * i + 1], (float)k[3 * i + 2], 0.f);
+    }
+    if (n) {
+        if (!h->dcons.d) {
+            CU(h, h->dcons.reserve(2 * (size_t)h->max_atoms, 0, h->stream));
+            CU(h, cudaMemsetAsync(h->dcons.d, 0, 2 * (size_t)h->max_atoms * 16, h->stream));
+        }
+        CU(h, cudaMemcpyAsync(h->dcons.d + 2 * (size_t)st.atom_off, c.data(), c.size() * 16, cudaMemcpyHostToDevice, h->stream));
+        st.flags |= SLOT_CONS;
+    } else {
+        st.flags &= ~SLOT_CONS;
+    }
+    return upload_slots(h, {slot});                    // waits, so c may go
+}
+
 int smr_get_pbc(smr_handle* h, int slot, double lvec[9], int npbc[3]) {
     if (!h || !lvec || !npbc) return SMR_ERR_ARG;
     SETTLE(h);
     if (!valid_slot(h, slot)) return fail(h, SMR_ERR_ARG, "slot %d not active", slot);
     for (int k = 0; k < 3; k++) {
         const float4 v = h->hlat[3 * (size_t)slot + k];
-        const bool on = h->hs[slot].pbc != 0;
+        const bool on = (h->hs[slot].flags & SLOT_PBC) != 0;
         lvec[3 * k] = on ? v.x : 0.0; lvec[3 * k + 1] = on ? v.y : 0.0; lvec[3 * k + 2] = on ? v.z : 0.0;
         npbc[k] = on ? (int)v.w : 0;
     }
@@ -1311,7 +1339,7 @@ static void sig_args(std::vector<long long>& v, const KernelArgs& a) {
     v.push_back(a.phase_limit); v.push_back(a.step_budget); P(a.ecomp); v.push_back(a.nmax); v.push_back(a.nfmax);
     P(a.a2f); P(a.a2f_idx); P(a.own_geo); P(a.own_par); P(a.own_meta); v.push_back(a.nb_lanes);
     P(a.gscratch); v.push_back((long long)a.gscratch_bytes);
-    P(a.neighc); P(a.lat);
+    P(a.neighc); P(a.lat); P(a.cons);
     P(a.nbl); P(a.nbl_cnt); P(a.nbl_ref); v.push_back(a.nbl_cap); v.push_back(a.nbl_min); F(a.nbl_skin);
     v.push_back(a.fold.on); v.push_back(a.fold.nx); v.push_back(a.fold.ny); v.push_back(a.fold.nz);
     for (int k = 0; k < 4; k++) { F(a.fold.inv[k]); F(a.fold.inv_lo[k]); }

@@ -53,7 +53,7 @@ __host__ __device__ inline size_t red_bytes(int T) { return T > 32 ? size_t(T / 
 __host__ __device__ inline size_t team_bytes(int nmax, int nfmax, int T, int form) {
     size_t n = (size_t)nmax;
     return n * 16 * 5 + n * 64 + align16(n * 4) + align16(n * 8) + red_bytes(T) +
-           (form == FORM_GATHER || form == FORM_GATHER_PBC ? (size_t)nfmax * 16 : 0) + (form == FORM_OWNER ? n * 64 : 0);
+           (form == FORM_GATHER || form == FORM_GATHER_EXT ? (size_t)nfmax * 16 : 0) + (form == FORM_OWNER ? n * 64 : 0);
 }
 
 // Shared memory of one team: one base pointer and the capacity; every array's address is
@@ -331,6 +331,16 @@ __device__ __forceinline__ float bonds_atom_pbc(Smem S, const float4* bk_, const
     return E;
 }
 
+// Position constraint of one atom (the constr / constrK springs of updateAtomsMMFFf4,
+// opencl/UFF.cl:974-982): (target - position) * max(k, 0) when the atom has one.
+__device__ __forceinline__ float3 constraint_force(const float4* cons, size_t g, float4 p, float4 lo) {
+    const float4 c = __ldg(cons + 2 * g);
+    if (!(c.w > 0.f)) return make_float3(0.f, 0.f, 0.f);
+    const float4 k = __ldg(cons + 2 * g + 1);
+    return make_float3(((c.x - p.x) - lo.x) * fmaxf(k.x, 0.f), ((c.y - p.y) - lo.y) * fmaxf(k.y, 0.f),
+                       ((c.z - p.z) - lo.z) * fmaxf(k.z, 0.f));
+}
+
 // beyond_cutoff_fp64 for a partner image shifted by s
 __device__ __noinline__ bool beyond_cutoff_fp64_shift(float4 pi, float4 li, float4 pj, float4 lj, float sx, float sy, float sz, float rc2) {
     const double dx = ((double)pj.x - (double)pi.x) + ((double)lj.x - (double)li.x) + (double)sx;
@@ -486,9 +496,9 @@ template <int T, int GDT, bool EVAL, int FORM>
 __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* __restrict__ tpp, int N, int rank, EAcc<EVAL>& acc,
                             const float4* lat, bool use_list = false, size_t ga0 = 0) {
 #define TP(f) __ldg(&tpp->f)
-    // periodic systems (lat: the slot's lattice rows) run in FORM_GATHER_PBC, the gather form plus
+    // periodic systems (lat: the slot's lattice rows) run in FORM_GATHER_EXT, the gather form plus
     // bonds to a partner's image in another cell (neighCell, UFF.cl:229-236) and NB image sums
-    constexpr bool PBC = FORM == FORM_GATHER_PBC;
+    constexpr bool PBC = FORM == FORM_GATHER_EXT;
     constexpr int BF = PBC ? FORM_GATHER : FORM;
     const bool pbc_bonds = PBC && lat != nullptr && TP(pbc_bonds) != 0;
     // A: bonds and hneigh, one atom per rank (opencl/UFF.cl:141-322)
@@ -969,7 +979,7 @@ __device__ void run_system(const KernelArgs& a, const Smem& S, int w, int rank) 
     team_sync<T>();
 
     EAcc<EVAL> acc;
-    const float4* lat = st.pbc ? a.lat + 3 * (size_t)slot : nullptr;
+    const float4* lat = (st.flags & SLOT_PBC) ? a.lat + 3 * (size_t)slot : nullptr;
     if (EVAL) {
         eval_forces<T, GDT, EVAL, FORM>(a, S, tpp, N, rank, acc, lat);
         for (int i = rank; i < N; i += T) a.force[st.atom_off + i] = S.F()[i];
@@ -989,13 +999,16 @@ __device__ void run_system(const KernelArgs& a, const Smem& S, int w, int rank) 
 
     // neighbour list: rebuilt on the first step after positions were set (fresh FIRE state) and
     // whenever an atom has moved more than skin / 2; both depend only on this system's trajectory
-    const bool use_list = a.nbl != nullptr && N >= a.nbl_min && a.rc2 < 1e37f && FORM != FORM_GATHER_PBC;
+    const bool use_list = a.nbl != nullptr && N >= a.nbl_min && a.rc2 < 1e37f && FORM != FORM_GATHER_EXT;
     const size_t ga0 = (size_t)st.atom_off;
     bool need_build = use_list && fresh;
     double dt = fresh ? a.fire.dt0 : st.dt, alpha = fresh ? a.fire.alpha0 : st.alpha;
     int npos = fresh ? 0 : st.npos, status = st.status;
     float fmax = st.fmax;
     const float flim = (float)a.fire.flimit, flim2 = flim * flim;
+    // constraint springs (extended form only): added after the force limit, they drive FIRE but
+    // are not stored with the forces, as updateAtomsMMFFf4 stores the force before them
+    const bool cons_on = FORM == FORM_GATHER_EXT && (st.flags & SLOT_CONS) != 0;
     int ran = 0;
     for (int it = 0; it < nsteps; it++) {
         if (use_list) {
@@ -1015,6 +1028,11 @@ __device__ void run_system(const KernelArgs& a, const Smem& S, int w, int rank) 
                 const float s = flim / sqrtf(f2);
                 f.x *= s; f.y *= s; f.z *= s;
                 S.F()[i] = f;
+                f2 = f.x * f.x + f.y * f.y + f.z * f.z;
+            }
+            if (cons_on) {
+                const float3 fc = constraint_force(a.cons, ga0 + i, S.P()[i], S.Lo()[i]);
+                f.x += fc.x; f.y += fc.y; f.z += fc.z;
                 f2 = f.x * f.x + f.y * f.y + f.z * f.z;
             }
             f2m = fmaxf(f2m, f2);
@@ -1039,7 +1057,11 @@ __device__ void run_system(const KernelArgs& a, const Smem& S, int w, int rank) 
         for (int i = rank; i < N; i += T) {
             float4 v = S.V()[i];
             if (mix) {
-                const float4 f = S.F()[i];
+                float4 f = S.F()[i];
+                if (cons_on) {
+                    const float3 fc = constraint_force(a.cons, ga0 + i, S.P()[i], S.Lo()[i]);
+                    f.x += fc.x; f.y += fc.y; f.z += fc.z;
+                }
                 v.x = v.x * cv + f.x * cf; v.y = v.y * cv + f.y * cf; v.z = v.z * cv + f.z * cf;
             } else {
                 v = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -1150,7 +1172,7 @@ int launch_team(const KernelArgs& a, int team, cudaStream_t s, int num_sms) {
     if (a.gscratch) {
         // global-state launches exist for the gather form with 128-512 threads (the host sends
         // every system too large for shared memory there)
-        if constexpr (FORM == FORM_GATHER || FORM == FORM_GATHER_PBC) {
+        if constexpr (FORM == FORM_GATHER || FORM == FORM_GATHER_EXT) {
             switch (team) {
                 case 128: return launch_t<128, GDT, EVAL, FORM, true>(a, s, num_sms);
                 case 256: return launch_t<256, GDT, EVAL, FORM, true>(a, s, num_sms);
@@ -1205,11 +1227,11 @@ int launch_relax(const KernelArgs& a, int team, int form, int eval_only, cudaStr
     int r;
     if (eval_only) r = form == FORM_GATHER ? launch_dtype<true, FORM_GATHER>(a, team, s, num_sms)
                      : form == FORM_OWNER ? launch_dtype<true, FORM_OWNER>(a, team, s, num_sms)
-                     : form == FORM_GATHER_PBC ? launch_dtype<true, FORM_GATHER_PBC>(a, team, s, num_sms)
+                     : form == FORM_GATHER_EXT ? launch_dtype<true, FORM_GATHER_EXT>(a, team, s, num_sms)
                                           : launch_dtype<true, FORM_ROUNDS>(a, team, s, num_sms);
     else r = form == FORM_GATHER ? launch_dtype<false, FORM_GATHER>(a, team, s, num_sms)
            : form == FORM_OWNER ? launch_dtype<false, FORM_OWNER>(a, team, s, num_sms)
-           : form == FORM_GATHER_PBC ? launch_dtype<false, FORM_GATHER_PBC>(a, team, s, num_sms)
+           : form == FORM_GATHER_EXT ? launch_dtype<false, FORM_GATHER_EXT>(a, team, s, num_sms)
                                 : launch_dtype<false, FORM_ROUNDS>(a, team, s, num_sms);
     if (launches && r == 0) (*launches)++;
     return r;

@@ -346,6 +346,17 @@ class RelaxMulti:
         self._chk(self.L.smr_get_pbc(self.h, int(slot), _p(lat, N.DP), _p(nimg, N.IP)), "smr_get_pbc")
         return lat.reshape(3, 3), nimg
 
+    def set_constraints(self, slot, atoms=(), target=None, k=None):
+        """Harmonic position constraints of one system: atoms (n,), target (n, 3) positions, k (n, 3)
+        or (n,) or scalar stiffness per axis (eV/A^2).  No atoms: remove them."""
+        atoms = _i(np.ravel(atoms))
+        n = len(atoms)
+        tgt = _d(np.asarray(target if n else np.zeros((0, 3)), float).reshape(n, 3))
+        kk = np.asarray(k if n else 0.0, float)
+        kk = _d(np.broadcast_to(kk.reshape(-1, 1) if kk.ndim == 1 else kk, (n, 3)))
+        self._chk(self.L.smr_set_constraints(self.h, int(slot), n, _p(atoms, N.IP), _p(tgt, N.DP), _p(kk, N.DP)),
+                  "smr_set_constraints")
+
     def topology_counts(self, topo_id):
         """(natoms, nbonds, nang, ndih, ninv, type-rounds) of a topology on the handle."""
         c = (C.c_int * 6)()
