@@ -975,6 +975,136 @@ int orc_folded_points(const orc_folded* f, int n, const double* pos, const doubl
     return 0;
 }
 
+// ------------------------------------------------------------------ RAFF multi-replica step (FP64)
+// One step per replica as compute_collision_multi, compute_ports_current_multi and
+// apply_corrections_multi (opencl/RRsp3.cl:1774-2048, massless_rot = 0), each pass over the
+// positions of the step's start.  cfg = (dt, relaxation, momentum_beta, rot_mass_scale).
+// Per replica and atom: pos (x, y, z, inverse mass), quat (x, y, z, w), momenta dmom / dqmom (4
+// each); coll_out (3 per atom) and dnode_out (3 per node) receive the last step's corrections.
+namespace {
+struct Q4d { double x, y, z, w; };
+inline Q4d qmul(Q4d a, Q4d b) {
+    return {a.w * b.x + a.x * b.w + a.y * b.z - a.z * b.y, a.w * b.y - a.x * b.z + a.y * b.w + a.z * b.x,
+            a.w * b.z + a.x * b.y - a.y * b.x + a.z * b.w, a.w * b.w - a.x * b.x - a.y * b.y - a.z * b.z};
+}
+inline Q4d qnorm(Q4d q) {
+    const double n2 = q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w;
+    if (n2 < 1e-16) return {0, 0, 0, 1};
+    const double s = 1.0 / std::sqrt(n2);
+    return {q.x * s, q.y * s, q.z * s, q.w * s};
+}
+inline V3 qrot(Q4d q, V3 v) {   // v + w t + u x t, t = 2 u x v
+    const V3 u{q.x, q.y, q.z};
+    const V3 t = cross(u, v) * 2.0;
+    return v + t * q.w + cross(u, t);
+}
+}  // namespace
+
+int orc_raff_step(int n, int nn, int nsys, int nsteps, const double* cfg, int collide, const double* radius, const int* neighs,
+                  const int* excl1, const int* excl2, const int* fixmask, const double* port_local, const double* kport,
+                  const int* bk, double* pos, double* quat, double* dmom, double* dqmom, double* coll_out, double* dnode_out) {
+    const double dt = cfg[0], relax = cfg[1], beta = cfg[2], rms = cfg[3];
+    std::vector<V3> C(n), DN(nn), DR(nn), DG(4 * (size_t)nn);
+    for (int r = 0; r < nsys; r++) {
+        double* P = pos + 4 * (size_t)r * n; double* Q = quat + 4 * (size_t)r * n;
+        double* M = dmom + 4 * (size_t)r * n; double* MQ = dqmom + 4 * (size_t)r * n;
+        auto p3 = [&](int i) { return V3{P[4 * i], P[4 * i + 1], P[4 * i + 2]}; };
+        for (int it = 0; it < nsteps; it++) {
+            for (int i = 0; i < n; i++) {                  // collisions (RRsp3.cl:1776-1832)
+                C[i] = {0, 0, 0};
+                if (!collide) continue;
+                const double invMi = P[4 * i + 3], ri = radius[i];
+                if (!(invMi > 1e-12) || !(ri > 0)) continue;
+                for (int j = 0; j < n; j++) {
+                    if (j == i) continue;
+                    bool ex = false;
+                    for (int k = 0; k < 4; k++) ex = ex || excl1[4 * i + k] == j || excl2[4 * i + k] == j;
+                    if (ex) continue;
+                    const double invMj = P[4 * j + 3], rj = radius[j];
+                    if (!(invMj > 1e-12) || !(rj > 0)) continue;
+                    const V3 d = p3(i) - p3(j);
+                    const double d2 = dot(d, d), rs = ri + rj;
+                    if (d2 < rs * rs && d2 > 1e-16) {
+                        const double dist = std::sqrt(d2);
+                        const double dl = 0.5 * (rs - dist) / (invMi + invMj + 1e-12);
+                        C[i] = C[i] + d * (dl * invMi / dist);
+                    }
+                }
+            }
+            for (int i = 0; i < nn && i < n; i++) {        // ports (RRsp3.cl:1837-1934)
+                const double invMi = P[4 * i + 3];
+                DN[i] = DR[i] = {0, 0, 0};
+                for (int k = 0; k < 4; k++) DG[4 * i + k] = {0, 0, 0};
+                if (!(invMi > 1e-12)) continue;
+                const Q4d qi{Q[4 * i], Q[4 * i + 1], Q[4 * i + 2], Q[4 * i + 3]};
+                const double invI = rms / (0.4 / invMi + 1e-12), dt2 = dt * dt + 1e-16;
+                for (int k = 0; k < 4; k++) {
+                    const int j = neighs[4 * i + k];
+                    if (j < 0 || j >= n) continue;
+                    const double K = kport[4 * i + k];
+                    if (!(K > 0)) continue;
+                    const double invMj = P[4 * j + 3];
+                    if (!(invMj > 1e-12)) continue;
+                    const double* pl = port_local + 4 * (4 * i + k);
+                    const V3 r_arm = qrot(qi, V3{pl[0], pl[1], pl[2]});
+                    const V3 diff = p3(j) - (p3(i) + r_arm);
+                    const double dist2 = dot(diff, diff);
+                    if (dist2 < 1e-16) continue;
+                    const double dist = std::sqrt(dist2);
+                    const V3 nv = diff * (1.0 / dist);
+                    const V3 rxn = cross(r_arm, nv);
+                    const double w_ang = dot(rxn, rxn) * invI;
+                    const bool jnode = j < nn;
+                    double w_total = invMi + invMj + w_ang + 1.0 / (K * dt2) + 1e-12;
+                    if (jnode) w_total += w_ang;
+                    double imp = dist / w_total;
+                    if (jnode) imp *= 0.5;
+                    const V3 Pv = nv * imp;
+                    DN[i] = DN[i] + Pv * invMi;
+                    DR[i] = DR[i] + cross(r_arm, Pv) * invI;
+                    DG[4 * i + k] = Pv * (-invMj);
+                }
+            }
+            for (int i = 0; i < n; i++) {                  // corrections (RRsp3.cl:1939-2046)
+                if (!(P[4 * i + 3] > 1e-12)) continue;
+                const bool isnode = i < nn;
+                V3 dx_port{0, 0, 0};
+                if (isnode) dx_port = dx_port + DN[i];
+                for (int k = 0; k < 4; k++) { const int sl = bk[4 * i + k]; if (sl >= 0) dx_port = dx_port + DG[sl]; }
+                V3 dx = C[i] + dx_port;
+                const int msk = fixmask ? fixmask[i] : 0;
+                if (msk & 1) dx.x = 0;
+                if (msk & 2) dx.y = 0;
+                if (msk & 4) dx.z = 0;
+                V3 move = dx * relax;
+                if (beta != 0) move = move + V3{M[4 * i], M[4 * i + 1], M[4 * i + 2]} * beta;
+                if (msk & 8) { if (std::fabs(P[4 * i + 2]) > 1e-6) move.z -= P[4 * i + 2]; else move.z = 0; }
+                P[4 * i] += move.x; P[4 * i + 1] += move.y; P[4 * i + 2] += move.z;
+                M[4 * i] = move.x; M[4 * i + 1] = move.y; M[4 * i + 2] = move.z; M[4 * i + 3] = 0;
+                if (!isnode || (msk & 7)) continue;
+                const V3 dth = DR[i] * relax;
+                const double angle = std::sqrt(dot(dth, dth));
+                const Q4d qo{Q[4 * i], Q[4 * i + 1], Q[4 * i + 2], Q[4 * i + 3]};
+                Q4d q = qo;
+                if (angle > 1e-8) {
+                    const double s = std::sin(0.5 * angle), c = std::cos(0.5 * angle);
+                    q = qnorm(qmul(Q4d{dth.x / angle * s, dth.y / angle * s, dth.z / angle * s, c}, qo));
+                }
+                if (beta != 0) q = {q.x + MQ[4 * i] * beta, q.y + MQ[4 * i + 1] * beta, q.z + MQ[4 * i + 2] * beta, q.w + MQ[4 * i + 3] * beta};
+                q = qnorm(q);
+                if (q.x * qo.x + q.y * qo.y + q.z * qo.z + q.w * qo.w < 0) q = {-q.x, -q.y, -q.z, -q.w};
+                Q[4 * i] = q.x; Q[4 * i + 1] = q.y; Q[4 * i + 2] = q.z; Q[4 * i + 3] = q.w;
+                MQ[4 * i] = q.x - qo.x; MQ[4 * i + 1] = q.y - qo.y; MQ[4 * i + 2] = q.z - qo.z; MQ[4 * i + 3] = q.w - qo.w;
+            }
+        }
+        if (nsteps > 0) {
+            if (coll_out) for (int i = 0; i < n; i++) { coll_out[3 * ((size_t)r * n + i)] = C[i].x; coll_out[3 * ((size_t)r * n + i) + 1] = C[i].y; coll_out[3 * ((size_t)r * n + i) + 2] = C[i].z; }
+            if (dnode_out) for (int i = 0; i < nn; i++) { dnode_out[3 * ((size_t)r * nn + i)] = DN[i].x; dnode_out[3 * ((size_t)r * nn + i) + 1] = DN[i].y; dnode_out[3 * ((size_t)r * nn + i) + 2] = DN[i].z; }
+        }
+    }
+    return 0;
+}
+
 int orc_eval(const orc_sys* S, const double* pos, const orc_grid* g, const double* nbp, double* F, double* Ea, double* Ec) {
     std::vector<V3> P(S->n), FF(S->n);
     for (int a = 0; a < S->n; a++) P[a] = {pos[3 * a], pos[3 * a + 1], pos[3 * a + 2]};

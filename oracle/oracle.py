@@ -359,3 +359,113 @@ def build_grid_fast(ions, ion_req, Lx, Ly, nx, ny, nz, p0, step, alpha=1.5, npbc
     if r != 0:
         raise ValueError("grid must lie above the slab")
     return coef
+
+
+# ---------------------------------------------------------------------------------------------
+# RAFF multi-replica (crates/libs/oclff/src/rrsp3.rs:699-1088, opencl/RRsp3.cl:1774-2048)
+
+def raff_step(pos4, quat4, natoms, nnode, nsteps, topo, dt=0.1, relaxation=0.5, beta=0.0, rot_mass_scale=1.0,
+              dmom=None, dqmom=None):
+    """FP64 restatement of nsteps multi-replica steps.  pos4 / quat4: (nsys, natoms, 4) with the
+    inverse mass in pos4[..., 3]; topo: dict(radius, neighs, excl1, excl2, fixmask, port_local,
+    k, bk) in the reference's layouts.  Returns dict(pos, quat, dmom, dqmom, coll, dnode)."""
+    L = lib()
+    if not getattr(L, "_raff_bound", False):
+        L.orc_raff_step.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, DP, C.c_int, DP, IP, IP, IP, IP, DP, DP, IP,
+                                    DP, DP, DP, DP, DP, DP]
+        L._raff_bound = True
+    P = _d(pos4).copy()
+    nsys = P.shape[0]
+    Q = _d(quat4).copy()
+    M = np.zeros_like(P) if dmom is None else _d(dmom).copy()
+    MQ = np.zeros_like(P) if dqmom is None else _d(dqmom).copy()
+    coll = np.zeros((nsys, natoms, 3))
+    dnode = np.zeros((nsys, max(nnode, 1), 3))
+    radius = _d(topo["radius"])
+    collide = int((radius > 0).any())
+    ints = [np.ascontiguousarray(topo[k], dtype=np.int32) for k in ("neighs", "excl1", "excl2", "fixmask", "bk")]
+    cfg = _d([dt, relaxation, beta, rot_mass_scale])
+    L.orc_raff_step(natoms, nnode, nsys, nsteps, _dp(cfg), collide, _dp(radius), _ip(ints[0]), _ip(ints[1]), _ip(ints[2]),
+                    _ip(ints[3]), _dp(_d(topo["port_local"])), _dp(_d(topo["k"])), _ip(ints[4]),
+                    _dp(P), _dp(Q), _dp(M), _dp(MQ), _dp(coll), _dp(dnode))
+    return dict(pos=P, quat=Q, dmom=M, dqmom=MQ, coll=coll, dnode=dnode[:, :nnode])
+
+
+def raff_node_order(natoms, bonds):
+    """pack_molecules (crates/libs/oclff/src/pack.rs:54-116) for one molecule: nodes (bond degree > 1)
+    first, then caps, each in input order.  Returns (perm, nnode)."""
+    deg = np.zeros(natoms, int)
+    for i, j in bonds:
+        if i != j:
+            deg[i] += 1
+            deg[j] += 1
+    nodes = [i for i in range(natoms) if deg[i] > 1]
+    return np.array(nodes + [i for i in range(natoms) if deg[i] <= 1], np.int32), len(nodes)
+
+
+def raff_build_neighs(natoms, bonds):
+    """build_neighs_from_bonds (pack.rs:155-172)."""
+    ng = -np.ones((natoms, 4), np.int32)
+    deg = np.zeros(natoms, int)
+    for i, j in bonds:
+        if deg[i] >= 4 or deg[j] >= 4:
+            raise ValueError(f"atom degree > 4 at bond {i}-{j}")
+        ng[i, deg[i]] = j
+        ng[j, deg[j]] = i
+        deg[i] += 1
+        deg[j] += 1
+    return ng
+
+
+def raff_exclusions(neighs):
+    """make_exclusions_1st_2nd (pack.rs:176-212)."""
+    n = len(neighs)
+    e1 = -np.ones((n, 4), np.int32)
+    e2 = -np.ones((n, 4), np.int32)
+    for i in range(n):
+        n1 = [int(j) for j in neighs[i] if j >= 0][:4]
+        e1[i, :len(n1)] = n1
+        s2 = []
+        for j in n1:
+            for t in neighs[j]:
+                if len(s2) >= 4:
+                    break
+                t = int(t)
+                if t < 0 or t == i or t in n1 or t in s2:
+                    continue
+                s2.append(t)
+        e2[i, :len(s2)] = s2
+    return e1, e2
+
+
+def raff_bk_slots(neighs, nnode):
+    """make_bk_slots_clustered (pack.rs:218-246) for one group."""
+    n = len(neighs)
+    bk = -np.ones((n, 4), np.int32)
+    cnt = np.zeros(n, int)
+    for il in range(nnode):
+        for k in range(4):
+            ja = neighs[il, k]
+            if ja < 0:
+                continue
+            if cnt[ja] >= 4:
+                raise ValueError(f"atom {ja} has more than 4 back slots")
+            bk[ja, cnt[ja]] = 4 * il + k
+            cnt[ja] += 1
+    return bk
+
+
+def raff_ports(pos, neighs, k_stiff):
+    """make_ports_from_neighs (pack.rs:293-313), float32 as the reference."""
+    pos = np.asarray(pos, np.float32)
+    n = len(neighs)
+    pl = np.zeros((n, 4, 4), np.float32)
+    k = np.zeros((n, 4), np.float32)
+    for i in range(n):
+        for s in range(4):
+            j = neighs[i, s]
+            if j < 0:
+                continue
+            pl[i, s, :3] = pos[j] - pos[i]
+            k[i, s] = k_stiff
+    return pl, k

@@ -59,6 +59,15 @@ class SmrTopologyDesc(C.Structure):
 
 
 # name -> (restype, argtypes); every function declared in include/surfmol_relax.h
+
+class SmrRaffConfig(C.Structure):
+    _fields_ = [("device", C.c_int), ("natoms", C.c_int), ("nsys", C.c_int), ("reserved", C.c_int * 5)]
+
+
+class SmrRaffStepConfig(C.Structure):
+    _fields_ = [("dt", C.c_float), ("k_coll", C.c_float), ("relaxation", C.c_float), ("momentum_beta", C.c_float),
+                ("rot_mass_scale", C.c_float), ("reserved", C.c_int * 3)]
+
 SIGNATURES = {
     "smr_create": (C.c_int, [C.POINTER(SmrConfig), C.POINTER(VP)]),
     "smr_destroy": (C.c_int, [VP]),
@@ -119,6 +128,28 @@ SIGNATURES = {
     "smr_get_schedule": (C.c_int, [VP, IP, IP, IP]),
     "smr_set_stages": (C.c_int, [VP, C.c_int, IP, IP, IP, C.c_int]),
     "smr_get_stages": (C.c_int, [VP, IP, IP, IP, IP]),
+    # multi-replica rigid-atom relaxation (include/surfmol_raff.h)
+    "smr_raff_create": (C.c_int, [C.POINTER(SmrRaffConfig), C.POINTER(VP)]),
+    "smr_raff_destroy": (C.c_int, [VP]),
+    "smr_raff_last_error": (C.c_char_p, [VP]),
+    "smr_raff_upload_radius": (C.c_int, [VP, FP]),
+    "smr_raff_upload_neighs_and_exclusions": (C.c_int, [VP, IP, IP, IP]),
+    "smr_raff_upload_fixmask": (C.c_int, [VP, IP]),
+    "smr_raff_upload_cluster_ports": (C.c_int, [VP, FP, FP, C.c_int]),
+    "smr_raff_upload_bk_slots": (C.c_int, [VP, IP]),
+    "smr_raff_upload_state": (C.c_int, [VP, FP, FP, FP]),
+    "smr_raff_step": (C.c_int, [VP, C.c_int, C.POINTER(SmrRaffStepConfig)]),
+    "smr_raff_last_ms": (C.c_int, [VP, FP]),
+    "smr_raff_download_pos": (C.c_int, [VP, C.c_int, FP]),
+    "smr_raff_download_quat": (C.c_int, [VP, C.c_int, FP]),
+    "smr_raff_download_dpos_coll": (C.c_int, [VP, C.c_int, FP]),
+    "smr_raff_download_dpos_node": (C.c_int, [VP, C.c_int, FP]),
+    "smr_raff_node_order": (C.c_int, [C.c_int, C.c_int, IP, IP]),
+    "smr_raff_build_neighs": (C.c_int, [C.c_int, C.c_int, IP, IP]),
+    "smr_raff_exclusions": (C.c_int, [C.c_int, IP, IP, IP]),
+    "smr_raff_bk_slots": (C.c_int, [C.c_int, C.c_int, IP, IP]),
+    "smr_raff_ports": (C.c_int, [C.c_int, FP, IP, C.c_float, FP, FP]),
+    "smr_raff_element_mass": (C.c_float, [C.c_int]),
 }
 
 _lib = None

@@ -9,7 +9,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libsurfmol_b200.so")
-SOURCES = ["relax.cu", "grid.cu", "topology.cpp", "abi.cpp"]
+SOURCES = ["relax.cu", "grid.cu", "raff.cu", "topology.cpp", "abi.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

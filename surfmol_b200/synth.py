@@ -159,6 +159,56 @@ def ragged_molecule(rng, target: int) -> Molecule:
     raise RuntimeError("could not generate a ragged molecule")
 
 
+def _tetra_rest(a, b):
+    """The two remaining unit directions of an ideal tetrahedron given two bond directions a, b."""
+    m = -(a + b) / 2.0
+    u = np.cross(a, b)
+    u /= np.linalg.norm(u)
+    return m + u * math.sqrt(2.0 / 3.0), m - u * math.sqrt(2.0 / 3.0)
+
+
+def pentitol(cc: float = 1.53, co: float = 1.43, ch: float = 1.09, oh: float = 0.96):
+    """A xylitol-like pentitol, HOCH2-(CHOH)3-CH2OH (C5H12O5, 22 atoms, 21 bonds, 10 nodes: the C
+    and O atoms), on an ideal tetrahedral zigzag chain.  Returns a Molecule with its bonds."""
+    dx, dy = cc * math.sin(math.radians(109.4712 / 2.0)), cc * math.cos(math.radians(109.4712 / 2.0))
+    Cp = [np.array([k * dx, (k % 2) * dy, 0.0]) for k in range(5)]
+    Z, P, bonds = [6] * 5, list(Cp), [(k, k + 1) for k in range(4)]
+
+    def add(z, p, to):
+        Z.append(z)
+        P.append(p)
+        bonds.append((to, len(Z) - 1))
+        return len(Z) - 1
+
+    for k in range(5):
+        nb = [Cp[j] - Cp[k] for j in (k - 1, k + 1) if 0 <= j < 5]
+        dirs = [v / np.linalg.norm(v) for v in nb]
+        if len(dirs) == 1:                                   # chain end: continue the zigzag
+            a = dirs[0]
+            nxt = Cp[k] + (Cp[k] - (Cp[k - 1] if k else Cp[1])) * np.array([1.0, -1.0, 1.0])
+            b = (nxt - Cp[k]) / np.linalg.norm(nxt - Cp[k])
+            c, d = _tetra_rest(a, b)
+            free = [b, c, d]
+        else:
+            free = list(_tetra_rest(dirs[0], dirs[1]))
+        o_dir = free[0] if k % 2 == 0 else free[1]
+        o = add(8, Cp[k] + co * o_dir, k)
+        for f in free:
+            if f is not o_dir:
+                add(1, Cp[k] + ch * f, k)
+        # hydroxyl H: 109.5 degrees from the O-C bond, in the plane of the O-C bond and z
+        a = -o_dir
+        p = np.cross(a, np.array([0.0, 0.0, 1.0]))
+        if np.linalg.norm(p) < 1e-6:
+            p = np.cross(a, np.array([1.0, 0.0, 0.0]))
+        p /= np.linalg.norm(p)
+        t = math.radians(109.4712)
+        add(1, P[o] + oh * (math.cos(t) * a + math.sin(t) * p), o)
+    pos = np.array(P)
+    pos -= pos.mean(0)
+    return Molecule(np.array(Z, np.int32), pos, bonds)
+
+
 def polyacene_ribbon(ncell: int, cc: float = 1.40, ch: float = 1.08):
     """A periodic polyacene ribbon along x: ``ncell`` repeats of C4H2 (a rung of two carbons and
     the two apex CH of the next ring), period ``cc * sqrt(3)``.  Returns (Molecule, lattice (3, 3))
