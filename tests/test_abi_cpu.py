@@ -1,5 +1,6 @@
-"""The C-ABI library loads and exports every entry point include/surfmol_relax.h declares (CPU, no compute)."""
+"""The C-ABI library loads and exports every entry point include/*.h declares (CPU, no compute)."""
 import ctypes
+import glob
 import os
 import re
 
@@ -7,7 +8,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def declared():
-    txt = open(os.path.join(ROOT, "include", "surfmol_relax.h")).read()
+    txt = "".join(open(p).read() for p in sorted(glob.glob(os.path.join(ROOT, "include", "*.h"))))
     txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
     return sorted(set(re.findall(r"\b(smr_[a-z_0-9]+)\s*\(", txt)))
 
