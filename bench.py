@@ -661,7 +661,7 @@ def run_ragged_dist(args):
 
 
 # ---------------------------------------------------------------------------------------- RAFF multi-replica
-RAFF = dict(nsys=5000, k=200.0, dt=0.1, relaxation=0.5, beta=0.0, amp=0.2, amp_h=0.3, steps_per_call=100)
+RAFF = dict(nsys=5000, k=200.0, dt=0.1, relaxation=0.5, beta=0.0, amp=0.2, amp_h=0.3, steps_per_call=10000)
 RAFF_METRIC = "RAFF multi-replica real atom-steps/s"
 
 

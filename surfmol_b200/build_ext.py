@@ -34,7 +34,7 @@ def build(verbose: bool = False, extra: list | None = None) -> str:
                "-c", path, "-o", obj]
         if src.endswith(".cu"):
             cmd += ["--expt-relaxed-constexpr"]
-            if src == "relax.cu":
+            if src in ("relax.cu", "raff.cu"):
                 cmd += ["-use_fast_math"]
         if verbose:
             cmd += ["-Xptxas", "-v"]

@@ -125,58 +125,70 @@ __device__ float3 collision(const RaffTopo& t, const float4* P, int i) {
     return sum;
 }
 
-// Ports of node i (compute_ports_current_multi, RRsp3.cl:1837-1934): for each bonded neighbour an
-// XPBD impulse pulling the neighbour onto the port tip xi + R(qi) r_local; the node collects its
-// translation and rotation, the neighbour's recoil goes to its slot.
-__device__ void ports(const RaffArgs& a, const float4* P, const float4* Q, float4* dnode, float4* drot, float4* dneigh, int i) {
-    const RaffTopo& t = a.t;
-    const int n = t.natoms, nn = t.nnode;
+// One port of the team (compute_ports_current_multi, RRsp3.cl:1837-1934): task t is slot t & 3 of
+// node t >> 2, an XPBD impulse pulling the neighbour onto the port tip xi + R(qi) r_local.  The
+// neighbour's recoil goes to the port's slot; the node's translation and rotation parts are
+// returned for the 4-lane sum over its slots.
+__device__ void port_task(const RaffArgs& a, const float4* P, const float4* Q, float4* dneigh, int t, float3& sdp, float3& sdt) {
+    const RaffTopo& tp = a.t;
+    const int i = t >> 2, k = t & 3;
+    sdp = make_float3(0.f, 0.f, 0.f); sdt = make_float3(0.f, 0.f, 0.f);
+    float4* out = dneigh + t;
+    *out = make_float4(0.f, 0.f, 0.f, 0.f);
     const float4 pi4 = P[i];
     const float invMi = pi4.w;
-    if (!(invMi > 1e-12f)) {
-        for (int k = 0; k < 4; k++) dneigh[4 * i + k] = make_float4(0.f, 0.f, 0.f, 0.f);
-        dnode[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-        drot[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-        return;
-    }
-    const float3 xi = f3(pi4);
-    const float4 qi = Q[i];
+    if (!(invMi > 1e-12f)) return;
+    const int4 ng = __ldg(tp.neighs + i);
+    const int j = k == 0 ? ng.x : (k == 1 ? ng.y : (k == 2 ? ng.z : ng.w));
+    if (j < 0 || j >= tp.natoms) return;
+    const float K = __ldg(tp.kport + t);
+    if (!(K > 0.f)) return;
+    const float4 pj4 = P[j];
+    const float invMj = pj4.w;
+    if (!(invMj > 1e-12f)) return;
     const float mi = 1.0f / invMi;
     const float invI = a.rot_mass_scale / (0.4f * mi + 1e-12f);
     const float dt2 = a.dt * a.dt + 1e-16f;
-    float3 sdp = make_float3(0.f, 0.f, 0.f), sdt = make_float3(0.f, 0.f, 0.f);
-    const int4 ng = __ldg(t.neighs + i);
-    for (int k = 0; k < 4; k++) {
-        const int j = k == 0 ? ng.x : (k == 1 ? ng.y : (k == 2 ? ng.z : ng.w));
-        float4* out = dneigh + 4 * i + k;
-        if (j < 0 || j >= n) { *out = make_float4(0.f, 0.f, 0.f, 0.f); continue; }
-        const float K = __ldg(t.kport + 4 * i + k);
-        if (!(K > 0.f)) { *out = make_float4(0.f, 0.f, 0.f, 0.f); continue; }
-        const float4 pj4 = P[j];
-        const float invMj = pj4.w;
-        if (!(invMj > 1e-12f)) { *out = make_float4(0.f, 0.f, 0.f, 0.f); continue; }
-        const float3 r_arm = qrot(qi, f3(__ldg(t.port_local + 4 * i + k)));
-        const float3 diff = f3(pj4) - (xi + r_arm);
-        const float dist2 = dot3(diff, diff);
-        if (dist2 < 1e-16f) { *out = make_float4(0.f, 0.f, 0.f, 0.f); continue; }
-        const float dist = sqrtf(dist2);
-        const float3 nv = div3(diff, dist);
-        const float3 rxn = cross3(r_arm, nv);
-        const float w_ang = dot3(rxn, rxn) * invI;
-        const float alpha = 1.0f / (K * dt2);
-        const bool jnode = j < nn;
-        float w_total = invMi + invMj + w_ang + alpha + 1e-12f;
-        if (jnode) w_total += w_ang;                   // as the reference: the node's own angular term again
-        float imp = dist / w_total;
-        if (jnode) imp *= 0.5f;                        // node-node ports act from both ends
-        const float3 Pv = nv * imp;
-        sdp = sdp + Pv * invMi;
-        sdt = sdt + cross3(r_arm, Pv) * invI;
-        const float3 rec = Pv * (-invMj);
-        *out = make_float4(rec.x, rec.y, rec.z, 0.f);
+    const float3 r_arm = qrot(Q[i], f3(__ldg(tp.port_local + t)));
+    const float3 diff = f3(pj4) - (f3(pi4) + r_arm);
+    const float dist2 = dot3(diff, diff);
+    if (dist2 < 1e-16f) return;
+    const float dist = sqrtf(dist2);
+    const float3 nv = div3(diff, dist);
+    const float3 rxn = cross3(r_arm, nv);
+    const float w_ang = dot3(rxn, rxn) * invI;
+    const float alpha = 1.0f / (K * dt2);
+    const bool jnode = j < tp.nnode;
+    float w_total = invMi + invMj + w_ang + alpha + 1e-12f;
+    if (jnode) w_total += w_ang;                       // as the reference: the node's own angular term again
+    float imp = dist / w_total;
+    if (jnode) imp *= 0.5f;                            // node-node ports act from both ends
+    const float3 Pv = nv * imp;
+    sdp = Pv * invMi;
+    sdt = cross3(r_arm, Pv) * invI;
+    const float3 rec = Pv * (-invMj);
+    *out = make_float4(rec.x, rec.y, rec.z, 0.f);
+}
+
+// All ports of the team: 4 nnode tasks over the team's lanes (the 4 slots of a node on 4
+// consecutive lanes of one warp), node sums by two shuffle steps.
+template <int T>
+__device__ void ports_all(const RaffArgs& a, const float4* P, const float4* Q, float4* dnode, float4* drot, float4* dneigh, int rank) {
+    const int ntask = 4 * min(a.t.nnode, a.t.natoms);
+    for (int t0 = 0; t0 < ntask; t0 += T) {            // uniform trip count: every lane reaches the shuffles
+        const int t = t0 + rank;
+        float3 sdp = make_float3(0.f, 0.f, 0.f), sdt = make_float3(0.f, 0.f, 0.f);
+        if (t < ntask) port_task(a, P, Q, dneigh, t, sdp, sdt);
+        for (int o = 1; o < 4; o <<= 1) {
+            sdp.x += __shfl_xor_sync(0xffffffffu, sdp.x, o); sdp.y += __shfl_xor_sync(0xffffffffu, sdp.y, o);
+            sdp.z += __shfl_xor_sync(0xffffffffu, sdp.z, o); sdt.x += __shfl_xor_sync(0xffffffffu, sdt.x, o);
+            sdt.y += __shfl_xor_sync(0xffffffffu, sdt.y, o); sdt.z += __shfl_xor_sync(0xffffffffu, sdt.z, o);
+        }
+        if (t < ntask && (t & 3) == 0) {
+            dnode[t >> 2] = make_float4(sdp.x, sdp.y, sdp.z, 0.f);
+            drot[t >> 2] = make_float4(sdt.x, sdt.y, sdt.z, 0.f);
+        }
     }
-    dnode[i] = make_float4(sdp.x, sdp.y, sdp.z, 0.f);
-    drot[i] = make_float4(sdt.x, sdt.y, sdt.z, 0.f);
 }
 
 // Correction of atom i (apply_corrections_multi, RRsp3.cl:1939-2046, massless_rot = 0): collision
@@ -252,7 +264,7 @@ __global__ void __launch_bounds__(T == 32 ? 128 : T) raff_kernel(const RaffArgs 
         for (int it = 0; it < a.nsteps; it++) {
             if (a.collide)
                 for (int i = rank; i < n; i += T) { const float3 c = collision(a.t, P, i); C[i] = make_float4(c.x, c.y, c.z, 0.f); }
-            for (int i = rank; i < nn && i < n; i += T) ports(a, P, Q, DN, DR, DG, i);
+            ports_all<T>(a, P, Q, DN, DR, DG, rank);
             team_sync<T>();
             for (int i = rank; i < n; i += T) correct(a, P, Q, M, MQ, C, DN, DR, DG, i);
             team_sync<T>();
