@@ -550,6 +550,86 @@ struct Xorshift {
     unsigned long long next() { s ^= s << 13; s ^= s >> 7; s ^= s << 17; return s; }
 };
 
+// Lower bound on the rounds: capacity, and per atom the terms in which it holds a role (a role
+// and its mirror under reversal share one count that may split over two orientations).
+template <int R>
+int rounds_lower_bound(int n, int nterms, const std::vector<int>& atoms, int team) {
+    int lb = (nterms + team - 1) / team;
+    std::vector<int> c((size_t)R * n, 0);
+    bool rev = false;
+    for (int t = 0; t < nterms; t++) {
+        const int* a0 = &atoms[(size_t)t * 2 * R];
+        const int* a1 = a0 + R;
+        if (!std::equal(a0, a0 + R, a1)) rev = true;
+        for (int k = 0; k < R; k++) c[(size_t)k * n + a0[k]]++;
+    }
+    for (int a = 0; a < n; a++)
+        for (int k = 0; k < R; k++) {
+            const int m = R - 1 - k;
+            if (!rev || m == k) lb = std::max(lb, c[(size_t)k * n + a]);
+            else if (k < m) lb = std::max(lb, (c[(size_t)k * n + a] + c[(size_t)m * n + a] + 1) / 2);
+        }
+    return lb;
+}
+
+// Min-conflicts search for an assignment in `rounds` rounds: each term's round and orientation
+// are moved, one conflicted term at a time, to the choice that clashes least (atoms sharing a
+// role in a round, rounds over capacity).  Deterministic (seeded); gives up after a bounded
+// number of moves.  Returns true with round_of / orient_of set when it found no clash.
+template <int R>
+bool pack_min_conflicts(int n, int nterms, const std::vector<int>& atoms, int team, int rounds, std::vector<int>& round_of,
+                        std::vector<int>& orient_of, unsigned long long seed) {
+    Xorshift rng{seed};
+    std::vector<int> occ((size_t)rounds * R * n, 0), cnt(rounds, 0);
+    auto at = [&](int t, int o) { return &atoms[((size_t)t * 2 + o) * R]; };
+    auto slot = [&](int r, int k, int a) -> int& { return occ[((size_t)r * R + k) * n + a]; };
+    std::vector<int> ro(nterms), oo(nterms);
+    for (int t = 0; t < nterms; t++) {            // start from the greedy assignment folded into `rounds`
+        ro[t] = round_of[t] < rounds ? round_of[t] : (int)(rng.next() % (unsigned long long)rounds);
+        oo[t] = orient_of[t];
+        const int* a = at(t, oo[t]);
+        for (int k = 0; k < R; k++) slot(ro[t], k, a[k])++;
+        cnt[ro[t]]++;
+    }
+    auto clash = [&](int t, int r, int o, bool self) {
+        const int* a = at(t, o);
+        int c = 0;
+        for (int k = 0; k < R; k++) c += slot(r, k, a[k]) - (self ? 1 : 0);
+        const int load = cnt[r] - (self ? 1 : 0);
+        if (load >= team) c += 1 + load - team;
+        return c;
+    };
+    // iterations: generous for small term sets, bounded total work (each move scans the terms)
+    const long long budget = std::min<long long>(5000LL * nterms + 100000, 200000000LL / std::max(nterms, 1));
+    for (long long it = 0; it < budget; it++) {
+        // a conflicted term: scan from a random start
+        int t0 = (int)(rng.next() % (unsigned long long)nterms), t = -1;
+        for (int q = 0; q < nterms; q++) {
+            const int u = (t0 + q) % nterms;
+            if (clash(u, ro[u], oo[u], true) > 0) { t = u; break; }
+        }
+        if (t < 0) { round_of = ro; orient_of = oo; return true; }
+        const int* a = at(t, oo[t]);
+        for (int k = 0; k < R; k++) slot(ro[t], k, a[k])--;
+        cnt[ro[t]]--;
+        int best = 1 << 30, br = ro[t], bo = oo[t], ties = 0;
+        const int no = std::equal(at(t, 0), at(t, 0) + R, at(t, 1)) ? 1 : 2;
+        for (int r = 0; r < rounds; r++)
+            for (int o = 0; o < no; o++) {
+                int c = clash(t, r, o, false);
+                if (r == ro[t] && o == oo[t]) c += 1;   // prefer moving
+                if (c < best) { best = c; br = r; bo = o; ties = 1; }
+                else if (c == best && rng.next() % (unsigned long long)(++ties) == 0) { br = r; bo = o; }
+            }
+        if (rng.next() % 16 == 0) { br = (int)(rng.next() % (unsigned long long)rounds); bo = no == 2 ? (int)(rng.next() & 1) : 0; }
+        ro[t] = br; oo[t] = bo;
+        a = at(t, bo);
+        for (int k = 0; k < R; k++) slot(br, k, a[k])++;
+        cnt[br]++;
+    }
+    return false;
+}
+
 // atoms[t*R*2 + o*R + k]: atom of role k in orientation o (o = 1 may equal o = 0)
 template <int R>
 int pack_assign(int n, int nterms, const std::vector<int>& atoms, int team, std::vector<int>& round_of,
@@ -583,6 +663,18 @@ int pack_assign(int n, int nterms, const std::vector<int>& atoms, int team, std:
             if ((int)used.size() >= best) break;
         }
         if ((int)used.size() < best) { best = (int)used.size(); round_of = r_of; pos_of = p_of; orient_of = o_of; }
+    }
+    // fewer rounds than the greedy found, down to the lower bound, by min-conflicts search
+    const int lb = rounds_lower_bound<R>(n, nterms, atoms, team);
+    for (int rr = lb; rr < best; rr++) {
+        std::vector<int> ro = round_of, oo = orient_of;
+        if (!pack_min_conflicts<R>(n, nterms, atoms, team, rr, ro, oo, 0xD1B54A32D192ED03ull ^ ((unsigned long long)nterms << 8) ^ rr))
+            continue;
+        std::vector<int> fill(rr, 0);
+        for (int t = 0; t < nterms; t++) pos_of[t] = fill[ro[t]]++;
+        round_of = ro; orient_of = oo;
+        best = rr;
+        break;
     }
     return best;
 }
