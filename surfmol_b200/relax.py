@@ -169,6 +169,7 @@ class RelaxMulti:
         self.h = h
         self.natoms_of = {}     # slot -> natoms
         self.topo_n = []        # topology id -> natoms
+        self._nat = np.zeros(int(max_systems), np.int64)   # slot -> natoms (0: free), for vectorised checks
 
     # -- lifecycle
     def finish(self):
@@ -485,6 +486,7 @@ class RelaxMulti:
                   "smr_add_systems")
         for s, t in zip(slots, topo_ids):
             self.natoms_of[int(s)] = self.topo_n[int(t)]
+        self._nat[slots] = np.asarray(self.topo_n, np.int64)[topo_ids]
         return slots
 
     upload_state_multi = add_systems
@@ -494,9 +496,24 @@ class RelaxMulti:
         self._chk(self.L.smr_remove_systems(self.h, len(slots), _p(slots, N.IP)), "smr_remove_systems")
         for s in slots:
             self.natoms_of.pop(int(s), None)
+        self._nat[slots] = 0
+
+    def _count(self, slots):
+        """Total atoms of the slots (0 for slots not active on this handle)."""
+        ok = (slots >= 0) & (slots < len(self._nat))
+        return int(self._nat[slots[ok]].sum())
 
     def set_positions(self, slots, positions):
+        """positions: one (n, 3) array per slot, or one stacked array ((nsys, n, 3) or (atoms, 3)) in
+        slot order."""
         slots = _i(slots)
+        if isinstance(positions, np.ndarray) and positions.ndim >= 2 and positions.shape[-1] == 3:
+            flat = _f(positions.reshape(-1, 3))
+            if flat.shape[0] != self._count(slots):
+                raise ValueError(f"{flat.shape[0]} positions for {self._count(slots)} atoms in {len(slots)} slots")
+            if len(slots):
+                self._chk(self.L.smr_set_positions(self.h, len(slots), _p(slots, N.IP), _p(flat, N.FP)), "smr_set_positions")
+            return
         if len(positions) != len(slots):
             raise ValueError(f"{len(slots)} slots but {len(positions)} position arrays")
         for s, p in zip(slots, positions):           # the C call reads natoms x 3 floats per slot
@@ -513,6 +530,9 @@ class RelaxMulti:
         self._chk(self.L.smr_reset_fire(self.h, len(slots), _p(slots, N.IP)), "smr_reset_fire")
 
     def _split(self, slots, flat, w):
+        nat = self._nat[slots] if len(slots) else np.zeros(0, np.int64)
+        if len(slots) and (nat == nat[0]).all():      # all systems alike: one (nsys, n, w) array
+            return flat.reshape(len(slots), int(nat[0]), w) if w > 1 else flat.reshape(len(slots), int(nat[0]))
         out, k = [], 0
         for s in slots:
             n = self.natoms_of[int(s)]
@@ -523,7 +543,7 @@ class RelaxMulti:
     def eval_forces(self, slots):
         """One force evaluation: list of (n, 4) float32 arrays (fx, fy, fz, E_atom), energies (nsys, 8)."""
         slots = _i(slots)
-        tot = sum(self.natoms_of.get(int(s), 0) for s in slots)
+        tot = self._count(slots)
         F = np.zeros((tot, 4), np.float32)
         E = np.zeros((len(slots), 8))
         self._chk(self.L.smr_eval_forces(self.h, len(slots), _p(slots, N.IP), _p(F, N.FP), _p(E, N.DP)),
@@ -541,7 +561,7 @@ class RelaxMulti:
 
     def download(self, slots, pos=True, forces=True):
         slots = _i(slots)
-        tot = sum(self.natoms_of.get(int(s), 0) for s in slots)
+        tot = self._count(slots)
         P = np.zeros((tot, 3), np.float32) if pos else None
         F = np.zeros((tot, 4), np.float32) if forces else None
         E = np.zeros((len(slots), 8))
@@ -555,7 +575,7 @@ class RelaxMulti:
     def download_pos64(self, slots):
         """Positions at full precision (float + its accumulated rounding error), list of (n, 3) float64."""
         slots = _i(slots)
-        tot = sum(self.natoms_of.get(int(s), 0) for s in slots)
+        tot = self._count(slots)
         P = np.zeros((tot, 3), np.float64)
         self._chk(self.L.smr_download_pos64(self.h, len(slots), _p(slots, N.IP), _p(P, N.DP)), "smr_download_pos64")
         return self._split(slots, P, 3)
