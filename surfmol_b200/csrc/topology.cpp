@@ -574,22 +574,33 @@ int rounds_lower_bound(int n, int nterms, const std::vector<int>& atoms, int tea
 
 // Min-conflicts search for an assignment in `rounds` rounds: each term's round and orientation
 // are moved, one conflicted term at a time, to the choice that clashes least (atoms sharing a
-// role in a round, rounds over capacity).  Deterministic (seeded); gives up after a bounded
-// number of moves.  Returns true with round_of / orient_of set when it found no clash.
+// role in a round, rounds over capacity).  Conflicted terms are drawn from a candidate list: a
+// term joining a clash is listed together with the round members it clashes with, so an empty
+// list means no clash is left (checked once more by a full scan).  Deterministic (seeded); gives
+// up after `budget` moves.  Returns true with round_of / orient_of set when it found no clash.
 template <int R>
 bool pack_min_conflicts(int n, int nterms, const std::vector<int>& atoms, int team, int rounds, std::vector<int>& round_of,
-                        std::vector<int>& orient_of, unsigned long long seed) {
+                        std::vector<int>& orient_of, unsigned long long seed, long long budget) {
     Xorshift rng{seed};
     std::vector<int> occ((size_t)rounds * R * n, 0), cnt(rounds, 0);
     auto at = [&](int t, int o) { return &atoms[((size_t)t * 2 + o) * R]; };
     auto slot = [&](int r, int k, int a) -> int& { return occ[((size_t)r * R + k) * n + a]; };
-    std::vector<int> ro(nterms), oo(nterms);
+    std::vector<int> ro(nterms), oo(nterms), cand, where(nterms);
+    std::vector<std::vector<int>> members(rounds);
+    std::vector<char> listed(nterms, 0);
+    auto add = [&](int t) { if (!listed[t]) { listed[t] = 1; cand.push_back(t); } };
+    auto join = [&](int t, int r) { where[t] = (int)members[r].size(); members[r].push_back(t); };
+    auto leave = [&](int t, int r) {
+        const int w = where[t], last = members[r].back();
+        members[r][w] = last; where[last] = w; members[r].pop_back();
+    };
     for (int t = 0; t < nterms; t++) {            // start from the greedy assignment folded into `rounds`
         ro[t] = round_of[t] < rounds ? round_of[t] : (int)(rng.next() % (unsigned long long)rounds);
         oo[t] = orient_of[t];
         const int* a = at(t, oo[t]);
         for (int k = 0; k < R; k++) slot(ro[t], k, a[k])++;
         cnt[ro[t]]++;
+        join(t, ro[t]);
     }
     auto clash = [&](int t, int r, int o, bool self) {
         const int* a = at(t, o);
@@ -599,19 +610,22 @@ bool pack_min_conflicts(int n, int nterms, const std::vector<int>& atoms, int te
         if (load >= team) c += 1 + load - team;
         return c;
     };
-    // iterations: generous for small term sets, bounded total work (each move scans the terms)
-    const long long budget = std::min<long long>(5000LL * nterms + 100000, 200000000LL / std::max(nterms, 1));
+    for (int t = 0; t < nterms; t++) if (clash(t, ro[t], oo[t], true) > 0) add(t);
     for (long long it = 0; it < budget; it++) {
-        // a conflicted term: scan from a random start
-        int t0 = (int)(rng.next() % (unsigned long long)nterms), t = -1;
-        for (int q = 0; q < nterms; q++) {
-            const int u = (t0 + q) % nterms;
-            if (clash(u, ro[u], oo[u], true) > 0) { t = u; break; }
+        if (cand.empty()) {
+            for (int t = 0; t < nterms; t++) if (clash(t, ro[t], oo[t], true) > 0) add(t);
+            if (cand.empty()) { round_of = ro; orient_of = oo; return true; }
         }
-        if (t < 0) { round_of = ro; orient_of = oo; return true; }
+        const size_t ci = (size_t)(rng.next() % (unsigned long long)cand.size());
+        const int t = cand[ci];
+        if (clash(t, ro[t], oo[t], true) == 0) {   // no longer in a clash: drop it from the list
+            cand[ci] = cand.back(); cand.pop_back(); listed[t] = 0;
+            continue;
+        }
         const int* a = at(t, oo[t]);
         for (int k = 0; k < R; k++) slot(ro[t], k, a[k])--;
         cnt[ro[t]]--;
+        leave(t, ro[t]);
         int best = 1 << 30, br = ro[t], bo = oo[t], ties = 0;
         const int no = std::equal(at(t, 0), at(t, 0) + R, at(t, 1)) ? 1 : 2;
         for (int r = 0; r < rounds; r++)
@@ -624,8 +638,19 @@ bool pack_min_conflicts(int n, int nterms, const std::vector<int>& atoms, int te
         if (rng.next() % 16 == 0) { br = (int)(rng.next() % (unsigned long long)rounds); bo = no == 2 ? (int)(rng.next() & 1) : 0; }
         ro[t] = br; oo[t] = bo;
         a = at(t, bo);
+        bool joined_clash = cnt[br] >= team;
+        for (int k = 0; k < R; k++) joined_clash = joined_clash || slot(br, k, a[k]) > 0;
+        if (joined_clash)                          // list the members it now clashes with
+            for (int u : members[br]) {
+                const int* b = at(u, oo[u]);
+                bool hit = cnt[br] >= team;
+                for (int k = 0; k < R && !hit; k++) hit = b[k] == a[k];
+                if (hit) add(u);
+            }
         for (int k = 0; k < R; k++) slot(br, k, a[k])++;
         cnt[br]++;
+        join(t, br);
+        if (clash(t, br, bo, true) == 0) { cand[ci] = cand.back(); cand.pop_back(); listed[t] = 0; }
     }
     return false;
 }
@@ -635,7 +660,7 @@ template <int R>
 int pack_assign(int n, int nterms, const std::vector<int>& atoms, int team, std::vector<int>& round_of,
                 std::vector<int>& pos_of, std::vector<int>& orient_of) {
     if (nterms == 0) { round_of.clear(); pos_of.clear(); orient_of.clear(); return 0; }
-    const int tries = std::max(1, std::min(64, 400000 / (nterms * R + 1)));
+    const int tries = std::max(1, std::min(8, 400000 / (nterms * R + 1)));
     Xorshift rng{0x9E3779B97F4A7C15ull ^ (unsigned long long)nterms};
     std::vector<int> order(nterms), r_of(nterms), p_of(nterms), o_of(nterms);
     int best = 1 << 30;
@@ -664,17 +689,19 @@ int pack_assign(int n, int nterms, const std::vector<int>& atoms, int team, std:
         }
         if ((int)used.size() < best) { best = (int)used.size(); round_of = r_of; pos_of = p_of; orient_of = o_of; }
     }
-    // fewer rounds than the greedy found, down to the lower bound, by min-conflicts search
+    // fewer rounds than the greedy found, one at a time down to the lower bound, by min-conflicts
+    // search; the first target it cannot reach within its budget ends the descent
     const int lb = rounds_lower_bound<R>(n, nterms, atoms, team);
-    for (int rr = lb; rr < best; rr++) {
+    const long long budget = std::min<long long>(30000, 300LL * nterms + 20000);
+    while (best > lb) {
+        const int rr = best - 1;
         std::vector<int> ro = round_of, oo = orient_of;
-        if (!pack_min_conflicts<R>(n, nterms, atoms, team, rr, ro, oo, 0xD1B54A32D192ED03ull ^ ((unsigned long long)nterms << 8) ^ rr))
-            continue;
+        if (!pack_min_conflicts<R>(n, nterms, atoms, team, rr, ro, oo, 0xD1B54A32D192ED03ull ^ ((unsigned long long)nterms << 8) ^ rr, budget))
+            break;
         std::vector<int> fill(rr, 0);
         for (int t = 0; t < nterms; t++) pos_of[t] = fill[ro[t]]++;
         round_of = ro; orient_of = oo;
         best = rr;
-        break;
     }
     return best;
 }
