@@ -742,7 +742,10 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
         auto nb_atoms = [&](auto cut_tag) {
         constexpr bool CUT = decltype(cut_tag)::value;
         for (int i0 = 0; i0 < N; i0 += G) {
-            const int i = i0 + rank / L;
+            // the last, partial pass spreads its atoms over all the team's lanes (uniform per team)
+            int Lp = L;
+            if (N - i0 < G) while (Lp < 32 && Lp * 2 * (N - i0) <= T) Lp <<= 1;
+            const int i = i0 + rank / Lp, cp = rank & (Lp - 1);
             float fx = 0.f, fy = 0.f, fz = 0.f, E = 0.f;
             if (i < N) {
                 const float4 pi = S.P()[i], qi = S.Q()[i], li = S.Lo()[i];
@@ -751,7 +754,7 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
                     // partners within rc + skin, ascending; exclusions were removed at the build
                     const unsigned short* row = a.nbl + (ga0 + i) * (size_t)a.nbl_cap;
 #pragma unroll 4
-                    for (int e = c; e < cnt; e += L) {
+                    for (int e = cp; e < cnt; e += Lp) {
                         const int j = row[e];
                         nb_pair<CUT>(a, pi, li, qi, S.P()[j], S.Lo()[j], S.Q()[j], false, fx, fy, fz, E);
                     }
@@ -763,17 +766,17 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
                     if (ng.z >= 0) ex |= 1ull << (ng.z & 63);
                     if (ng.w >= 0) ex |= 1ull << (ng.w & 63);
 #pragma unroll 4
-                    for (int j = c; j < N; j += L) {
+                    for (int j = cp; j < N; j += Lp) {
                         const bool excl = small ? (bool)((ex >> j) & 1ull) : (j == i || j == ng.x || j == ng.y || j == ng.z || j == ng.w);
                         nb_pair<CUT>(a, pi, li, qi, S.P()[j], S.Lo()[j], S.Q()[j], excl, fx, fy, fz, E);
                     }
                 }
             }
-            for (int o = 1; o < L; o <<= 1) {
+            for (int o = 1; o < Lp; o <<= 1) {
                 fx += __shfl_xor_sync(FULL, fx, o); fy += __shfl_xor_sync(FULL, fy, o);
                 fz += __shfl_xor_sync(FULL, fz, o); E += __shfl_xor_sync(FULL, E, o);
             }
-            if (c == 0 && i < N) {
+            if (cp == 0 && i < N) {
                 add4(S.F()[i], fx, fy, fz, E);
                 S.Eh()[i] += E;
                 acc.add(4, 0.5 * (double)E);
