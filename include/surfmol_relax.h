@@ -177,6 +177,19 @@ int smr_build_grid_static(int nions, const double* ions, const double* ion_re, d
                           const smr_grid_build_params_static* p, float* coef_out, void* stream,
                           char* err, int errlen);
 
+/* Sharded grid build over several GPUs (each builds an x-slab, an all-gather replicates the raw
+ * values, each fits the whole grid; the build of smr_build_grid split at its one exchange point):
+ * smr_grid_raw_slab writes the raw, unfitted FP64 values (Pauli, London, Coulomb triples,
+ * voxel-major, z-fastest) of the x-planes [x0, x0 + nxs) into raw, a DEVICE buffer of
+ * 3 nxs ny nz doubles the caller owns (planes beyond nx are computed and may be discarded, so
+ * equal slabs of ceil(nx / ranks) planes concatenate in rank order under an all-gather);
+ * smr_grid_from_raw fits and installs the whole grid from the gathered raw values (3 nx ny nz
+ * doubles on the device), as smr_build_grid would have built it.  No counterpart in the
+ * reference (its grid build is single-device). */
+int smr_grid_raw_slab(smr_handle* h, int nions, const double* ions, const double* ion_re, double Lx, double Ly,
+                      int nx, int ny, int nz, const double p0[3], const double step[3], const smr_grid_build_params* p,
+                      int x0, int nxs, double* raw);
+int smr_grid_from_raw(smr_handle* h, const double* raw, int nx, int ny, int nz, const double p0[3], const double step[3], int dtype);
 /* Re-encode the current grid to another storage dtype with per-channel scales (max|c| mapping). */
 int smr_convert_grid(smr_handle* h, int dtype);
 

@@ -880,6 +880,56 @@ int smr_build_grid(smr_handle* h, int nions, const double* ions, const double* i
     return SMR_OK;
 }
 
+// the sharded grid build's per-rank part: ions to the device, arguments, the raw evaluation
+int smr_grid_raw_slab(smr_handle* h, int nions, const double* ions, const double* ion_re, double Lx, double Ly,
+                      int nx, int ny, int nz, const double p0[3], const double step[3], const smr_grid_build_params* p,
+                      int x0, int nxs, double* raw) {
+    if (!h || !ions || !ion_re || !p0 || !step || !p || !raw || nions <= 0) return SMR_ERR_ARG;
+    SETTLE(h);
+    if (nx < 4 || ny < 4 || nz < 4) return fail(h, SMR_ERR_ARG, "grid must be at least 4x4x4");
+    if ((double)nx * ny * nz >= 2147483648.0) return fail(h, SMR_ERR_ARG, "grid of %dx%dx%d has 2^31 voxels or more", nx, ny, nz);
+    if (x0 < 0 || nxs < 1) return fail(h, SMR_ERR_ARG, "slab x0=%d, width %d", x0, nxs);
+    if (!(Lx > 0 && Ly > 0)) return fail(h, SMR_ERR_ARG, "cell must be positive");
+    double *dions = nullptr, *dre = nullptr;
+    CU(h, cudaMalloc(&dions, (size_t)nions * 32));
+    cudaError_t e = cudaMalloc(&dre, (size_t)nions * 32);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dions, ions, (size_t)nions * 32, cudaMemcpyHostToDevice, h->stream);
+    std::vector<double> re4(4 * (size_t)nions, 0.0);
+    for (int i = 0; i < nions; i++) { re4[4 * i] = ion_re[2 * i]; re4[4 * i + 1] = ion_re[2 * i + 1]; }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dre, re4.data(), re4.size() * 8, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) { cudaFree(dions); cudaFree(dre); return fail(h, SMR_ERR_CUDA, "grid slab: %s", cudaGetErrorString(e)); }
+    GridBuildArgs A{};
+    A.nions = nions; A.ions = dions; A.ion_re = dre; A.Lx = Lx; A.Ly = Ly; A.nx = nx; A.ny = ny; A.nz = nz;
+    for (int k = 0; k < 3; k++) { A.p0[k] = p0[k]; A.step[k] = step[k]; }
+    A.alpha = p->alpha_morse; A.npbc = p->npbc; A.ewald_tol = p->ewald_tol; A.morse_rcut = p->morse_rcut;
+    char msg[400] = {0};
+    const int r = grid_raw_slab_device(A, x0, nxs, raw, h->stream, msg, sizeof(msg));
+    cudaFree(dions); cudaFree(dre);
+    if (r) return fail(h, SMR_ERR_ARG, "grid slab: %s", msg);
+    return SMR_OK;
+}
+
+int smr_grid_from_raw(smr_handle* h, const double* raw, int nx, int ny, int nz, const double p0[3], const double step[3], int dtype) {
+    if (!h || !raw || !p0 || !step) return SMR_ERR_ARG;
+    SETTLE(h);
+    if (nx < 4 || ny < 4 || nz < 4) return fail(h, SMR_ERR_ARG, "grid must be at least 4x4x4");
+    if ((double)nx * ny * nz >= 2147483648.0) return fail(h, SMR_ERR_ARG, "grid of %dx%dx%d has 2^31 voxels or more", nx, ny, nz);
+    if (dtype < 0 || dtype > 2) return fail(h, SMR_ERR_ARG, "unknown grid dtype");
+    float4* out = nullptr;
+    CU(h, cudaMalloc(&out, (size_t)nx * ny * nz * 16));
+    char msg[400] = {0};
+    if (grid_from_raw_device(raw, nx, ny, nz, out, h->stream, msg, sizeof(msg))) { cudaFree(out); return fail(h, SMR_ERR_CUDA, "grid fit: %s", msg); }
+    if (h->grid) cudaFree(h->grid);
+    h->grid = out; h->grid_dtype = SMR_GRID_F32; h->has_grid = true;
+    h->gdim[0] = nx; h->gdim[1] = ny; h->gdim[2] = nz;
+    for (int k = 0; k < 3; k++) { h->gp0[k] = p0[k]; h->gstep[k] = step[k]; }
+    for (int k = 0; k < 4; k++) h->gscale[k] = 1.f;
+    h->gzscale.clear();
+    if (dtype != SMR_GRID_F32) return smr_convert_grid(h, dtype);
+    return SMR_OK;
+}
+
 int smr_add_molecule(smr_handle* h, int natoms, const int* Z, const double* pos, const double* charges,
                      double bond_cut, int* topo_id) {
     if (!h || !Z || !pos || !topo_id) return SMR_ERR_ARG;

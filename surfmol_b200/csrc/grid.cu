@@ -38,16 +38,17 @@ constexpr double kPi = 3.14159265358979323846;
 #define GB_CHECK(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) { std::snprintf(err, errlen, "%s: %s", #x, cudaGetErrorString(e_)); return -1; } } while (0)
 
 // ---------------------------------------------------------------- Morse
+// x-planes [x0, x0 + xs) of the grid; outputs indexed within that slab (z-fastest)
 __global__ void morse_kernel(int nions, const double* __restrict__ ions, const double* __restrict__ re,
-                             double Lx, double Ly, int npbc, int nx, int ny, int nz, double p0x, double p0y, double p0z,
+                             double Lx, double Ly, int npbc, int x0, int xs, int ny, int nz, double p0x, double p0y, double p0z,
                              double sx, double sy, double sz, float alpha, float rcut2, double* __restrict__ paul,
                              double* __restrict__ lond) {
     __shared__ float4 sI[128];
     __shared__ float2 sR[128];
-    const size_t N = (size_t)nx * ny * nz;
+    const size_t N = (size_t)xs * ny * nz;
     const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     const bool live = idx < N;
-    const int iz = (int)(idx % nz), iy = (int)((idx / nz) % ny), ix = (int)(idx / ((size_t)nz * ny));
+    const int iz = (int)(idx % nz), iy = (int)((idx / nz) % ny), ix = x0 + (int)(idx / ((size_t)nz * ny));
     // grid point relative coordinates in FP64, then FP32 per term
     const double px = p0x + ix * sx, py = p0y + iy * sy, pz = p0z + iz * sz;
     double P = 0.0, Lo = 0.0;
@@ -157,18 +158,19 @@ __global__ void ewald_stage1(int nrows, const int* __restrict__ rowptr, const in
 }
 
 // Stage 2: phi(ix, iy) = K (phi0 + Re sum_r B[r, ix] Ey[r, iy])
+// x-planes [x0, x0 + xs) of plane iz; B holds the x factors of all nx planes
 __global__ void ewald_stage2(int nrows, const double2* __restrict__ B, const double2* __restrict__ Ey, int nx, int ny,
-                             double phi0, int iz, int nz, double* __restrict__ out) {
+                             int x0, int xs, double phi0, int iz, int nz, double* __restrict__ out) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nx * ny) return;
-    const int iy = t % ny, ix = t / ny;
+    if (t >= xs * ny) return;
+    const int iy = t % ny, lx = t / ny, ix = x0 + lx;
     double acc = 0.0;
     for (int r = 0; r < nrows; r++) {
         const double2 b = B[(size_t)r * nx + ix];
         const double2 c = Ey[(size_t)r * ny + iy];
         acc += b.x * c.x - b.y * c.y;
     }
-    out[(size_t)iz + (size_t)nz * ((size_t)iy + (size_t)ny * ix)] = kCoulombD * (phi0 + acc);
+    out[(size_t)iz + (size_t)nz * ((size_t)iy + (size_t)ny * lx)] = kCoulombD * (phi0 + acc);
 }
 
 // ---------------------------------------------------------------- B-spline fit
@@ -371,10 +373,14 @@ int decode_grid_16(const void* src, float4* dst, size_t nvox, int nz, int dtype,
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
-int build_grid_device(const GridBuildArgs& A, float4* out, cudaStream_t s, char* err, int errlen) {
+namespace {
+
+// Raw (unfitted) FP64 channels of the x-planes [x0, x0 + xs): Morse (Pauli, London) and Ewald-2D,
+// each xs * ny * nz values, z-fastest, into paul / lond / coul (device).
+int grid_raw_channels(const GridBuildArgs& A, int x0, int xs, double* paul, double* lond, double* coul, DevBuf& buf,
+                      cudaStream_t s, char* err, int errlen) {
     const int nx = A.nx, ny = A.ny, nz = A.nz;
-    const size_t N = (size_t)nx * ny * nz;
-    DevBuf buf;
+    const size_t N = (size_t)xs * ny * nz;
     // host copy of ions for layer grouping and the geometry checks
     std::vector<double> hion(4 * (size_t)A.nions);
     GB_CHECK(cudaMemcpyAsync(hion.data(), A.ions, hion.size() * 8, cudaMemcpyDeviceToHost, s));
@@ -385,14 +391,11 @@ int build_grid_device(const GridBuildArgs& A, float4* out, cudaStream_t s, char*
     if (!(dmin > 0.05)) { std::snprintf(err, errlen, "grid bottom z=%g must lie above the top ion z=%g", A.p0[2], ztop); return -1; }
     if (std::fabs(qsum) > 1e-6 * std::max(1.0, (double)A.nions)) { std::snprintf(err, errlen, "slab charge %g is not neutral", qsum); return -1; }
 
-    double *paul, *lond, *coul;
-    GB_CHECK(buf.alloc(&paul, N)); GB_CHECK(buf.alloc(&lond, N)); GB_CHECK(buf.alloc(&coul, N));
-
     // Morse channels
     {
         const float rc2 = A.morse_rcut > 0 ? (float)(A.morse_rcut * A.morse_rcut) : 3.0e38f;
         const unsigned blocks = (unsigned)((N + 127) / 128);
-        morse_kernel<<<blocks, 128, 0, s>>>(A.nions, A.ions, A.ion_re, A.Lx, A.Ly, A.npbc, nx, ny, nz, A.p0[0], A.p0[1], A.p0[2],
+        morse_kernel<<<blocks, 128, 0, s>>>(A.nions, A.ions, A.ion_re, A.Lx, A.Ly, A.npbc, x0, xs, ny, nz, A.p0[0], A.p0[1], A.p0[2],
                                             A.step[0], A.step[1], A.step[2], (float)A.alpha, rc2, paul, lond);
         GB_CHECK(cudaGetLastError());
     }
@@ -482,13 +485,19 @@ int build_grid_device(const GridBuildArgs& A, float4* out, cudaStream_t s, char*
                 plane_amp_kernel<<<(ne + 255) / 256, 256, 0, s>>>(ne, damp, dgn, iz * A.step[2], thresh, dampz);
                 ewald_stage1<<<(nrows * nx + 127) / 128, 128, 0, s>>>(nrows, drow, dhidx, dampz, Ex, nx, B);
             }
-            ewald_stage2<<<(nx * ny + 127) / 128, 128, 0, s>>>(nrows, B, Ey, nx, ny, phi0, iz, nz, coul);
+            ewald_stage2<<<(xs * ny + 127) / 128, 128, 0, s>>>(nrows, B, Ey, nx, ny, x0, xs, phi0, iz, nz, coul);
             GB_CHECK(cudaGetLastError());
         }
         GB_CHECK(cudaStreamSynchronize(s));
     }
 
-    // exact B-spline fit of each channel, then pack
+    return 0;
+}
+
+// exact B-spline fit of each channel (whole grid), then pack into float4
+int fit_and_pack(double* paul, double* lond, double* coul, int nx, int ny, int nz, float4* out, DevBuf& buf, cudaStream_t s,
+                 char* err, int errlen) {
+    const size_t N = (size_t)nx * ny * nz;
     if (fit_channel(paul, nx, ny, nz, s, buf, err, errlen)) return -1;
     if (fit_channel(lond, nx, ny, nz, s, buf, err, errlen)) return -1;
     if (fit_channel(coul, nx, ny, nz, s, buf, err, errlen)) return -1;
@@ -496,6 +505,51 @@ int build_grid_device(const GridBuildArgs& A, float4* out, cudaStream_t s, char*
     GB_CHECK(cudaGetLastError());
     GB_CHECK(cudaStreamSynchronize(s));
     return 0;
+}
+
+// three channels <-> one voxel-major array of (Pauli, London, Coulomb) triples
+__global__ void interleave_kernel(size_t n, const double* __restrict__ a, const double* __restrict__ b,
+                                  const double* __restrict__ c, double* __restrict__ out) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) { out[3 * i] = a[i]; out[3 * i + 1] = b[i]; out[3 * i + 2] = c[i]; }
+}
+__global__ void deinterleave_kernel(size_t n, const double* __restrict__ in, double* __restrict__ a, double* __restrict__ b,
+                                    double* __restrict__ c) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) { a[i] = in[3 * i]; b[i] = in[3 * i + 1]; c[i] = in[3 * i + 2]; }
+}
+
+}  // namespace
+
+int build_grid_device(const GridBuildArgs& A, float4* out, cudaStream_t s, char* err, int errlen) {
+    const size_t N = (size_t)A.nx * A.ny * A.nz;
+    DevBuf buf;
+    double *paul, *lond, *coul;
+    GB_CHECK(buf.alloc(&paul, N)); GB_CHECK(buf.alloc(&lond, N)); GB_CHECK(buf.alloc(&coul, N));
+    if (grid_raw_channels(A, 0, A.nx, paul, lond, coul, buf, s, err, errlen)) return -1;
+    return fit_and_pack(paul, lond, coul, A.nx, A.ny, A.nz, out, buf, s, err, errlen);
+}
+
+int grid_raw_slab_device(const GridBuildArgs& A, int x0, int xs, double* raw, cudaStream_t s, char* err, int errlen) {
+    const size_t N = (size_t)xs * A.ny * A.nz;
+    DevBuf buf;
+    double *paul, *lond, *coul;
+    GB_CHECK(buf.alloc(&paul, N)); GB_CHECK(buf.alloc(&lond, N)); GB_CHECK(buf.alloc(&coul, N));
+    if (grid_raw_channels(A, x0, xs, paul, lond, coul, buf, s, err, errlen)) return -1;
+    interleave_kernel<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(N, paul, lond, coul, raw);
+    GB_CHECK(cudaGetLastError());
+    GB_CHECK(cudaStreamSynchronize(s));
+    return 0;
+}
+
+int grid_from_raw_device(const double* raw, int nx, int ny, int nz, float4* out, cudaStream_t s, char* err, int errlen) {
+    const size_t N = (size_t)nx * ny * nz;
+    DevBuf buf;
+    double *paul, *lond, *coul;
+    GB_CHECK(buf.alloc(&paul, N)); GB_CHECK(buf.alloc(&lond, N)); GB_CHECK(buf.alloc(&coul, N));
+    deinterleave_kernel<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(N, raw, paul, lond, coul);
+    GB_CHECK(cudaGetLastError());
+    return fit_and_pack(paul, lond, coul, nx, ny, nz, out, buf, s, err, errlen);
 }
 
 }  // namespace smr
@@ -637,7 +691,7 @@ extern "C" int smr_build_grid_static(int nions, const double* ions, const double
     ST_CHECK(cudaMemcpyAsync(dions, ions, (size_t)nions * 32, cudaMemcpyHostToDevice, s));
     ST_CHECK(cudaMemcpy2DAsync(dre, 32, ion_re, 16, 16, nions, cudaMemcpyHostToDevice, s));
     const float rc2 = p->morse_rcut > 0 ? (float)(p->morse_rcut * p->morse_rcut) : 3.0e38f;
-    morse_kernel<<<(unsigned)((N + 127) / 128), 128, 0, s>>>(nions, dions, dre, Lx, Ly, p->npbc, nx, ny, nz, p0[0], p0[1], p0[2],
+    morse_kernel<<<(unsigned)((N + 127) / 128), 128, 0, s>>>(nions, dions, dre, Lx, Ly, p->npbc, 0, nx, ny, nz, p0[0], p0[1], p0[2],
                                                              step[0], step[1], step[2], (float)p->alpha_morse, rc2, paul, lond);
     static_structure_factor<<<(w * nk + 127) / 128, 128, 0, s>>>(nions, dions, p0[2], H, K, g1, g2, S);
     static_phase<<<(w * nx + 255) / 256, 256, 0, s>>>(nx, H, p0[0], step[0], g1, Ex);
@@ -647,7 +701,7 @@ extern "C" int smr_build_grid_static(int nions, const double* ions, const double
         const double z = p0[2] + iz * step[2];
         const double phi0 = -(2.0 * kPi / area) * (qsum * z - qz);
         static_stage1<<<(nk * nx + 127) / 128, 128, 0, s>>>(H, K, S, gmax, g1, g2, area, iz * step[2], nx, Ex, B);
-        ewald_stage2<<<(nx * ny + 127) / 128, 128, 0, s>>>(nk, B, Ey, nx, ny, phi0, iz, nz, coul);
+        ewald_stage2<<<(nx * ny + 127) / 128, 128, 0, s>>>(nk, B, Ey, nx, ny, 0, nx, phi0, iz, nz, coul);
     }
     ST_CHECK(cudaGetLastError());
     // exact B-spline fit: z open, y and x cyclic (tables from the host stack)

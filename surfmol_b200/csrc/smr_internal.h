@@ -213,6 +213,10 @@ struct GridBuildArgs {
     double alpha; int npbc; double ewald_tol; double morse_rcut;
 };
 int build_grid_device(const GridBuildArgs& a, float4* out_f32, cudaStream_t s, char* err, int errlen);
+// sharded build: raw FP64 (Pauli, London, Coulomb) triples of the x-planes [x0, x0 + xs), voxel-major
+// z-fastest, into raw (device); then the fit and pack of a whole grid from such triples
+int grid_raw_slab_device(const GridBuildArgs& a, int x0, int xs, double* raw, cudaStream_t s, char* err, int errlen);
+int grid_from_raw_device(const double* raw, int nx, int ny, int nz, float4* out_f32, cudaStream_t s, char* err, int errlen);
 // 16-bit storage with one power-of-two scale per z plane and channel: plane_scale_out gets nz x 4
 // floats (host); decode takes them as a device table
 int encode_grid_16(const float4* src, void* dst, size_t nvox, int nz, int dtype, float* plane_scale_out, cudaStream_t s);

@@ -231,6 +231,22 @@ class RelaxMulti:
         self._chk(self.L.smr_build_grid(self.h, len(ions), _p(ions, N.DP), _p(re, N.DP), Lx, Ly, nx, ny, nz,
                                         _p(_d(p0), N.DP), _p(_d(step), N.DP), C.byref(p)), "smr_build_grid")
 
+    def grid_raw_slab(self, ions, ion_re, Lx, Ly, nx, ny, nz, p0, step, x0, nxs, raw_dev_ptr, alpha_morse=1.5, npbc=1,
+                      ewald_tol=1e-12, morse_rcut=0.0):
+        """Raw FP64 (Pauli, London, Coulomb) triples of x-planes [x0, x0 + nxs) into the device buffer at
+        raw_dev_ptr (an int address, e.g. a torch tensor's data_ptr(); 3 nxs ny nz doubles)."""
+        ions = _d(ions)
+        re = _d(np.asarray(ion_re)[:, :2])
+        p = N.SmrGridBuildParams(alpha_morse, npbc, ewald_tol, GRID_F32, morse_rcut)
+        self._chk(self.L.smr_grid_raw_slab(self.h, len(ions), _p(ions, N.DP), _p(re, N.DP), Lx, Ly, nx, ny, nz,
+                                           _p(_d(p0), N.DP), _p(_d(step), N.DP), C.byref(p), int(x0), int(nxs),
+                                           N.VP(int(raw_dev_ptr))), "smr_grid_raw_slab")
+
+    def grid_from_raw(self, raw_dev_ptr, nx, ny, nz, p0, step, dtype=GRID_F32):
+        """Fit and install the grid from 3 nx ny nz raw FP64 values on the device (grid_raw_slab's layout)."""
+        self._chk(self.L.smr_grid_from_raw(self.h, N.VP(int(raw_dev_ptr)), nx, ny, nz, _p(_d(p0), N.DP), _p(_d(step), N.DP),
+                                           int(dtype)), "smr_grid_from_raw")
+
     def convert_grid(self, dtype):
         self._chk(self.L.smr_convert_grid(self.h, dtype), "smr_convert_grid")
 

@@ -53,3 +53,43 @@ def max_over_ranks(value: float) -> float:
     t = torch.tensor([float(value)], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def grid_slabs(nx: int, world: int) -> tuple[int, list[tuple[int, int]]]:
+    """Equal x-slabs for a sharded grid build: width ceil(nx / world) and each rank's [x0, x0 + width);
+    the last slabs may reach past nx (their extra planes are computed and dropped), so the slabs
+    concatenate in rank order under an all-gather of equal chunks."""
+    if world <= 0:
+        raise ValueError("world must be positive")
+    w = -(-int(nx) // world)
+    return w, [(r * w, r * w + w) for r in range(world)]
+
+
+def gather_slabs(chunks, nx: int, ny: int, nz: int):
+    """Host assembly of rank-ordered raw slabs (each 3 * width * ny * nz values) into the 3 * nx * ny * nz
+    array of the whole grid: what the all-gather produces, trimmed to nx planes."""
+    flat = np.concatenate([np.asarray(c).reshape(-1) for c in chunks])
+    return flat[:3 * nx * ny * nz]
+
+
+def build_grid_sharded(R, ions, ion_re, Lx, Ly, nx, ny, nz, p0, step, group=None, dtype=0, **params):
+    """Substrate grid built across the ranks of a torch.distributed group (NCCL on GPUs): each rank
+    evaluates the raw Morse and Ewald-2D values of its x-slab, one all-gather over NVLink replicates
+    them, and every rank fits and installs the whole grid.  With one rank (or no process group) it
+    is the single-GPU build split at the same point.  R: a RelaxMulti on this rank's GPU."""
+    import torch
+    import torch.distributed as dist
+    ws = dist.get_world_size(group) if dist.is_available() and dist.is_initialized() else 1
+    rank = dist.get_rank(group) if ws > 1 else 0
+    w, slabs = grid_slabs(nx, ws)
+    x0, _ = slabs[rank]
+    local = torch.empty(3 * w * ny * nz, dtype=torch.float64, device="cuda")
+    R.grid_raw_slab(ions, ion_re, Lx, Ly, nx, ny, nz, p0, step, x0, w, local.data_ptr(), **params)
+    if ws > 1:
+        full = torch.empty(ws * local.numel(), dtype=torch.float64, device="cuda")
+        dist.all_gather_into_tensor(full, local, group=group)
+    else:
+        full = local
+    torch.cuda.synchronize()
+    R.grid_from_raw(full.data_ptr(), nx, ny, nz, p0, step, dtype=dtype)
+    del local, full

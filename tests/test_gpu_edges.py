@@ -202,3 +202,32 @@ def test_topology_file_relaxes_like_pipeline(env, tmp_path):
     out = R.download(s)
     assert np.array_equal(out["pos"][0], out["pos"][1]) and out["steps"][0] == out["steps"][1] == 200
     R.remove_systems(s)
+
+
+@pytest.mark.parametrize("world", [1, 3, 4])
+def test_sharded_grid_build_equals_single_build(world):
+    """The sharded build's two halves (raw x-slabs, then the fit of the gathered whole) give the
+    single-call grid bit for bit; the ranks' slabs are built one after another on this GPU into
+    the buffer an all-gather would fill (3 ranks: slabs reach past nx, the extra planes dropped)."""
+    import torch
+    from surfmol_b200 import RelaxMulti
+    from surfmol_b200.shard import build_grid_sharded, grid_slabs
+    slab, dims, p0, step = small_slab_grid()
+    nx, ny, nz = dims
+    R = RelaxMulti(max_systems=4, max_atoms=400)
+    try:
+        ref = build_device_grid(R, slab, dims, p0, step)
+        w, slabs = grid_slabs(nx, world)
+        full = torch.empty(world * 3 * w * ny * nz, dtype=torch.float64, device="cuda")
+        for k, (x0, _) in enumerate(slabs):
+            part = full[k * 3 * w * ny * nz:(k + 1) * 3 * w * ny * nz]
+            R.grid_raw_slab(slab.ions, slab.req()[:, :2], slab.Lx, slab.Ly, nx, ny, nz, p0, step, x0, w, part.data_ptr(),
+                            alpha_morse=1.5, npbc=1)
+        torch.cuda.synchronize()
+        R.grid_from_raw(full.data_ptr(), nx, ny, nz, p0, step)
+        got = R.get_grid()
+        assert np.array_equal(got["coef"], ref["coef"])
+        build_grid_sharded(R, slab.ions, slab.req()[:, :2], slab.Lx, slab.Ly, nx, ny, nz, p0, step, alpha_morse=1.5, npbc=1)
+        assert np.array_equal(R.get_grid()["coef"], ref["coef"])
+    finally:
+        R.finish()

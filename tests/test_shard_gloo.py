@@ -74,3 +74,61 @@ def test_two_gloo_ranks_shard_and_reduce():
     assert got == list(range(len(costs)))
     assert not set(res[0][1]) & set(res[1][1])
     assert res[0][2] == res[1][2] == 11.0
+
+
+def test_grid_slabs_partition():
+    from surfmol_b200.shard import gather_slabs, grid_slabs
+    for nx, world in ((28, 1), (28, 3), (226, 8), (904, 8), (5, 4)):
+        w, slabs = grid_slabs(nx, world)
+        assert slabs[0][0] == 0 and all(slabs[k][1] == slabs[k + 1][0] for k in range(world - 1))
+        assert slabs[-1][1] >= nx and w * world - nx < world
+        ny, nz = 3, 2
+        full = np.arange(3 * nx * ny * nz, dtype=np.float64)
+        pad = np.concatenate([full, -np.ones(3 * (w * world - nx) * ny * nz)])
+        chunks = [pad[3 * x0 * ny * nz:3 * x1 * ny * nz] for x0, x1 in slabs]
+        assert np.array_equal(gather_slabs(chunks, nx, ny, nz), full)
+
+
+def _slab_rank(rank, world, port, nx, ny, nz, out_q):
+    import torch
+    import torch.distributed as dist
+    from surfmol_b200.shard import grid_slabs
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
+    try:
+        w, slabs = grid_slabs(nx, world)
+        x0, x1 = slabs[rank]
+        # this rank's raw slab: voxel-major triples whose values encode (plane, y, z, channel)
+        x = np.arange(x0, x1)[:, None, None, None]
+        y = np.arange(ny)[None, :, None, None]
+        z = np.arange(nz)[None, None, :, None]
+        c = np.arange(3)[None, None, None, :]
+        local = torch.from_numpy((1000 * x + 100 * y + 10 * z + c).astype(np.float64).reshape(-1))
+        parts = [torch.empty_like(local) for _ in range(world)]
+        dist.all_gather(parts, local)
+        full = torch.cat(parts)[:3 * nx * ny * nz]
+        out_q.put((rank, full.numpy().tolist()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_gather_grid_slabs():
+    """The raw slabs of two ranks, gathered in rank order, are the voxel-major raw array of the
+    whole grid (the exchange step of the sharded grid build)."""
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    nx, ny, nz = 7, 3, 4
+    ps = [ctx.Process(target=_slab_rank, args=(r, 2, port, nx, ny, nz, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    res = dict(q.get(timeout=120) for _ in range(2))
+    for p in ps:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    x = np.arange(nx)[:, None, None, None]
+    y = np.arange(ny)[None, :, None, None]
+    z = np.arange(nz)[None, None, :, None]
+    c = np.arange(3)[None, None, None, :]
+    want = (1000 * x + 100 * y + 10 * z + c).reshape(-1)
+    assert np.array_equal(res[0], want) and np.array_equal(res[1], want)
