@@ -121,6 +121,11 @@ int smr_set_nb_params(smr_handle* h, const smr_nb_params* p);
 int smr_set_grid(smr_handle* h, const void* coef, int dtype, const float scale[4],
                  int nx, int ny, int nz, const double p0[3], const double step[3]);
 int smr_get_grid(smr_handle* h, void* coef_out, int* dtype, float scale[4], int dims[3], double p0[3], double step[3]);
+/* smr_set_grid from DEVICE memory (the "device pointer" form of the boundary's set_grid): the
+ * coefficients are copied device to device on the handle's stream (the caller may free or reuse
+ * its buffer on return).  Refused if dev_coef is not device memory. */
+int smr_set_grid_device(smr_handle* h, const void* dev_coef, int dtype, const float scale[4],
+                        int nx, int ny, int nz, const double p0[3], const double step[3]);
 /* 16-bit grids with one scale per z plane and channel (value = stored * plane_scale[4*iz + c]);
  * smr_convert_grid to F16 / BF16 produces such grids (power-of-two scales fitted per plane: the
  * channels grow by orders of magnitude towards the surface, one scale per channel would waste

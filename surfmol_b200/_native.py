@@ -78,6 +78,7 @@ SIGNATURES = {
     "smr_get_grid": (C.c_int, [VP, VP, IP, FP, IP, DP, DP]),
     "smr_set_grid_planes": (C.c_int, [VP, VP, C.c_int, FP, C.c_int, C.c_int, C.c_int, DP, DP]),
     "smr_get_grid_planes": (C.c_int, [VP, FP]),
+    "smr_set_grid_device": (C.c_int, [VP, VP, C.c_int, FP, C.c_int, C.c_int, C.c_int, DP, DP]),
     "smr_set_surface_folded": (C.c_int, [VP, VP]),
     "smr_grid_raw_slab": (C.c_int, [VP, C.c_int, DP, DP, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, DP, DP,
                                     C.POINTER(SmrGridBuildParams), C.c_int, C.c_int, VP]),

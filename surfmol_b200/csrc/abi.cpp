@@ -788,6 +788,34 @@ int smr_set_grid(smr_handle* h, const void* coef, int dtype, const float scale[4
     return SMR_OK;
 }
 
+int smr_set_grid_device(smr_handle* h, const void* dev_coef, int dtype, const float scale[4], int nx, int ny, int nz,
+                        const double p0[3], const double step[3]) {
+    if (!h || !dev_coef || !p0 || !step) return SMR_ERR_ARG;
+    SETTLE(h);
+    if (dtype < 0 || dtype > 2) return fail(h, SMR_ERR_ARG, "unknown grid dtype %d", dtype);
+    if (nx < 4 || ny < 4 || nz < 4) return fail(h, SMR_ERR_ARG, "grid must be at least 4x4x4 (got %dx%dx%d)", nx, ny, nz);
+    if ((double)nx * ny * nz >= 2147483648.0) return fail(h, SMR_ERR_ARG, "grid of %dx%dx%d has 2^31 voxels or more", nx, ny, nz);
+    if (!(step[0] > 0 && step[1] > 0 && step[2] > 0)) return fail(h, SMR_ERR_ARG, "grid steps must be positive");
+    cudaPointerAttributes attr{};
+    if (cudaPointerGetAttributes(&attr, dev_coef) != cudaSuccess || attr.type != cudaMemoryTypeDevice) {
+        cudaGetLastError();
+        return fail(h, SMR_ERR_ARG, "coefficients are not in device memory");
+    }
+    const size_t bytes = (size_t)nx * ny * nz * voxel_bytes(dtype);
+    void* d = nullptr;
+    CU(h, cudaMalloc(&d, bytes));
+    cudaError_t e = cudaMemcpyAsync(d, dev_coef, bytes, cudaMemcpyDeviceToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) { cudaFree(d); return fail(h, SMR_ERR_CUDA, "grid copy: %s", cudaGetErrorString(e)); }
+    if (h->grid) cudaFree(h->grid);
+    h->grid = d; h->grid_dtype = dtype; h->has_grid = true;
+    h->gdim[0] = nx; h->gdim[1] = ny; h->gdim[2] = nz;
+    for (int k = 0; k < 3; k++) { h->gp0[k] = p0[k]; h->gstep[k] = step[k]; }
+    for (int k = 0; k < 4; k++) h->gscale[k] = scale ? scale[k] : 1.f;
+    h->gzscale.clear();
+    return SMR_OK;
+}
+
 int smr_get_grid(smr_handle* h, void* coef_out, int* dtype, float scale[4], int dims[3], double p0[3], double step[3]) {
     if (!h) return SMR_ERR_ARG;
     SETTLE(h);

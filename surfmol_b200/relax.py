@@ -208,6 +208,13 @@ class RelaxMulti:
         self._chk(self.L.smr_set_grid(self.h, coef.ctypes.data_as(N.VP), dtype, _p(sc, N.FP), nx, ny, nz,
                                       _p(_d(p0), N.DP), _p(_d(step), N.DP)), "smr_set_grid")
 
+    def set_grid_device(self, dev_ptr, dims, p0, step, dtype=GRID_F32, scale=(1, 1, 1, 1)):
+        """Grid coefficients already on the device (an int address, e.g. a torch tensor's data_ptr();
+        dims = (nx, ny, nz), layout as set_grid), copied device to device."""
+        sc = _f(scale)
+        self._chk(self.L.smr_set_grid_device(self.h, N.VP(int(dev_ptr)), dtype, _p(sc, N.FP), int(dims[0]), int(dims[1]),
+                                             int(dims[2]), _p(_d(p0), N.DP), _p(_d(step), N.DP)), "smr_set_grid_device")
+
     def get_grid(self):
         dt = C.c_int()
         sc = (C.c_float * 4)()

@@ -231,3 +231,26 @@ def test_sharded_grid_build_equals_single_build(world):
         assert np.array_equal(R.get_grid()["coef"], ref["coef"])
     finally:
         R.finish()
+
+
+def test_set_grid_from_device_memory():
+    """smr_set_grid_device: a grid held by torch on the GPU goes in device to device and reads back
+    unchanged; host memory is refused."""
+    import torch
+    from surfmol_b200 import RelaxMulti
+    from surfmol_b200.relax import SmrError
+    slab, dims, p0, step = small_slab_grid()
+    R = RelaxMulti(max_systems=4, max_atoms=400)
+    try:
+        g = build_device_grid(R, slab, dims, p0, step)
+        t = torch.from_numpy(g["coef"].copy()).cuda()
+        R2 = RelaxMulti(max_systems=4, max_atoms=400)
+        try:
+            R2.set_grid_device(t.data_ptr(), dims, p0, step)
+            assert np.array_equal(R2.get_grid()["coef"], g["coef"])
+            with pytest.raises(SmrError, match="device memory"):
+                R2.set_grid_device(g["coef"].ctypes.data, dims, p0, step)
+        finally:
+            R2.finish()
+    finally:
+        R.finish()
