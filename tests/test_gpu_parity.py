@@ -94,6 +94,7 @@ def test_forces_energies_match_oracle(R, oracle, slab_grid, n, team, form):
     for c in range(1, 7):
         assert abs(E[0, c] - Eco[c]) < 2e-6 * max(1.0, abs(Eco[c])), (c, E[0, c], Eco[c])
     assert abs(E[0, 0] - Eco[0]) < 2e-6 * max(1.0, np.abs(Eco[1:7]).sum())
+    assert abs(E[0, 0] - Eco[0]) < 1e-6 * abs(Eco[0])            # total energy within 1e-6 relative
     R.remove_systems(s)
     R.set_team_size(1 << 20, 0)
     R.set_schedule(0, 0, 0)
