@@ -1004,8 +1004,10 @@ int orc_raff_step(int n, int nn, int nsys, int nsteps, const double* cfg, int co
                   const int* excl1, const int* excl2, const int* fixmask, const double* port_local, const double* kport,
                   const int* bk, double* pos, double* quat, double* dmom, double* dqmom, double* coll_out, double* dnode_out) {
     const double dt = cfg[0], relax = cfg[1], beta = cfg[2], rms = cfg[3];
-    std::vector<V3> C(n), DN(nn), DR(nn), DG(4 * (size_t)nn);
+    // replicas are independent: one per thread
+#pragma omp parallel for schedule(dynamic)
     for (int r = 0; r < nsys; r++) {
+        std::vector<V3> C(n), DN(nn), DR(nn), DG(4 * (size_t)nn);
         double* P = pos + 4 * (size_t)r * n; double* Q = quat + 4 * (size_t)r * n;
         double* M = dmom + 4 * (size_t)r * n; double* MQ = dqmom + 4 * (size_t)r * n;
         auto p3 = [&](int i) { return V3{P[4 * i], P[4 * i + 1], P[4 * i + 2]}; };
