@@ -235,6 +235,16 @@ int smr_topology_cells(smr_handle* h, int topo_id, int* cells);
  * replaces the system's constraints; n = 0 removes them.  Constrained systems run in the
  * extended gather form. */
 int smr_set_constraints(smr_handle* h, int slot, int n, const int* atoms, const double* target, const double* k);
+/* Langevin drive: the TDrives input of updateAtomsMMFFf4 (opencl/UFF.cl:982-991), per system
+ * tdrive[4 i ..] = (T [K], gamma, seed increment per FIRE step, seed).  While gamma > 0 the force
+ * FIRE uses gains -gamma v + noise sqrt(2 kB T gamma / dt), with v the velocity before the step,
+ * dt the system's current FIRE step and noise the kernel's hashed vector of the atom index and
+ * seed.  The reference's host changes the seed between launches.  Here the seed of FIRE step s
+ * (counted from the last reset) is fma(increment, s, seed): an increment of 0 keeps the kernel's
+ * fixed pattern, so chunked and unchunked runs stay identical either way.  Like the constraint
+ * springs, the drive acts on FIRE (power, norms, the max|F| test) but not on the returned forces.
+ * gamma <= 0 turns the drive off.  Driven systems run in the extended gather form. */
+int smr_set_thermal_drive(smr_handle* h, int nsys, const int* slot_ids, const double* tdrive);
 /* counts[6] = natoms, nbonds, nang, ndih, ninv, type-rounds (schedule length) */
 int smr_topology_counts(smr_handle* h, int topo_id, int counts[6]);
 /* Any output pointer may be null.  Layouts as the arrays of smr_topology_desc plus

@@ -672,23 +672,66 @@ void eval_forces(const orc_sys& S, const V3* P, const orc_grid* g, const NBParam
 
 struct FireParams { double dt0, dt_max, alpha0, f_inc, f_dec, f_alpha; int n_min; double fconv, flimit; };
 
+const double KB_EV = 8.617333262145e-5;            // eV/K, opencl/UFF.cl:52
+
+// The pseudo-random vector of the thermal drive of updateAtomsMMFFf4 (opencl/UFF.cl:982-991):
+// per component k a byte of (ia + c_k + (int)(m_k seed)) * 2654435761 (64-bit product, shifted
+// right by 16) scaled to [0, 1), then sin((r_k + seed) * 124.4565) with the sum and product in
+// FP32, as the kernel forms them, and the sine in FP64.
+V3 langevin_noise(int ia, float seed) {
+    static const int c[3] = {136, 778, 4578};
+    static const float m[3] = {1000.f, 1013.f, 998.f};
+    double out[3];
+    for (int k = 0; k < 3; k++) {
+        const float ms = m[k] * seed;
+        const long long x = (long long)(ia + c[k] + (int)ms);
+        const float r = (float)((x * 2654435761LL) >> 16 & 0xFF) * 0.00390625f;
+        const float s = r + seed;
+        const float arg = s * 124.4565f;
+        out[k] = std::sin((double)arg);
+    }
+    return {out[0], out[1], out[2]};
+}
+
+// Driving terms of updateAtomsMMFFf4 that act on FIRE but are not stored with the forces:
+// constraint springs (UFF.cl:974-982; per atom target xyz + on flag, stiffness xyz) and the
+// Langevin drive (UFF.cl:982-991; td = T [K], gamma, seed increment per step, seed).
+struct Drive {
+    const double* cons = nullptr;    // n x 7: target x, y, z, on (> 0), kx, ky, kz
+    const double* td = nullptr;      // 4 values, or null
+};
+
 // relax_fire, crates/apps/molengine/src/main.rs:237-277 (unit masses).  The step
 // uses the dt read at the top of the iteration (main.rs:242), positions advance
-// even on the converging step (main.rs:270-275), then the loop breaks.
+// even on the converging step (main.rs:270-275), then the loop breaks.  With a drive, the
+// force FIRE uses at step s is the limited force plus the springs at the current positions
+// plus -gamma v + noise(seed + s * seed_step) sqrt(2 kB T gamma / dt), v the velocity before
+// the step.
 int relax_fire(const orc_sys& S, V3* P, const orc_grid* g, const NBParams& nb, const FireParams& fp, int max_steps,
-               V3* F, double* Ea, double* Ec, double* fmax_out, int* conv_out) {
+               V3* F, double* Ea, double* Ec, double* fmax_out, int* conv_out, const Drive& dr = Drive{}) {
     int n = S.n;
-    std::vector<V3> V(n, V3{0, 0, 0});
+    std::vector<V3> V(n, V3{0, 0, 0}), Fd(n);
     double dt = fp.dt0, alpha = fp.alpha0; int npos = 0;
     int steps = 0; double fmax = 0; int conv = 0;
+    const bool therm = dr.td && dr.td[1] > 0.0;
     for (int itr = 0; itr < max_steps; itr++) {
         const double dt_old = dt;
         eval_forces(S, P, g, nb, F, Ea, Ec);
         double vf = 0, vv = 0, ff = 0, f2max = 0;
+        const float seed = therm ? std::fma((float)dr.td[2], (float)itr, (float)dr.td[3]) : 0.f;
+        const double amp = therm ? std::sqrt(2.0 * KB_EV * (double)(float)dr.td[0] * (double)(float)dr.td[1] / dt_old) : 0.0;
         for (int a = 0; a < n; a++) {
             V3 f = F[a];
             double f2 = dot(f, f);
             if (fp.flimit > 0 && f2 > fp.flimit * fp.flimit) { f = f * (fp.flimit / std::sqrt(f2)); F[a] = f; f2 = dot(f, f); }
+            if (dr.cons && dr.cons[7 * a + 3] > 0.0) {
+                const double* c = dr.cons + 7 * a;
+                f = f + V3{(c[0] - P[a].x) * std::max(c[4], 0.0), (c[1] - P[a].y) * std::max(c[5], 0.0),
+                           (c[2] - P[a].z) * std::max(c[6], 0.0)};
+            }
+            if (therm) f = f + V[a] * -(double)(float)dr.td[1] + langevin_noise(a, seed) * amp;
+            f2 = dot(f, f);
+            Fd[a] = f;
             if (f2 > f2max) f2max = f2;
             ff += f2;
             V[a] = V[a] + f * dt_old;
@@ -697,7 +740,7 @@ int relax_fire(const orc_sys& S, V3* P, const orc_grid* g, const NBParams& nb, c
         }
         if (vf > 0.0 && ff > 1e-30 && vv > 1e-30) {
             double vm = std::sqrt(vv), fm = std::sqrt(ff);
-            for (int a = 0; a < n; a++) V[a] = V[a] * (1.0 - alpha) + (F[a] * (1.0 / fm)) * (alpha * vm);
+            for (int a = 0; a < n; a++) V[a] = V[a] * (1.0 - alpha) + (Fd[a] * (1.0 / fm)) * (alpha * vm);
             npos++;
             if (npos > fp.n_min) { dt = std::min(dt * fp.f_inc, fp.dt_max); alpha *= fp.f_alpha; }
         } else {
@@ -1122,6 +1165,23 @@ int orc_relax(const orc_sys* S, double* pos, const orc_grid* g, const double* nb
     int steps = relax_fire(*S, P.data(), g, nbp_of(nbp), fp_of(fp), max_steps, FF.data(), Ea, Ec, fmax, conv);
     for (int a = 0; a < S->n; a++) { pos[3 * a] = P[a].x; pos[3 * a + 1] = P[a].y; pos[3 * a + 2] = P[a].z; if (F) { F[3 * a] = FF[a].x; F[3 * a + 1] = FF[a].y; F[3 * a + 2] = FF[a].z; } }
     return steps;
+}
+
+// orc_relax with the driving terms of updateAtomsMMFFf4: cons (n x 7, or null) and td (4, or null)
+int orc_relax_drive(const orc_sys* S, double* pos, const orc_grid* g, const double* nbp, const double* fp, int max_steps,
+                    const double* cons, const double* td, double* F, double* Ea, double* Ec, double* fmax, int* conv) {
+    std::vector<V3> P(S->n), FF(S->n);
+    for (int a = 0; a < S->n; a++) P[a] = {pos[3 * a], pos[3 * a + 1], pos[3 * a + 2]};
+    Drive dr; dr.cons = cons; dr.td = td;
+    int steps = relax_fire(*S, P.data(), g, nbp_of(nbp), fp_of(fp), max_steps, FF.data(), Ea, Ec, fmax, conv, dr);
+    for (int a = 0; a < S->n; a++) { pos[3 * a] = P[a].x; pos[3 * a + 1] = P[a].y; pos[3 * a + 2] = P[a].z; if (F) { F[3 * a] = FF[a].x; F[3 * a + 1] = FF[a].y; F[3 * a + 2] = FF[a].z; } }
+    return steps;
+}
+
+// the thermal drive's pseudo-random vectors of atoms 0..n-1 at one seed (n x 3)
+int orc_langevin_noise(int n, float seed, double* out) {
+    for (int a = 0; a < n; a++) { V3 r = langevin_noise(a, seed); out[3 * a] = r.x; out[3 * a + 1] = r.y; out[3 * a + 2] = r.z; }
+    return 0;
 }
 
 // CPU baseline: independent systems relaxed in parallel, one system per thread.

@@ -60,6 +60,9 @@ def lib():
         L.orc_folded_points.argtypes = [C.POINTER(OrcFolded), C.c_int, DP, DP, DP, DP]
         L.orc_relax.restype = C.c_int
         L.orc_relax.argtypes = [C.c_void_p, DP, C.POINTER(OrcGrid), DP, DP, C.c_int, DP, DP, DP, DP, IP]
+        L.orc_relax_drive.restype = C.c_int
+        L.orc_relax_drive.argtypes = [C.c_void_p, DP, C.POINTER(OrcGrid), DP, DP, C.c_int, DP, DP, DP, DP, DP, DP, IP]
+        L.orc_langevin_noise.argtypes = [C.c_int, C.c_float, DP]
         L.orc_relax_batch.argtypes = [C.c_int, C.POINTER(C.c_void_p), C.POINTER(DP), C.POINTER(OrcGrid), DP, DP,
                                       C.c_int, IP, DP, IP, DP, C.c_int]
         L.orc_max_threads.restype = C.c_int
@@ -267,6 +270,29 @@ class System:
                                 C.byref(conv))
         return dict(pos=pos, F=F, Ea=Ea, Ec=Ec, steps=steps, fmax=fmax.value, conv=bool(conv.value))
 
+    def relax_drive(self, pos, grid: Grid | None = None, max_steps=2000, nb=None, cons=None, tdrive=None, **fire):
+        """relax with the driving terms of updateAtomsMMFFf4: cons = (atoms, target (m, 3), k (m, 3))
+        springs, tdrive = (T [K], gamma, seed increment per step, seed) Langevin drive."""
+        pos = _d(pos).copy()
+        F = np.zeros((self.n, 3))
+        Ea = np.zeros(self.n)
+        Ec = np.zeros(8)
+        fmax = C.c_double()
+        conv = C.c_int()
+        cv = None
+        if cons is not None:
+            atoms, target, k = cons
+            cv = np.zeros((self.n, 7))
+            cv[np.asarray(atoms, int), :3] = np.asarray(target, float).reshape(-1, 3)
+            cv[np.asarray(atoms, int), 3] = 1.0
+            cv[np.asarray(atoms, int), 4:] = np.broadcast_to(np.asarray(k, float), (len(atoms), 3))
+        td = None if tdrive is None else _d(tdrive)
+        steps = lib().orc_relax_drive(self.h, _dp(pos), grid.ptr() if grid is not None else None,
+                                      _dp(nb_vec(**(nb or {}))), _dp(fire_vec(**fire)), max_steps,
+                                      _dp(cv) if cv is not None else None, _dp(td) if td is not None else None,
+                                      _dp(F), _dp(Ea), _dp(Ec), C.byref(fmax), C.byref(conv))
+        return dict(pos=pos, F=F, Ea=Ea, Ec=Ec, steps=steps, fmax=fmax.value, conv=bool(conv.value))
+
 
 E_TOT, E_BOND, E_ANG, E_DIH, E_INV, E_NB, E_GRID = range(7)
 
@@ -284,6 +310,13 @@ def relax_batch(systems, positions, grid=None, max_steps=2000, nthreads=0, nb=No
     lib().orc_relax_batch(ns, hs, pp, grid.ptr() if grid is not None else None, _dp(nb_vec(**(nb or {}))),
                           _dp(fire_vec(**fire)), max_steps, _ip(steps), _dp(fmax), _ip(conv), _dp(etot), nthreads)
     return dict(pos=pos, steps=steps, fmax=fmax, conv=conv.astype(bool), etot=etot)
+
+
+def langevin_noise(n, seed):
+    """The thermal drive's pseudo-random vectors of atoms 0..n-1 (updateAtomsMMFFf4, UFF.cl:982-991)."""
+    out = np.zeros((n, 3))
+    lib().orc_langevin_noise(n, C.c_float(seed), _dp(out))
+    return out
 
 
 def max_threads():

@@ -94,6 +94,7 @@ SIGNATURES = {
     "smr_get_pbc": (C.c_int, [VP, C.c_int, DP, IP]),
     "smr_topology_cells": (C.c_int, [VP, C.c_int, IP]),
     "smr_set_constraints": (C.c_int, [VP, C.c_int, C.c_int, IP, DP, DP]),
+    "smr_set_thermal_drive": (C.c_int, [VP, C.c_int, IP, DP]),
     "smr_add_molecules": (C.c_int, [VP, C.c_int, IP, IP, DP, DP, C.c_double, IP]),
     "smr_add_topology": (C.c_int, [VP, C.POINTER(SmrTopologyDesc), IP]),
     "smr_topology_counts": (C.c_int, [VP, C.c_int, IP]),

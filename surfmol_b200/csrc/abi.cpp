@@ -99,6 +99,7 @@ struct smr_handle {
     std::vector<float4> hlat;
     DArr<float4> dlat;
     DArr<float4> dcons;                 // per state atom 2 float4: constraint target (+ on) and stiffness
+    DArr<float4> dtdrive;               // per slot: Langevin drive (T, gamma, seed increment per step, seed)
     DArr<AngRec> dang; DArr<DihRec> ddih; DArr<InvRec> dinv;
     std::vector<int2> ha2f; std::vector<int> hidx;      // gather form: per atom (start, count), piece indices
     DArr<int2> da2f; DArr<int> didx;
@@ -430,7 +431,7 @@ KernelArgs base_args(smr_handle* h) {
     a.slots = h->slots;
     a.topos = h->dtd.d;
     a.req = h->dreq.d; a.neigh = h->dneigh.d; a.bk = h->dbk.d; a.bl = h->dbl.d;
-    a.neighc = h->dneighc.d; a.lat = h->dlat.d; a.cons = h->dcons.d;
+    a.neighc = h->dneighc.d; a.lat = h->dlat.d; a.cons = h->dcons.d; a.tdrive = h->dtdrive.d;
     a.angs = h->dang.d; a.dihs = h->ddih.d; a.invs = h->dinv.d;
     a.a2f = h->da2f.d; a.a2f_idx = h->didx.d;
     a.own_geo = h->down_geo.d; a.own_par = h->down_par.d; a.own_meta = h->down_meta.d;
@@ -1063,6 +1064,34 @@ int smr_set_constraints(smr_handle* h, int slot, int n, const int* atoms, const 
     return upload_slots(h, {slot});                    // waits, so c may go
 }
 
+int smr_set_thermal_drive(smr_handle* h, int nsys, const int* slot_ids, const double* tdrive) {
+    if (!h || nsys < 0 || (nsys && (!slot_ids || !tdrive))) return SMR_ERR_ARG;
+    SETTLE(h);
+    for (int i = 0; i < nsys; i++) {
+        if (!valid_slot(h, slot_ids[i])) return fail(h, SMR_ERR_ARG, "slot %d not active", slot_ids[i]);
+        const double* t = tdrive + 4 * (size_t)i;
+        for (int k = 0; k < 4; k++)
+            if (!std::isfinite(t[k])) return fail(h, SMR_ERR_ARG, "system %d: non-finite drive value", i);
+        if (t[0] < 0.0) return fail(h, SMR_ERR_ARG, "system %d: temperature %g below 0", i, t[0]);
+    }
+    if (nsys == 0) return SMR_OK;
+    if (!h->dtdrive.d) {
+        CU(h, h->dtdrive.reserve(h->hs.size(), 0, h->stream));
+        CU(h, cudaMemsetAsync(h->dtdrive.d, 0, h->hs.size() * 16, h->stream));
+    }
+    std::vector<float4> td(nsys);
+    std::vector<int> ids(slot_ids, slot_ids + nsys);
+    for (int i = 0; i < nsys; i++) {
+        const double* t = tdrive + 4 * (size_t)i;
+        td[i] = make_float4((float)t[0], (float)t[1], (float)t[2], (float)t[3]);
+        SlotState& st = h->hs[slot_ids[i]];
+        // the drive acts while gamma > 0, as in updateAtomsMMFFf4
+        st.flags = td[i].y > 0.f ? (st.flags | SLOT_THERM) : (st.flags & ~SLOT_THERM);
+        CU(h, cudaMemcpyAsync(h->dtdrive.d + slot_ids[i], &td[i], 16, cudaMemcpyHostToDevice, h->stream));
+    }
+    return upload_slots(h, ids);                      // waits, so td may go
+}
+
 int smr_get_pbc(smr_handle* h, int slot, double lvec[9], int npbc[3]) {
     if (!h || !lvec || !npbc) return SMR_ERR_ARG;
     SETTLE(h);
@@ -1417,7 +1446,7 @@ static void sig_args(std::vector<long long>& v, const KernelArgs& a) {
     v.push_back(a.phase_limit); v.push_back(a.step_budget); P(a.ecomp); v.push_back(a.nmax); v.push_back(a.nfmax);
     P(a.a2f); P(a.a2f_idx); P(a.own_geo); P(a.own_par); P(a.own_meta); v.push_back(a.nb_lanes);
     P(a.gscratch); v.push_back((long long)a.gscratch_bytes);
-    P(a.neighc); P(a.lat); P(a.cons);
+    P(a.neighc); P(a.lat); P(a.cons); P(a.tdrive);
     P(a.nbl); P(a.nbl_cnt); P(a.nbl_ref); v.push_back(a.nbl_cap); v.push_back(a.nbl_min); F(a.nbl_skin);
     v.push_back(a.fold.on); v.push_back(a.fold.nx); v.push_back(a.fold.ny); v.push_back(a.fold.nz);
     for (int k = 0; k < 4; k++) { F(a.fold.inv[k]); F(a.fold.inv_lo[k]); }

@@ -341,6 +341,40 @@ __device__ __forceinline__ float3 constraint_force(const float4* cons, size_t g,
                        ((c.z - p.z) - lo.z) * fmaxf(k.z, 0.f));
 }
 
+// Pseudo-random vector of the Langevin drive of updateAtomsMMFFf4 (opencl/UFF.cl:982-991) for
+// atom ia of its system: per component a byte of the 64-bit product (ia + c + (int)(m seed)) *
+// 2654435761 >> 16, scaled to [0, 1), then sin((r + seed) * 124.4565).  The sum and product
+// are rounded to FP32 as the kernel forms them; the sine is taken in FP64 and rounded, since
+// the fast single-precision sine loses accuracy at these arguments (up to ~1e5 rad).
+__device__ __noinline__ float3 langevin_noise(int ia, float seed) {
+    const int c[3] = {136, 778, 4578};
+    const float m[3] = {1000.f, 1013.f, 998.f};
+    float out[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const long long x = (long long)(ia + c[k] + __float2int_rz(__fmul_rn(m[k], seed)));
+        const float r = __fmul_rn((float)((x * 2654435761LL) >> 16 & 0xFF), 0.00390625f);
+        const float arg = __fmul_rn(__fadd_rn(r, seed), 124.4565f);
+        out[k] = (float)sin((double)arg);
+    }
+    return make_float3(out[0], out[1], out[2]);
+}
+
+constexpr double KB_EV = 8.617333262145e-5;        // eV/K, opencl/UFF.cl:52
+
+// f += -gamma v + noise(ia, seed) amp, in the kernel's order (damping first)
+__device__ __forceinline__ void add_langevin(float4& f, float4 v, int ia, float seed, float amp, float gamma) {
+    const float3 r = langevin_noise(ia, seed);
+    f.x = __fmaf_rn(r.x, amp, __fmaf_rn(v.x, -gamma, f.x));
+    f.y = __fmaf_rn(r.y, amp, __fmaf_rn(v.y, -gamma, f.y));
+    f.z = __fmaf_rn(r.z, amp, __fmaf_rn(v.z, -gamma, f.z));
+}
+
+// v + f dt with explicit roundings, so that both FIRE passes form the same velocity
+__device__ __forceinline__ float4 kick(float4 v, float4 f, float dt) {
+    return make_float4(__fmaf_rn(f.x, dt, v.x), __fmaf_rn(f.y, dt, v.y), __fmaf_rn(f.z, dt, v.z), v.w);
+}
+
 // beyond_cutoff_fp64 for a partner image shifted by s
 __device__ __noinline__ bool beyond_cutoff_fp64_shift(float4 pi, float4 li, float4 pj, float4 lj, float sx, float sy, float sz, float rc2) {
     const double dx = ((double)pj.x - (double)pi.x) + ((double)lj.x - (double)li.x) + (double)sx;
@@ -1012,6 +1046,11 @@ __device__ void run_system(const KernelArgs& a, const Smem& S, int w, int rank) 
     // constraint springs (extended form only): added after the force limit, they drive FIRE but
     // are not stored with the forces, as updateAtomsMMFFf4 stores the force before them
     const bool cons_on = FORM == FORM_GATHER_EXT && (st.flags & SLOT_CONS) != 0;
+    // Langevin drive (extended form only, UFF.cl:982-991): -gamma v + noise(seed) sqrt(2 kB T gamma / dt)
+    // on the force FIRE uses, v the velocity before the step; the seed advances by td.z per step
+    // of the system, so chunked and unchunked runs draw the same numbers
+    const bool therm_on = FORM == FORM_GATHER_EXT && (st.flags & SLOT_THERM) != 0;
+    const float4 td = therm_on ? __ldg(a.tdrive + slot) : make_float4(0.f, 0.f, 0.f, 0.f);
     int ran = 0;
     for (int it = 0; it < nsteps; it++) {
         if (use_list) {
@@ -1024,6 +1063,8 @@ __device__ void run_system(const KernelArgs& a, const Smem& S, int w, int rank) 
         const float dtf = (float)dt_old;
         double vf = 0.0, vv = 0.0, ff = 0.0;
         float f2m = 0.f;
+        const float seed = therm_on ? __fmaf_rn(td.z, (float)steps, td.w) : 0.f;
+        const float amp = therm_on ? (float)sqrt(2.0 * KB_EV * (double)td.x * (double)td.y / dt_old) : 0.f;
         for (int i = rank; i < N; i += T) {
             float4 f = S.F()[i];
             float f2 = f.x * f.x + f.y * f.y + f.z * f.z;
@@ -1038,11 +1079,17 @@ __device__ void run_system(const KernelArgs& a, const Smem& S, int w, int rank) 
                 f.x += fc.x; f.y += fc.y; f.z += fc.z;
                 f2 = f.x * f.x + f.y * f.y + f.z * f.z;
             }
+            float4 v = S.V()[i];
+            if (therm_on) {
+                add_langevin(f, v, i, seed, amp, td.y);
+                f2 = f.x * f.x + f.y * f.y + f.z * f.z;
+                v = kick(v, f, dtf);          // the second pass rebuilds this velocity from the stored one
+            } else {
+                v.x += f.x * dtf; v.y += f.y * dtf; v.z += f.z * dtf;
+                S.V()[i] = v;
+            }
             f2m = fmaxf(f2m, f2);
             ff += (double)f2;
-            float4 v = S.V()[i];
-            v.x += f.x * dtf; v.y += f.y * dtf; v.z += f.z * dtf;
-            S.V()[i] = v;
             vf += (double)(v.x * f.x + v.y * f.y + v.z * f.z);
             vv += (double)(v.x * v.x + v.y * v.y + v.z * v.z);
         }
@@ -1059,13 +1106,18 @@ __device__ void run_system(const KernelArgs& a, const Smem& S, int w, int rank) 
         }
         for (int i = rank; i < N; i += T) {
             float4 v = S.V()[i];
-            if (mix) {
+            if (mix || therm_on) {
                 float4 f = S.F()[i];
                 if (cons_on) {
                     const float3 fc = constraint_force(a.cons, ga0 + i, S.P()[i], S.Lo()[i]);
                     f.x += fc.x; f.y += fc.y; f.z += fc.z;
                 }
-                v.x = v.x * cv + f.x * cf; v.y = v.y * cv + f.y * cf; v.z = v.z * cv + f.z * cf;
+                if (therm_on) {
+                    add_langevin(f, v, i, seed, amp, td.y);
+                    v = kick(v, f, dtf);
+                }
+                if (mix) { v.x = v.x * cv + f.x * cf; v.y = v.y * cv + f.y * cf; v.z = v.z * cv + f.z * cf; }
+                else v = make_float4(0.f, 0.f, 0.f, 0.f);
             } else {
                 v = make_float4(0.f, 0.f, 0.f, 0.f);
             }

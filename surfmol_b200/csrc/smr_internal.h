@@ -63,7 +63,8 @@ struct SlotState {
     double dt, alpha;             // FIRE adaptive state
     double energy;                // total physical energy at the last force evaluation
     float fmax;                   // max |F| at the last force evaluation
-    int flags;                    // SLOT_PBC: lattice in KernelArgs::lat; SLOT_CONS: position constraints in KernelArgs::cons
+    int flags;                    // SLOT_PBC: lattice in KernelArgs::lat; SLOT_CONS: position constraints in KernelArgs::cons;
+                                  // SLOT_THERM: Langevin drive in KernelArgs::tdrive
 };
 
 enum GridDtype { GRID_F32 = 0, GRID_F16 = 1, GRID_BF16 = 2 };
@@ -106,6 +107,8 @@ struct KernelArgs {
     const short4* neighc; const float4* lat;
     // position constraints: per state atom g, cons[2 g] = (target x, y, z, on), cons[2 g + 1] = (kx, ky, kz, 0)
     const float4* cons;
+    // Langevin drive per slot: (T [K], gamma, seed increment per FIRE step, seed)
+    const float4* tdrive;
     const AngRec* angs; const DihRec* dihs; const InvRec* invs;
     float4* pos; float4* plo; float4* vel; float4* force;
     GridView grid; int has_grid;
@@ -201,7 +204,7 @@ int build_listed_topology(int n, const int* Z, const int* type_ids, const double
 // FORM_GATHER_EXT: the gather form with the code of the rarer per-system features compiled in
 // (periodic systems: bond shifts, NB image sums; position constraints); the host sends every
 // system that uses one there, so the other forms carry none of it
-enum SlotFlags { SLOT_PBC = 1, SLOT_CONS = 2 };
+enum SlotFlags { SLOT_PBC = 1, SLOT_CONS = 2, SLOT_THERM = 4 };
 enum KernelForm { FORM_ROUNDS = 0, FORM_GATHER = 1, FORM_OWNER = 2, FORM_GATHER_EXT = 3 };
 int launch_relax(const KernelArgs& a, int team, int form, int eval_only, cudaStream_t s, int num_sms, long long* launches);
 size_t team_smem_bytes(int nmax, int nfmax, int team, int form);

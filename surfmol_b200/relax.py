@@ -381,6 +381,14 @@ class RelaxMulti:
         self._chk(self.L.smr_set_constraints(self.h, int(slot), n, _p(atoms, N.IP), _p(tgt, N.DP), _p(kk, N.DP)),
                   "smr_set_constraints")
 
+    def set_thermal_drive(self, slots, T, gamma, seed=0.0, seed_step=0.0):
+        """Langevin drive of updateAtomsMMFFf4 on systems: temperature T [K], damping gamma, seed and
+        the seed's increment per FIRE step (each a scalar or one value per slot).  gamma <= 0: off."""
+        slots = _i(np.ravel(slots))
+        n = len(slots)
+        td = _d(np.stack([np.broadcast_to(np.asarray(x, float), (n,)) for x in (T, gamma, seed_step, seed)], 1))
+        self._chk(self.L.smr_set_thermal_drive(self.h, n, _p(slots, N.IP), _p(td, N.DP)), "smr_set_thermal_drive")
+
     def topology_counts(self, topo_id):
         """(natoms, nbonds, nang, ndih, ninv, type-rounds) of a topology on the handle."""
         c = (C.c_int * 6)()
