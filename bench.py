@@ -377,7 +377,7 @@ def run_ours(args, ws, rank, local):
 
 
 # ---------------------------------------------------------------------------------------- ragged workload
-RAGGED = dict(nsys=16384, nmin=20, nmax=400, rcut=10.0, fconv=1e-4, max_steps=3000, tune_sample=1024)
+RAGGED = dict(nsys=16384, nmin=20, nmax=400, rcut=10.0, fconv=1e-4, max_steps=3000, tune_sample=4096)
 
 
 def ragged_desc(w, nsys):
@@ -516,7 +516,10 @@ def run_ragged(args, ws, rank, local):
                        "fire_steps_p50": float(np.percentile(steps_all, 50)), "fire_steps_p99": float(np.percentile(steps_all, 99)),
                        "host_s": {"generate": round(tgen, 2), "autotune": round(ttune, 2), "add_molecules": round(tadd, 2)},
                        "tuned": None if tune is None else {"team_by_class": tune.team_by_class, "form0": tune.form0,
-                                                            "nb_lanes": tune.nb_lanes, "stages": tune.stages}},
+                                                            "nb_lanes": tune.nb_lanes, "stages": tune.stages,
+                                                            "sample_relax_ms": {k: round(tune.timings[k], 1) for k in
+                                                                                ("relax_ms_tuned_shape", "relax_ms_default_shape",
+                                                                                 "relax_ms_tuned") if k in tune.timings}}},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "traffic": None, "peak_source": peak_kind,
                          "algorithmic_bytes": "1024 B per atom-step (64 float4 grid voxels), state resident in shared memory"},

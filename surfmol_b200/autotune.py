@@ -10,6 +10,12 @@ by measurement on the device, on a sample of the workload:
 * the FIRE step at which systems move to the latency-oriented gather form (the tail of a batch
   is a few slow systems, which want more threads each).
 
+The per-class picks are timed one class at a time, while in a real run the classes share the GPU;
+so the whole tuned shape is checked against the library's default shape on a full relaxation of
+the sample, and the default is kept when it is faster.  Copies of sample systems (when the sample
+is smaller than the probe) start at other lateral positions: identical copies would share their
+grid lines in L2 and make memory-bound shapes look faster than they are on distinct systems.
+
 Everything is timed with the library's own CUDA-event timer (``RelaxMulti.last_timing``) around
 the relaxation launches; each candidate runs from the same start positions.
 """
@@ -104,14 +110,25 @@ class Autotuner:
         rep_f = max(1.0, min(float(full_count or len(Zs)), float(self.max_probe_systems)) / len(Zs))
 
         def replicate(idx):
+            """probe systems for sample systems idx: (sample index, copy number) towards full_count"""
             k = max(1, int(round(len(idx) * rep_f)))
-            return [int(idx[j % len(idx)]) for j in range(k)]
+            return [(int(idx[j % len(idx)]), j // len(idx)) for j in range(k)]
+
+        def start(i, copy):
+            """start positions of a copy of sample system i: copies after the first move laterally
+            (the grid is periodic in x and y), so that they read other grid lines, as distinct systems
+            of the real run do, instead of sharing the original's cached lines"""
+            if copy == 0:
+                return poss[i]
+            shift = np.array([(copy * 0.6180339887) % 1.0, (copy * 0.4142135624) % 1.0, 0.0]) * 37.0
+            return np.asarray(poss[i], float) + shift
         classes = sorted({_class_of(int(k)) for k in n})
         # 1. per class: form and threads per system of stage 0 (probe_steps from the start positions)
         best_forms = {}
         for c in classes:
             idx = np.nonzero([_class_of(int(k)) == c for k in n])[0]
-            sys_idx = replicate(idx)                          # systems of this class in the probe
+            probe = replicate(idx)                            # systems of this class in the probe
+            sys_idx = [i for i, _ in probe]
             pos_of = {int(i): j for j, i in enumerate(idx)}
             best = None
             for t in _candidates(c):
@@ -119,7 +136,7 @@ class Autotuner:
                 try:
                     R.set_team_size(c, t)
                     tids = R.add_molecules([Zs[i] for i in idx], [poss[i] for i in idx], [qs[i] for i in idx])
-                    slots = R.add_systems([tids[pos_of[i]] for i in sys_idx], [poss[i] for i in sys_idx])
+                    slots = R.add_systems([tids[pos_of[i]] for i in sys_idx], [start(i, cp) for i, cp in probe])
                     for form in (FORM_ROUNDS, FORM_OWNER):
                         R.set_stages([0], [form], [0])
                         self._rate(R, slots, n[sys_idx], 5)   # first launch of this shape: not timed
@@ -141,14 +158,31 @@ class Autotuner:
                 score[form] += w / max(r, 1e-9)
         res.form0 = min(score, key=score.get)
         # 2. interaction tiling and 3. the tail switch, on the whole sample (replicated)
-        all_idx = replicate(np.arange(len(Zs)))
+        all_probe = replicate(np.arange(len(Zs)))
+        all_idx = [i for i, _ in all_probe]
         n_all = n[all_idx]
-        R = self.make_handle(len(all_idx), int(n_all.sum()))
+        handles = []
+
+        def sample_handle(teams):
+            H = self.make_handle(len(all_idx), int(n_all.sum()))
+            handles.append(H)
+            for c, t in teams.items():
+                H.set_team_size(c, t)
+            tids = H.add_molecules(Zs, poss, qs)
+            return H, H.add_systems([tids[i] for i in all_idx], [start(i, cp) for i, cp in all_probe])
+
+        def full_ms(H, slots):
+            """device ms of a full relaxation of the sample (best of two) and its step counts"""
+            best = None
+            for _ in range(2):
+                H.reset_fire(slots)
+                H.run_fire(self.max_steps, step_budget=self.max_steps, **self.fire)
+                ms = H.last_timing()[0]
+                best = ms if best is None else min(best, ms)
+            return best, H.download(slots, pos=False, forces=False)["steps"]
+
         try:
-            for c, t in res.team_by_class.items():
-                R.set_team_size(c, t)
-            tids = R.add_molecules(Zs, poss, qs)
-            slots = R.add_systems([tids[i] for i in all_idx], [poss[i] for i in all_idx])
+            R, slots = sample_handle(res.team_by_class)
             n = n_all
             R.set_stages([0], [res.form0], [0])
             best_l, best_r = 0, -1.0
@@ -163,10 +197,19 @@ class Autotuner:
             res.nb_lanes = best_l
             R.set_nb_lanes(best_l)
             # full relaxation of the sample in the throughput form: the step distribution
-            R.reset_fire(slots)
-            R.run_fire(self.max_steps, step_budget=self.max_steps, **self.fire)
-            base_ms = R.last_timing()[0]
-            steps = R.download(slots, pos=False, forces=False)["steps"]
+            base_ms, steps = full_ms(R, slots)
+            # the per-class picks were timed one class at a time, but in the real run the classes
+            # share the GPU: keep them only if the whole shape beats the library's default shape
+            D, dslots = sample_handle({})
+            D.set_stages([0], [FORM_ROUNDS], [0])
+            D.set_nb_lanes(0)
+            def_ms, def_steps = full_ms(D, dslots)
+            res.timings["relax_ms_tuned_shape"] = base_ms
+            res.timings["relax_ms_default_shape"] = def_ms
+            self._log(f"tuned shape {base_ms:.1f} ms, default shape {def_ms:.1f} ms")
+            if def_ms < base_ms:
+                res.team_by_class, res.form0, res.nb_lanes = {}, FORM_ROUNDS, 0
+                R, slots, base_ms, steps = D, dslots, def_ms, def_steps
             cands = [((0,), (res.form0,), (0,), base_ms)]
             for q in (0.5, 0.65, 0.8):
                 s1 = int(np.quantile(steps, q))
@@ -186,5 +229,6 @@ class Autotuner:
             res.timings["relax_ms_single_stage"] = base_ms
             res.timings["relax_ms_tuned"] = ms
         finally:
-            R.finish()
+            for H in handles:
+                H.finish()
         return res
