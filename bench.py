@@ -459,7 +459,9 @@ def run_ragged(args, ws, rank, local):
     else:
         rng = np.random.default_rng(SEED)
         pick = np.sort(rng.choice(nsys, size=min(nsys, RAGGED["tune_sample"]), replace=False))
-        tune = Autotuner(make_handle, fire, probe_steps=100, max_steps=max_steps, max_probe_systems=4096).tune(
+        # the probes hold as many systems as the real run (copies of the sample, moved laterally):
+        # with fewer, one wave fits on the GPU and latency-oriented shapes win the probe but not the run
+        tune = Autotuner(make_handle, fire, probe_steps=100, max_steps=max_steps, max_probe_systems=nsys).tune(
             [w.Z[i] for i in pick], [w.pos[i] for i in pick], [w.q[i] for i in pick], full_count=nsys)
     ttune = time.perf_counter() - t0
     R = make_handle(nsys, int(natoms.sum()))

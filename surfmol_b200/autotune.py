@@ -104,7 +104,8 @@ class Autotuner:
     def tune(self, Zs, poss, qs, full_count: int | None = None) -> TuneResult:
         """Zs / poss / qs: a sample of the workload; full_count: systems in the whole workload.  The
         probes replicate the sample towards full_count (at most max_probe_systems), so the GPU is
-        as full as in the real run: occupancy decides which team size wins."""
+        as full as in the real run: occupancy decides which team size wins.  A probe that fits on
+        the GPU in one wave measures latency, and favours large teams that lose on a full run."""
         n = np.array([len(z) for z in Zs])
         res = TuneResult()
         rep_f = max(1.0, min(float(full_count or len(Zs)), float(self.max_probe_systems)) / len(Zs))
