@@ -69,6 +69,17 @@ def _class_of(n):
     return CLASS_MAX[-1]
 
 
+def copy_start(pos, copy: int):
+    """Start positions of probe copy `copy` of a sample system: copy 0 is the system itself; later
+    copies move laterally by a low-discrepancy offset of up to 37 A (the grid is periodic in x and
+    y), so that they read other grid lines, as distinct systems of the real run do, instead of
+    sharing the original's cached lines.  z is unchanged."""
+    if copy == 0:
+        return pos
+    shift = np.array([(copy * 0.6180339887) % 1.0, (copy * 0.4142135624) % 1.0, 0.0]) * 37.0
+    return np.asarray(pos, float) + shift
+
+
 def _candidates(cmax):
     lo = {64: 32, 160: 32, 448: 64, 1024: 128}.get(cmax, 256)
     return [t for t in TEAMS if t >= lo][:3]
@@ -116,13 +127,7 @@ class Autotuner:
             return [(int(idx[j % len(idx)]), j // len(idx)) for j in range(k)]
 
         def start(i, copy):
-            """start positions of a copy of sample system i: copies after the first move laterally
-            (the grid is periodic in x and y), so that they read other grid lines, as distinct systems
-            of the real run do, instead of sharing the original's cached lines"""
-            if copy == 0:
-                return poss[i]
-            shift = np.array([(copy * 0.6180339887) % 1.0, (copy * 0.4142135624) % 1.0, 0.0]) * 37.0
-            return np.asarray(poss[i], float) + shift
+            return copy_start(poss[i], copy)
         classes = sorted({_class_of(int(k)) for k in n})
         # 1. per class: form and threads per system of stage 0 (probe_steps from the start positions)
         best_forms = {}

@@ -77,3 +77,17 @@ def test_rejects_overbonded_atom():
     pos = np.array([[0, 0, 0], [1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1]], float)
     with pytest.raises(SmrError):
         Topology([6, 1, 1, 1, 1, 1], pos)
+
+
+def test_autotuner_probe_copies_move_laterally():
+    """Probe copies of a sample system keep its shape and height and sit at distinct lateral offsets."""
+    from surfmol_b200.autotune import copy_start
+    P = np.random.default_rng(0).normal(0, 3, (30, 3))
+    assert copy_start(P, 0) is P
+    shifts = []
+    for c in range(1, 8):
+        Q = copy_start(P, c)
+        d = Q - P
+        assert np.allclose(d, d[0]) and d[0, 2] == 0.0 and 0 <= d[0, 0] < 37 and 0 <= d[0, 1] < 37
+        shifts.append(tuple(np.round(d[0, :2], 6)))
+    assert len(set(shifts)) == len(shifts)
