@@ -1200,6 +1200,22 @@ int orc_relax_batch(int nsys, const orc_sys* const* S, double* const* pos, const
     return 0;
 }
 
+// getLJQH (UFF.cl:82-95) on n pairs: dp (n x 3), mixed REQij (n x 4: R0, E0, Q, H) -> (fx, fy, fz, E)
+void orc_ljqh_pairs(int n, const double* dp, const double* reqij, double R2damp, double* out) {
+    for (int i = 0; i < n; i++) {
+        V3 f;
+        const double E = getLJQH(V3{dp[3 * i], dp[3 * i + 1], dp[3 * i + 2]}, reqij[4 * i], reqij[4 * i + 1], reqij[4 * i + 2],
+                                 R2damp, f);
+        out[4 * i] = f.x; out[4 * i + 1] = f.y; out[4 * i + 2] = f.z; out[4 * i + 3] = E;
+    }
+}
+
+// fe3d_pbc_comb (UFF.cl:1459-1511) at np points u (grid units, np x 3) with prefactors PLQH (np x 4):
+// (dE/du_x, dE/du_y, dE/du_z, E) per point
+void orc_sample_points(const orc_grid* g, int np, const double* u, const double* plqh, double* out) {
+    for (int i = 0; i < np; i++) sample_grid(*g, plqh + 4 * i, V3{u[3 * i], u[3 * i + 1], u[3 * i + 2]}, out + 4 * i);
+}
+
 int orc_max_threads() {
 #ifdef _OPENMP
     return omp_get_max_threads();

@@ -79,6 +79,8 @@ def lib():
                                           C.c_double, C.c_int, C.c_double, DP]
         L.orc_substrate_direct.argtypes = [C.c_int, DP, DP, C.c_int, DP, DP, C.c_double, C.c_double, C.c_int,
                                            C.c_double, C.c_double, C.c_double, DP]
+        L.orc_ljqh_pairs.argtypes = [C.c_int, DP, DP, C.c_double, DP]
+        L.orc_sample_points.argtypes = [C.POINTER(OrcGrid), C.c_int, DP, DP, DP]
         _lib = L
     return _lib
 
@@ -321,6 +323,23 @@ def langevin_noise(n, seed):
 
 def max_threads():
     return lib().orc_max_threads()
+
+
+def ljqh_pairs(dp, reqij, rdamp=1.0):
+    """getLJQH (UFF.cl:82-95) in FP64 on pairs: dp (n, 3), mixed REQij (n, 4) -> (n, 4) (f, E)."""
+    dp, reqij = _d(dp).reshape(-1, 3), _d(reqij).reshape(-1, 4)
+    out = np.zeros((len(dp), 4))
+    lib().orc_ljqh_pairs(len(dp), _dp(dp), _dp(reqij), float(rdamp) ** 2, _dp(out))
+    return out
+
+
+def sample_points(grid: Grid, u, plqh):
+    """fe3d_pbc_comb (UFF.cl:1459-1511) in FP64: u (n, 3) grid units, PLQH (n, 4) -> (n, 4)
+    (dE/du_x, dE/du_y, dE/du_z, E)."""
+    u, plqh = _d(u).reshape(-1, 3), _d(plqh).reshape(-1, 4)
+    out = np.zeros((len(u), 4))
+    lib().orc_sample_points(grid.ptr(), len(u), _dp(u), _dp(plqh), _dp(out))
+    return out
 
 
 def morse_points(pts, ions, ion_req, Lx, Ly, npbc=1, alpha=1.5):
