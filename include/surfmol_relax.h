@@ -79,12 +79,17 @@ typedef struct {
 } smr_fire_params;
 
 /* Non-bonded / grid-coupling parameters: GFFParams.x (rdamp), GFFParams.y (Morse alpha)
- * of opencl/UFF.cl:1534-1545; rcut <= 0 keeps every intramolecular pair. */
+ * of opencl/UFF.cl:1534-1545; rcut <= 0 keeps every intramolecular pair.
+ * excl13 = 0: bonded (1-2) pairs excluded, getNonBond_GridFF_Bspline (UFF.cl:1524-1718);
+ * excl13 = 1: 1-2 and 1-3 pairs excluded, getNonBond_GridFF_Bspline_ex2 (UFF.cl:1722-1930)
+ * with the exclusion lists of NonBondedFF::make_second_neighs (molff/src/nonbonded.rs:112-137).
+ * A system with PBC images runs only with excl13 = 0 (the reference has no image-aware 1-3
+ * list builder); smr_run_fire / smr_eval_forces refuse the combination with SMR_ERR_ARG. */
 typedef struct {
     float rdamp;
     float alpha_morse;
     float rcut;
-    int   reserved;
+    int   excl13;
 } smr_nb_params;
 
 /* Grid build: Morse (Pauli, London) image sums + Ewald-2D Coulomb, exact B-spline fit. */
@@ -161,15 +166,18 @@ int smr_build_grid(smr_handle* h, int nions, const double* ions, const double* i
                    const smr_grid_build_params* p);
 /* Allocation-free grid build.  No counterpart in the reference.  For callers that cannot call
  * cudaMalloc (a host that owns all device memory through its own pool and forbids allocation
- * after start-up, or code issuing work during stream capture): builds the same float32 grid as
- * smr_build_grid, without a handle, into coef_out (a DEVICE buffer of nx*ny*nz*4 floats the
- * caller owns), on the caller's stream (void* cudaStream_t; 0 = default stream), asynchronously.
- * ions / ion_re are host arrays as for smr_build_grid.  Scratch is one 8 MiB static device array
- * per GPU (held until exit): three FP64 channels (24 B per voxel) plus the Ewald tables must fit,
- * i.e. at most ~340,000 voxels (less for large cells or many ions), 4 <= nx, ny, nz <= 512.
- * Larger requests fail with SMR_ERR_CAPACITY and a message in err.  The first call on a device looks up the array's address (make it before any
- * stream capture); calls whose GPU work overlaps share the array and race.  Returns SMR_OK or a
- * negative SMR_ERR_* code; never allocates device memory. */
+ * after start-up): builds the same float32 grid as smr_build_grid, without a handle, into
+ * coef_out (a DEVICE buffer of nx*ny*nz*4 floats the caller owns), on the caller's stream
+ * (void* cudaStream_t; 0 = default stream), asynchronously: order later uses of coef_out, and
+ * other static builds, after that stream's work.  ions / ion_re are host arrays as for
+ * smr_build_grid; pinned ones must stay unchanged until the stream's work is done (pageable ones
+ * are copied before the call returns).  Scratch is one 8 MiB static device array per GPU (held
+ * until exit): three FP64 channels (24 B per voxel) plus the Ewald tables must fit, i.e. at most
+ * ~340,000 voxels (less for large cells or many ions), 4 <= nx, ny, nz <= 512.  Larger requests
+ * fail with SMR_ERR_CAPACITY and a message in err.  The first call on a device looks up the
+ * array's device address (make it before any stream capture); calls whose GPU work overlaps
+ * share the array and race.  Returns SMR_OK or a negative SMR_ERR_* code; never allocates
+ * device memory. */
 typedef struct {
     double alpha_morse;
     int    npbc;

@@ -31,7 +31,7 @@ class SmrFireParams(C.Structure):
 
 
 class SmrNbParams(C.Structure):
-    _fields_ = [("rdamp", C.c_float), ("alpha_morse", C.c_float), ("rcut", C.c_float), ("reserved", C.c_int)]
+    _fields_ = [("rdamp", C.c_float), ("alpha_morse", C.c_float), ("rcut", C.c_float), ("excl13", C.c_int)]
 
 
 class SmrFoldedSurface(C.Structure):

@@ -459,6 +459,7 @@ KernelArgs base_args(smr_handle* h) {
     a.R2damp = h->nb.rdamp * h->nb.rdamp;
     a.alpha_morse = h->nb.alpha_morse;
     a.rc2 = h->nb.rcut > 0 ? h->nb.rcut * h->nb.rcut : 3.0e38f;
+    a.excl13 = h->nb.excl13 ? 1 : 0;
     return a;
 }
 
@@ -472,8 +473,8 @@ int latency_team_for(int requested, int n) {
 
 // Launch segments for a list of slots.  The form of every system is decided from the system
 // alone (the requested form when the topology supports it and its own shared memory fits, else
-// the rounds form with its topology's team; periodic or constrained systems always the extended
-// gather form), never from what it is batched with; segments group
+// the rounds form with its topology's team; periodic or constrained systems, and all systems
+// under 1-3 exclusion, always the extended gather form), never from what it is batched with; segments group
 // equal (form, team) and are split wherever the segment's largest system would no longer fit.
 std::vector<Seg> group_by(smr_handle* h, std::vector<int>& ids, int form, int req_team = 0) {
     struct Key { int form, team, n, nf; };
@@ -481,8 +482,9 @@ std::vector<Seg> group_by(smr_handle* h, std::vector<int>& ids, int form, int re
         const SlotState& st = h->hs[s];
         const TopoDev& td = h->htd[st.topo];
         const int n = st.natoms, nf = td.npieces;
-        if (st.flags) {
-            // periodic or constrained systems: the extended gather form, whatever the stage's form
+        if (st.flags || h->nb.excl13) {
+            // periodic or constrained systems, and every system while 1-3 exclusion is on: the
+            // extended gather form, whatever the stage's form
             const int t = req_team ? req_team : td.team;
             if (team_smem_bytes(n, nf, t, FORM_GATHER_EXT) <= h->smem_optin) return Key{FORM_GATHER_EXT, t, n, nf};
             return Key{FORM_GATHER_EXT, std::max(td.team, n > 1024 ? 512 : 256), n, nf};
@@ -564,6 +566,19 @@ int check_batch(smr_handle* h, int nsys, const int* ids) {
     return 0;
 }
 
+// excl13 (1-3 exclusion) is defined for systems without PBC images only
+int check_excl13(smr_handle* h, const int* ids, int n) {
+    if (!h->nb.excl13 || h->hlat.empty()) return 0;
+    for (int i = 0; i < n; i++) {
+        const int s = ids[i];
+        if (!(h->hs[s].flags & SLOT_PBC)) continue;
+        const float4* L = &h->hlat[3 * (size_t)s];
+        if (L[0].w + L[1].w + L[2].w > 0.f)
+            return fail(h, SMR_ERR_ARG, "slot %d has PBC images: 1-3 exclusion (excl13) is defined for systems without images", s);
+    }
+    return 0;
+}
+
 }  // namespace
 
 // ====================================================================== API
@@ -638,6 +653,7 @@ int smr_destroy(smr_handle* h) {
 int smr_set_nb_params(smr_handle* h, const smr_nb_params* p) {
     if (!h || !p) return SMR_ERR_ARG;
     if (!(p->rdamp >= 0.f) || !(p->alpha_morse > 0.f)) return fail(h, SMR_ERR_ARG, "rdamp must be >= 0 and alpha_morse > 0");
+    if (p->excl13 != 0 && p->excl13 != 1) return fail(h, SMR_ERR_ARG, "excl13 must be 0 or 1");
     h->nb = *p;
     return SMR_OK;
 }
@@ -1335,6 +1351,7 @@ int smr_eval_forces(smr_handle* h, int nsys, const int* slot_ids, float* forces,
     if (!h || nsys < 0 || (nsys && !slot_ids)) return SMR_ERR_ARG;
     SETTLE(h);
     { int r = check_batch(h, nsys, slot_ids); if (r) return r; }
+    { int r = check_excl13(h, slot_ids, nsys); if (r) return r; }
     if (nsys == 0) return SMR_OK;
     std::vector<int> sorted(slot_ids, slot_ids + nsys);
     auto segs = group_by(h, sorted, h->eval_form, h->eval_team);
@@ -1471,6 +1488,12 @@ int smr_run_fire(smr_handle* h, int max_steps, int step_budget, const smr_fire_p
     SETTLE(h);
     if (mode != SMR_MODE_BATCHED && mode != SMR_MODE_PLAIN) return fail(h, SMR_ERR_ARG, "unknown mode %d", mode);
     if (!(p->dt0 > 0 && p->dt_max > 0 && p->f_dec > 0 && p->f_inc > 0)) return fail(h, SMR_ERR_ARG, "invalid FIRE parameters");
+    {
+        std::vector<int> run;
+        for (int s = 0; s < h->max_systems; s++) if (h->hs[s].active && h->hs[s].status == SMR_ST_RUNNING) run.push_back(s);
+        int r = check_excl13(h, run.data(), (int)run.size());
+        if (r) return r;
+    }
     // every running slot may advance to min(steps + max_steps, step_budget) in this call
     std::vector<int> ids;
     std::vector<int> start(h->max_systems, 0);

@@ -32,6 +32,7 @@
 #include <cuda_bf16.h>
 #include <cstdio>
 #include <map>
+#include <mutex>
 #include <tuple>
 #include <type_traits>
 
@@ -259,6 +260,32 @@ __device__ __forceinline__ void ljq_pair(float dx, float dy, float dz, bool skip
     E += w * ((u6 - 2.0f) * vdW + Ec);
     const float fr = w * (-12.0f * (u6 - 1.0f) * vdW * ir2 - Ec * (rs * rs));
     fx += dx * fr; fy += dy * fr; fz += dz * fr;
+}
+
+// 1-3 exclusion (getNonBond_GridFF_Bspline_ex2, UFF.cl:1722-1930, with the lists of
+// make_second_neighs, molff/src/nonbonded.rs:112-137): the partners of atom i excluded beyond its
+// own bonds are its neighbours' neighbours.  They are read from the team's neighbour table in
+// shared memory; entries may repeat or name i itself, which is excluded anyway.
+struct Excl13 { short4 a, b, c, d; };
+
+__device__ __forceinline__ short4 ng_or_none(const Smem& S, int g) {
+    return g >= 0 ? S.Ng()[g] : make_short4(-1, -1, -1, -1);
+}
+__device__ __forceinline__ Excl13 excl13_of(const Smem& S, short4 ng) {
+    return Excl13{ng_or_none(S, ng.x), ng_or_none(S, ng.y), ng_or_none(S, ng.z), ng_or_none(S, ng.w)};
+}
+__device__ __forceinline__ bool in4(int j, short4 v) { return (j == v.x) | (j == v.y) | (j == v.z) | (j == v.w); }
+__device__ __forceinline__ bool is13(int j, const Excl13& e) { return in4(j, e.a) | in4(j, e.b) | in4(j, e.c) | in4(j, e.d); }
+// the neighbours of atom g as bits of a 64-bit mask (systems of <= 64 atoms)
+__device__ __forceinline__ unsigned long long ng_bits(const Smem& S, int g) {
+    if (g < 0) return 0ull;
+    const short4 n = S.Ng()[g];
+    unsigned long long m = 0ull;
+    if (n.x >= 0) m |= 1ull << (n.x & 63);
+    if (n.y >= 0) m |= 1ull << (n.y & 63);
+    if (n.z >= 0) m |= 1ull << (n.z & 63);
+    if (n.w >= 0) m |= 1ull << (n.w & 63);
+    return m;
 }
 
 // One pair of the team's atoms i, j (compensated positions); excluded pairs and, under a cutoff,
@@ -762,7 +789,7 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
     }
 
     // C: intramolecular LJ + damped Coulomb over all pairs except bonded (1-2) neighbours
-    // (opencl/UFF.cl:57-95, 1595-1665).  Excluded pairs are evaluated at r2 = 1 and masked out,
+    // (opencl/UFF.cl:57-95, 1595-1665), or except 1-2 and 1-3 pairs with excl13 (UFF.cl:1722-1930).  Excluded pairs are evaluated at r2 = 1 and masked out,
     // so the partner loop has no branch and independent pairs overlap.
     {
         // with a neighbour list the partner count, not N, sets the lanes per atom
@@ -799,10 +826,27 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
                     if (ng.y >= 0) ex |= 1ull << (ng.y & 63);
                     if (ng.z >= 0) ex |= 1ull << (ng.z & 63);
                     if (ng.w >= 0) ex |= 1ull << (ng.w & 63);
+                    // 1-3 exclusion is compiled into the extended form only (the host runs every
+                    // system in that form while it is on), so the other forms keep their registers
+                    if (FORM == FORM_GATHER_EXT && a.excl13) {
+                        if (small) {
+                            ex |= ng_bits(S, ng.x) | ng_bits(S, ng.y) | ng_bits(S, ng.z) | ng_bits(S, ng.w);
+                            for (int j = cp; j < N; j += Lp)
+                                nb_pair<CUT>(a, pi, li, qi, S.P()[j], S.Lo()[j], S.Q()[j], (bool)((ex >> j) & 1ull), fx, fy, fz, E);
+                        } else {
+                            const Excl13 e13 = excl13_of(S, ng);
+#pragma unroll 2
+                            for (int j = cp; j < N; j += Lp) {
+                                const bool excl = (j == i) | in4(j, ng) | is13(j, e13);
+                                nb_pair<CUT>(a, pi, li, qi, S.P()[j], S.Lo()[j], S.Q()[j], excl, fx, fy, fz, E);
+                            }
+                        }
+                    } else {
 #pragma unroll 4
-                    for (int j = cp; j < N; j += Lp) {
-                        const bool excl = small ? (bool)((ex >> j) & 1ull) : (j == i || j == ng.x || j == ng.y || j == ng.z || j == ng.w);
-                        nb_pair<CUT>(a, pi, li, qi, S.P()[j], S.Lo()[j], S.Q()[j], excl, fx, fy, fz, E);
+                        for (int j = cp; j < N; j += Lp) {
+                            const bool excl = small ? (bool)((ex >> j) & 1ull) : (j == i || j == ng.x || j == ng.y || j == ng.z || j == ng.w);
+                            nb_pair<CUT>(a, pi, li, qi, S.P()[j], S.Lo()[j], S.Q()[j], excl, fx, fy, fz, E);
+                        }
                     }
                 }
             }
@@ -1198,20 +1242,27 @@ int launch_t(const KernelArgs& a, cudaStream_t s, int num_sms) {
     const size_t state = (size_t)tpb * team_bytes(a.nmax, a.nfmax, T, FORM);
     const size_t smem = GS ? 0 : state;           // global-state launches use no dynamic shared memory
     auto kern = relax_kernel<T, GDT, EVAL, FORM, GS>;
-    static std::map<size_t, int> occ_cache;
-    int occ;
-    auto it = occ_cache.find(smem);
-    if (it == occ_cache.end()) {
-        if (smem > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e != cudaSuccess) return (int)e;
-        }
+    // blocks per SM of this instance, per (device, dynamic shared memory); handles driven from
+    // several host threads (one per GPU, say) share the cache under its lock
+    static std::mutex occ_mu;
+    static std::map<std::pair<int, size_t>, int> occ_cache;
+    int dev = 0;
+    { cudaError_t e = cudaGetDevice(&dev); if (e != cudaSuccess) return (int)e; }
+    int occ = -1;
+    {
+        std::lock_guard<std::mutex> lk(occ_mu);
+        auto it = occ_cache.find({dev, smem});
+        if (it != occ_cache.end()) occ = it->second;
+    }
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return (int)e;
+    }
+    if (occ < 0) {
         cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, block, smem);
         if (e != cudaSuccess) return (int)e;
-        occ_cache[smem] = occ;
-    } else {
-        occ = it->second;
-        if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        std::lock_guard<std::mutex> lk(occ_mu);
+        occ_cache[{dev, smem}] = occ;
     }
     if (occ < 1) return (int)cudaErrorInvalidConfiguration;
     int blocks_needed = (a.nwork + tpb - 1) / tpb;

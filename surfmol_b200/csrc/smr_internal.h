@@ -114,6 +114,7 @@ struct KernelArgs {
     GridView grid; int has_grid;
     FoldedView fold;              // fold.on: the substrate is the folded surface, not the grid
     float R2damp, alpha_morse, rc2;
+    int excl13;                   // 1: 1-3 pairs excluded too (getNonBond_GridFF_Bspline_ex2)
     FireDev fire;
     int phase_limit;              // this launch runs a system until SlotState::steps reaches min(target, phase_limit)
     int step_budget;              // a system reaching this many steps gets SMR_ST_MAXSTEPS (<=0: none)

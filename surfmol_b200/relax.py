@@ -190,8 +190,11 @@ class RelaxMulti:
             raise SmrError(f"{what} ({r}): {self.L.smr_last_error(self.h).decode()}")
 
     # -- parameters and grid
-    def set_nb(self, rdamp=1.0, alpha_morse=1.5, rcut=0.0):
-        p = N.SmrNbParams(rdamp, alpha_morse, rcut, 0)
+    def set_nb(self, rdamp=1.0, alpha_morse=1.5, rcut=0.0, excl13=False):
+        """GFFParams (rdamp, Morse alpha), intramolecular cutoff (<= 0: none) and the exclusion
+        rule: 1-2 pairs (getNonBond_GridFF_Bspline) or, with excl13, 1-2 and 1-3 pairs
+        (getNonBond_GridFF_Bspline_ex2)."""
+        p = N.SmrNbParams(rdamp, alpha_morse, rcut, 1 if excl13 else 0)
         self._chk(self.L.smr_set_nb_params(self.h, C.byref(p)), "smr_set_nb_params")
 
     def set_grid(self, coef, p0, step, dtype=GRID_F32, scale=(1, 1, 1, 1), plane_scale=None):
