@@ -559,7 +559,7 @@ int grid_from_raw_device(const double* raw, int nx, int ny, int nz, float4* out,
 // smr_build_grid_static: the same grid as smr_build_grid for small substrates, for callers that
 // cannot call cudaMalloc -- e.g. a host framework that owns all device memory through its own
 // pool and forbids allocation after start-up (the reference's GPU harness forbids allocation in
-// its step path), or code issuing work while a CUDA stream is being captured.  All scratch lives
+// its step path).  All scratch lives
 // in the file-scope array below: kStaticScratchBytes (8 MiB) held by every GPU that loads the
 // library, until the process exits.  In host code the array's name is only a host-side stand-in,
 // so the entry point looks up its device address with cudaGetSymbolAddress, once per device, on
@@ -622,12 +622,36 @@ __global__ void static_stage1(int H, int K, const double2* __restrict__ S, doubl
     B[t] = make_double2(br, bi);
 }
 
-// Thomas tables on the host stack (n <= kStaticMaxLine)
+// Thomas tables of the exact cubic B-spline fit for a line of n <= kStaticMaxLine points:
+// cp, m of tridiag(1/6, b0 | 2/3 | bn, 1/6), and for the cyclic lines (Sherman-Morrison) the
+// solved correction vector u.  Used by the host (for the scalar denominators) and by the device
+// kernel that writes the tables into the static scratch.
 constexpr int kStaticMaxLine = 512;
-void thomas_stack(int n, double b0, double bn, double* cp, double* m) {
+__host__ __device__ void thomas_tables(int n, double b0, double bn, double* cp, double* m) {
     const double a = 1.0 / 6.0, b = 2.0 / 3.0;
     m[0] = b0; cp[0] = a / m[0];
     for (int i = 1; i < n; i++) { const double di = (i == n - 1) ? bn : b; m[i] = di - a * cp[i - 1]; cp[i] = a / m[i]; }
+}
+__host__ __device__ void cyclic_u(int n, const double* cp, const double* m, double* u) {
+    const double a = 1.0 / 6.0, gamma = -2.0 / 3.0;
+    for (int i = 0; i < n; i++) u[i] = 0.0;
+    u[0] = gamma; u[n - 1] = a;
+    u[0] /= m[0];
+    for (int i = 1; i < n; i++) u[i] = (u[i] - a * u[i - 1]) / m[i];
+    for (int i = n - 2; i >= 0; i--) u[i] -= cp[i] * u[i + 1];
+}
+
+// One thread: the tables of the z (open), y and x (cyclic) lines into the static scratch;
+// the table pointers travel by value as a kernel argument.
+struct TabPtrs { double* p[8]; };
+__global__ void static_fit_tables(int nz, int ny, int nx, TabPtrs t) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const double a = 1.0 / 6.0, b = 2.0 / 3.0, gamma = -b;
+    thomas_tables(nz, b, b, t.p[0], t.p[1]);
+    thomas_tables(ny, b - gamma, b - a * a / gamma, t.p[2], t.p[3]);
+    cyclic_u(ny, t.p[2], t.p[3], t.p[4]);
+    thomas_tables(nx, b - gamma, b - a * a / gamma, t.p[5], t.p[6]);
+    cyclic_u(nx, t.p[5], t.p[6], t.p[7]);
 }
 
 }  // namespace
@@ -652,7 +676,12 @@ extern "C" int smr_build_grid_static(int nions, const double* ions, const double
     const double g1 = 2.0 * kPi / Lx, g2 = 2.0 * kPi / Ly, area = Lx * Ly;
     const double tol = p->ewald_tol > 0 ? p->ewald_tol : 1e-12;
     const double gmax = -std::log(tol) / dmin;
-    const int H = std::max(1, (int)std::floor(gmax / g1)), K = std::max(1, (int)std::floor(gmax / g2));
+    // reciprocal-lattice extents, bounded before the conversion to int (a large cell or a grid
+    // bottom close to the top ion gives quotients far beyond what the scratch could hold)
+    const double hq = std::floor(gmax / g1), kq = std::floor(gmax / g2);
+    if (!(hq <= 1e5 && kq <= 1e5)) return fail(-3, "reciprocal sum too large for the static scratch (raise ewald_tol or "
+                                                   "the grid bottom above the slab)");
+    const int H = std::max(1, (int)hq), K = std::max(1, (int)kq);
     const int w = 2 * H + 1, nk = 2 * K + 1;
     const size_t N = (size_t)nx * ny * nz;
     auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
@@ -693,36 +722,36 @@ extern "C" int smr_build_grid_static(int nions, const double* ions, const double
     const float rc2 = p->morse_rcut > 0 ? (float)(p->morse_rcut * p->morse_rcut) : 3.0e38f;
     morse_kernel<<<(unsigned)((N + 127) / 128), 128, 0, s>>>(nions, dions, dre, Lx, Ly, p->npbc, 0, nx, ny, nz, p0[0], p0[1], p0[2],
                                                              step[0], step[1], step[2], (float)p->alpha_morse, rc2, paul, lond);
-    static_structure_factor<<<(w * nk + 127) / 128, 128, 0, s>>>(nions, dions, p0[2], H, K, g1, g2, S);
-    static_phase<<<(w * nx + 255) / 256, 256, 0, s>>>(nx, H, p0[0], step[0], g1, Ex);
-    static_phase<<<(nk * ny + 255) / 256, 256, 0, s>>>(ny, K, p0[1], step[1], g2, Ey);
+    static_structure_factor<<<(unsigned)(((size_t)w * nk + 127) / 128), 128, 0, s>>>(nions, dions, p0[2], H, K, g1, g2, S);
+    static_phase<<<(unsigned)(((size_t)w * nx + 255) / 256), 256, 0, s>>>(nx, H, p0[0], step[0], g1, Ex);
+    static_phase<<<(unsigned)(((size_t)nk * ny + 255) / 256), 256, 0, s>>>(ny, K, p0[1], step[1], g2, Ey);
     ST_CHECK(cudaGetLastError());
     for (int iz = 0; iz < nz; iz++) {
         const double z = p0[2] + iz * step[2];
         const double phi0 = -(2.0 * kPi / area) * (qsum * z - qz);
-        static_stage1<<<(nk * nx + 127) / 128, 128, 0, s>>>(H, K, S, gmax, g1, g2, area, iz * step[2], nx, Ex, B);
+        static_stage1<<<(unsigned)(((size_t)nk * nx + 127) / 128), 128, 0, s>>>(H, K, S, gmax, g1, g2, area, iz * step[2], nx, Ex, B);
         ewald_stage2<<<(nx * ny + 127) / 128, 128, 0, s>>>(nk, B, Ey, nx, ny, 0, nx, phi0, iz, nz, coul);
     }
     ST_CHECK(cudaGetLastError());
-    // exact B-spline fit: z open, y and x cyclic (tables from the host stack)
+    // exact B-spline fit: z open, y and x cyclic.  The line tables are computed on the device
+    // into the scratch; the host computes only the two Sherman-Morrison denominators, from the
+    // same arithmetic, and passes them by value.
     const double a = 1.0 / 6.0, b = 2.0 / 3.0, gamma = -b;
-    double cp[kStaticMaxLine], m[kStaticMaxLine], u[kStaticMaxLine];
-    thomas_stack(nz, b, b, cp, m);
-    ST_CHECK(cudaMemcpyAsync(tab[0], cp, nz * 8, cudaMemcpyHostToDevice, s));
-    ST_CHECK(cudaMemcpyAsync(tab[1], m, nz * 8, cudaMemcpyHostToDevice, s));
+    {
+        TabPtrs t;
+        for (int k = 0; k < 8; k++) t.p[k] = tab[k];
+        static_fit_tables<<<1, 32, 0, s>>>(nz, ny, nx, t);
+        ST_CHECK(cudaGetLastError());
+    }
     double den[2];
-    for (int axis = 0; axis < 2; axis++) {
-        const int n = axis == 0 ? ny : nx;
-        thomas_stack(n, b - gamma, b - a * a / gamma, cp, m);
-        for (int i = 0; i < n; i++) u[i] = 0.0;
-        u[0] = gamma; u[n - 1] = a;
-        u[0] /= m[0];
-        for (int i = 1; i < n; i++) u[i] = (u[i] - a * u[i - 1]) / m[i];
-        for (int i = n - 2; i >= 0; i--) u[i] -= cp[i] * u[i + 1];
-        den[axis] = 1.0 + u[0] + a * u[n - 1] / gamma;
-        ST_CHECK(cudaMemcpyAsync(tab[2 + 3 * axis], cp, n * 8, cudaMemcpyHostToDevice, s));
-        ST_CHECK(cudaMemcpyAsync(tab[3 + 3 * axis], m, n * 8, cudaMemcpyHostToDevice, s));
-        ST_CHECK(cudaMemcpyAsync(tab[4 + 3 * axis], u, n * 8, cudaMemcpyHostToDevice, s));
+    {
+        double cp[kStaticMaxLine], m[kStaticMaxLine], u[kStaticMaxLine];
+        for (int axis = 0; axis < 2; axis++) {
+            const int n = axis == 0 ? ny : nx;
+            thomas_tables(n, b - gamma, b - a * a / gamma, cp, m);
+            cyclic_u(n, cp, m, u);
+            den[axis] = 1.0 + u[0] + a * u[n - 1] / gamma;
+        }
     }
     for (double* ch : {paul, lond, coul}) {
         fit_z<<<(nx * ny + 127) / 128, 128, 0, s>>>(ch, nx, ny, nz, tab[0], tab[1]);

@@ -1,7 +1,8 @@
 """Generate tests/golden/*.json from the reference's own files and documented answers.
 
-Run in a container that has the reference at /root/reference (read-only); the
-outputs are committed so the tests need no reference at run time.
+Run where the reference tree is present, naming it by SURFMOL_REFERENCE or as the first
+argument:  python tests/golden/make_golden.py <reference root>.  The outputs are committed,
+so the tests need no reference at run time.
 
 * pentacene.json  -- data/xyz/pentacene.xyz (36 atoms) plus the known answers of
   the reference's pentacene UFF test and docs:
@@ -18,9 +19,10 @@ outputs are committed so the tests need no reference at run time.
 """
 import json
 import os
+import sys
 
-REF = "/root/reference"
 HERE = os.path.dirname(os.path.abspath(__file__))
+REF = os.environ.get("SURFMOL_REFERENCE", "")
 
 
 def read_xyz(path):
@@ -48,6 +50,11 @@ def parse_dat(path, min_cols):
 
 
 def main():
+    global REF
+    if len(sys.argv) > 1:
+        REF = sys.argv[1]
+    if not REF or not os.path.isdir(REF):
+        sys.exit("give the reference root as the first argument or in SURFMOL_REFERENCE")
     el, pos = read_xyz(os.path.join(REF, "data/xyz/pentacene.xyz"))
     Zmap = {"H": 1, "C": 6, "N": 7, "O": 8}
     json.dump({
