@@ -384,8 +384,8 @@ int smr_set_team_size(smr_handle* h, int max_atoms, int threads);
  *                           when a cutoff is set (default 128; 0 = never): partners within
  *                           rc + skin, rebuilt when an atom has moved more than skin / 2
  *   SMR_TUNE_NBLIST_SKIN_MA skin in milli-Angstrom (default 1000)
- *   SMR_TUNE_NBLIST_CAP     partners per atom a list row holds (default 256; an atom with more
- *                           uses the all-pairs loop) */
+ *   SMR_TUNE_NBLIST_CAP     partners per atom a list row holds (default 256, a multiple of 4; an
+ *                           atom with more uses the all-pairs loop) */
 #define SMR_TUNE_NBLIST_MIN 2
 #define SMR_TUNE_NBLIST_SKIN_MA 3
 #define SMR_TUNE_NBLIST_CAP 4
@@ -394,6 +394,26 @@ int smr_set_team_size(smr_handle* h, int max_atoms, int threads);
  *                           next call on the handle first waits for it (bounded by the same limit)
  *                           and refreshes its copy of the per-system state, so no result is lost */
 #define SMR_TUNE_WATCHDOG_MS 5
+/*   SMR_TUNE_GRID_BRICKS    grid layout the relax kernel reads: -1 (default) the brick copy for
+ *                           grids larger than 128 MiB, 0 the z-fastest grid itself, 1 the brick
+ *                           copy always.  The copy holds each 128-byte piece of the interpolation
+ *                           stencil in one aligned line (8x the grid's memory); results are the
+ *                           same bit for bit either way */
+#define SMR_TUNE_GRID_BRICKS 6
+/*   SMR_TUNE_GRID_BRICKS_ACTIVE (smr_get_tuning only) 1 if the last launch read the brick copy */
+#define SMR_TUNE_GRID_BRICKS_ACTIVE 7
+/*   SMR_TUNE_GRID_PREFETCH  1: with the brick copy, each force evaluation starts by requesting its
+ *                           atoms' stencil lines into L2; 0 (default): no prefetch (on the ragged
+ *                           workload it measured 12 % slower) */
+#define SMR_TUNE_GRID_PREFETCH 8
+/*   SMR_TUNE_SMEM_CARVEOUT  preferred share of the SM's L1 given to shared memory for block teams,
+ *                           in percent (-1, default: the driver's choice)
+ *   SMR_TUNE_OCC_TIERS      1: launch segments of one form and team are split by the blocks per
+ *                           SM each system's shared memory allows, so small systems keep their
+ *                           occupancy; 0 (default): one segment per form and team (the split
+ *                           measured slower on the ragged workload) */
+#define SMR_TUNE_SMEM_CARVEOUT 9
+#define SMR_TUNE_OCC_TIERS 10
 int smr_set_tuning(smr_handle* h, int key, int value);
 int smr_get_tuning(smr_handle* h, int key, int* value);
 

@@ -1336,25 +1336,62 @@ void orc_substrate_direct(int np, const double* pts, const double* req_atom /*np
 // grids for the CPU baseline.
 int orc_build_grid_fast(int nions, const double* ions, const double* re, double Lx, double Ly,
                         int nx, int ny, int nz, const double* p0, const double* step, double alpha, int npbc, double gtol,
-                        double* coef) {
+                        double* coef, double morse_rcut) {
+    // Same values as orc_build_grid (make_MorseFF image sums, Ewald-2D, exact fit), evaluated
+    // faster: Morse over per-column lists of the ion images (with morse_rcut > 0 only those
+    // within morse_rcut of the column's points; 0 keeps every image, as make_MorseFF does), and
+    // the reciprocal sum from separable x / y phase tables, G terms below gtol of the largest
+    // amplitude at a plane skipped (their sum is below gtol relative).
     const size_t N = (size_t)nx * ny * nz;
-    double ztop = -1e300, qsum = 0, qz = 0;
-    for (int i = 0; i < nions; i++) { ztop = std::max(ztop, ions[4 * i + 2]); qsum += ions[4 * i + 3]; qz += ions[4 * i + 3] * ions[4 * i + 2]; }
+    double ztop = -1e300, zlow = 1e300, qsum = 0, qz = 0;
+    for (int i = 0; i < nions; i++) {
+        ztop = std::max(ztop, ions[4 * i + 2]); zlow = std::min(zlow, ions[4 * i + 2]);
+        qsum += ions[4 * i + 3]; qz += ions[4 * i + 3] * ions[4 * i + 2];
+    }
     const double dmin = p0[2] - ztop;
     if (!(dmin > 0)) return -1;
     std::vector<double> ch(3 * N);
+    // ion images (position, R, E) in the make_MorseFF image order
+    struct Img { double x, y, z, R, E; };
+    std::vector<Img> imgs;
+    for (int j = 0; j < nions; j++)
+        for (int iy = -npbc; iy <= npbc; iy++)
+            for (int ix = -npbc; ix <= npbc; ix++)
+                imgs.push_back({ions[4 * j] - ix * Lx, ions[4 * j + 1] - iy * Ly, ions[4 * j + 2], re[4 * j], re[4 * j + 1]});
+    const double zmax = p0[2] + (nz - 1) * step[2];
 #ifdef _OPENMP
 #pragma omp parallel for schedule(dynamic, 1)
 #endif
-    for (int ix = 0; ix < nx; ix++)
-        for (int iy = 0; iy < ny; iy++)
+    for (int ix = 0; ix < nx; ix++) {
+        std::vector<const Img*> col;
+        for (int iy = 0; iy < ny; iy++) {
+            const double x = p0[0] + ix * step[0], y = p0[1] + iy * step[1];
+            col.clear();
+            for (const Img& m : imgs) {
+                if (morse_rcut > 0) {
+                    const double dx = x - m.x, dy = y - m.y;
+                    // nearest z of the column to this ion (the column spans [p0z, zmax], ions lie below)
+                    const double dz = std::max(0.0, std::min(std::fabs(p0[2] - m.z), std::fabs(zmax - m.z)));
+                    if (dx * dx + dy * dy + dz * dz > morse_rcut * morse_rcut) continue;
+                }
+                col.push_back(&m);
+            }
             for (int iz = 0; iz < nz; iz++) {
-                V3 p{p0[0] + ix * step[0], p0[1] + iy * step[1], p0[2] + iz * step[2]};
-                size_t i = iz + (size_t)nz * (iy + (size_t)ny * ix);
-                double P_, L_;
-                morse_point(p, nions, ions, re, Lx, 0.0, 0.0, Ly, npbc, npbc, alpha, P_, L_);
+                const double z = p0[2] + iz * step[2];
+                double P_ = 0, L_ = 0;
+                for (const Img* m : col) {
+                    const double dx = x - m->x, dy = y - m->y, dz = z - m->z;
+                    const double r = std::sqrt(dx * dx + dy * dy + dz * dz + 1e-32);
+                    const double e = std::exp(-alpha * (r - m->R)), eM = m->E * e;
+                    P_ += eM * e;
+                    L_ += -2.0 * eM;
+                }
+                const size_t i = iz + (size_t)nz * (iy + (size_t)ny * ix);
                 ch[i] = P_; ch[N + i] = L_;
             }
+        }
+    }
+    (void)zlow;
     const double g1 = 2 * M_PI / Lx, g2 = 2 * M_PI / Ly, A = Lx * Ly;
     const double gmax = -std::log(gtol) / dmin;
     const int H = (int)std::floor(gmax / g1), K = (int)std::floor(gmax / g2);
@@ -1378,21 +1415,40 @@ int orc_build_grid_fast(int nions, const double* ions, const double* re, double 
         }
     std::vector<GT> act;
     for (auto& g : gs) if ((std::fabs(g.ar) + std::fabs(g.ai)) >= gtol * amax) act.push_back(g);
+    // phase tables: e^{i h g1 x_ix} and e^{i k g2 y_iy}
+    std::vector<double> cxh((size_t)(2 * H + 1) * nx), sxh(cxh.size()), cyk((size_t)(2 * K + 1) * ny), syk(cyk.size());
+    for (int h = -H; h <= H; h++)
+        for (int ix = 0; ix < nx; ix++) {
+            const double ph = h * g1 * (p0[0] + ix * step[0]);
+            cxh[(size_t)(h + H) * nx + ix] = std::cos(ph); sxh[(size_t)(h + H) * nx + ix] = std::sin(ph);
+        }
+    for (int k = -K; k <= K; k++)
+        for (int iy = 0; iy < ny; iy++) {
+            const double ph = k * g2 * (p0[1] + iy * step[1]);
+            cyk[(size_t)(k + K) * ny + iy] = std::cos(ph); syk[(size_t)(k + K) * ny + iy] = std::sin(ph);
+        }
 #ifdef _OPENMP
 #pragma omp parallel for schedule(dynamic, 1)
 #endif
     for (int iz = 0; iz < nz; iz++) {
         const double z = p0[2] + iz * step[2], dz = iz * step[2];
         const double phi0 = -(2 * M_PI / A) * (qsum * z - qz);
-        std::vector<double> cx, sx, cy, sy;
+        struct PG { const double *cx, *sx, *cy, *sy; double br, bi; };
+        std::vector<PG> pl;
+        for (auto& g : act) {
+            const double d = std::exp(-g.G * dz);
+            if ((std::fabs(g.ar) + std::fabs(g.ai)) * d < gtol * amax) continue;
+            pl.push_back({&cxh[(size_t)(g.h + H) * nx], &sxh[(size_t)(g.h + H) * nx], &cyk[(size_t)(g.k + K) * ny],
+                          &syk[(size_t)(g.k + K) * ny], d * g.ar, d * g.ai});
+        }
         for (int ix = 0; ix < nx; ix++)
             for (int iy = 0; iy < ny; iy++) {
-                double x = p0[0] + ix * step[0], y = p0[1] + iy * step[1], acc = 0;
-                for (auto& g : act) {
-                    double d = std::exp(-g.G * dz);
-                    if ((std::fabs(g.ar) + std::fabs(g.ai)) * d < gtol * amax) continue;
-                    double ph = g.h * g1 * x + g.k * g2 * y;
-                    acc += d * (g.ar * std::cos(ph) - g.ai * std::sin(ph));
+                double acc = 0;
+                for (const PG& q : pl) {
+                    // Re[(br + i bi) e^{i(phx + phy)}]
+                    const double c = q.cx[ix] * q.cy[iy] - q.sx[ix] * q.sy[iy];
+                    const double s = q.sx[ix] * q.cy[iy] + q.cx[ix] * q.sy[iy];
+                    acc += q.br * c - q.bi * s;
                 }
                 ch[2 * N + iz + (size_t)nz * (iy + (size_t)ny * ix)] = COULOMB_K * (phi0 + acc);
             }

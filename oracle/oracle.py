@@ -76,7 +76,7 @@ def lib():
                                      C.c_double, C.c_int, C.c_double, DP, DP]
         L.orc_build_grid_fast.restype = C.c_int
         L.orc_build_grid_fast.argtypes = [C.c_int, DP, DP, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, DP, DP,
-                                          C.c_double, C.c_int, C.c_double, DP]
+                                          C.c_double, C.c_int, C.c_double, DP, C.c_double]
         L.orc_substrate_direct.argtypes = [C.c_int, DP, DP, C.c_int, DP, DP, C.c_double, C.c_double, C.c_int,
                                            C.c_double, C.c_double, C.c_double, DP]
         L.orc_ljqh_pairs.argtypes = [C.c_int, DP, DP, C.c_double, DP]
@@ -403,11 +403,13 @@ def substrate_direct(pts, req_atom, ions, ion_req, Lx, Ly, npbc=1, alpha=1.5, gc
     return out
 
 
-def build_grid_fast(ions, ion_req, Lx, Ly, nx, ny, nz, p0, step, alpha=1.5, npbc=1, gtol=1e-12):
-    """orc_build_grid for a slab below the grid, with the separable Ewald evaluation (full-size grids)."""
+def build_grid_fast(ions, ion_req, Lx, Ly, nx, ny, nz, p0, step, alpha=1.5, npbc=1, gtol=1e-12, morse_rcut=0.0):
+    """orc_build_grid for a slab below the grid, with the separable Ewald evaluation (full-size grids).
+    morse_rcut > 0 drops Morse terms of ion images farther than that from a grid column (25 A:
+    dropped terms below 1e-15 of the nearest ion's); 0 keeps all, as make_MorseFF does."""
     coef = np.zeros((nx, ny, nz, 4))
     r = lib().orc_build_grid_fast(len(ions), _dp(_d(ions)), _dp(_d(ion_req)), Lx, Ly, nx, ny, nz, _dp(_d(p0)),
-                                  _dp(_d(step)), alpha, npbc, gtol, _dp(coef))
+                                  _dp(_d(step)), alpha, npbc, gtol, _dp(coef), float(morse_rcut))
     if r != 0:
         raise ValueError("grid must lie above the slab")
     return coef

@@ -134,6 +134,16 @@ struct smr_handle {
     std::vector<float> gzscale;         // 16-bit grids: nz x 4 per-plane channel scales (empty: gscale)
     DArr<float4> dzscale;
     bool has_grid = false;
+    // brick copy of the grid for the stencil reads (build_grid_bricks): rebuilt lazily before a
+    // launch whenever the grid changed; brick_mode -1 = on for grids larger than L2, 0 off, 1 on
+    unsigned long long grid_version = 0, brick_version = ~0ull;
+    void* bricks = nullptr;
+    size_t bricks_cap = 0;
+    int brick_mode = -1;
+    bool use_bricks = false;
+    int grid_prefetch = 0;
+    int smem_carveout = -1;             // block teams' preferred shared-memory carveout (%), -1 driver default
+    int occ_tiers = 0;                  // split launch segments by the occupancy a system's size allows
     // folded surface: while set it is the substrate in place of the grid
     bool fold_on = false;
     int fold_n[3] = {0, 0, 0};
@@ -425,6 +435,31 @@ int upload_slots(smr_handle* h, const std::vector<int>& ids) {
     return wait_stream(h, h->watchdog_s);
 }
 
+// The brick copy of the grid, (re)built when the grid changed since the last build; the grid of
+// base_args is then the copy.  Off for the folded surface, for grids up to 128 MiB in auto mode
+// (those stay in L2 and the 8x larger copy would not), and where the copy cannot be indexed.
+int ensure_bricks(smr_handle* h) {
+    h->use_bricks = false;
+    if (!h->has_grid || h->fold_on || h->brick_mode == 0) return 0;
+    const int nx = h->gdim[0], ny = h->gdim[1], nz = h->gdim[2];
+    const size_t plain = (size_t)nx * ny * nz * (h->grid_dtype == SMR_GRID_F32 ? 16 : 8);
+    if (h->brick_mode < 0 && plain <= (128u << 20)) return 0;
+    const size_t bytes = grid_brick_bytes(nx, ny, nz);
+    if (!bytes) return 0;
+    if (h->bricks && h->brick_version == h->grid_version) { h->use_bricks = true; return 0; }
+    if (bytes > h->bricks_cap) {
+        if (h->bricks) { CU(h, cudaStreamSynchronize(h->stream)); cudaFree(h->bricks); h->bricks = nullptr; h->bricks_cap = 0; }
+        cudaError_t e = cudaMalloc(&h->bricks, bytes);
+        if (e != cudaSuccess) { h->bricks = nullptr; return fail(h, SMR_ERR_CAPACITY, "grid bricks (%zu bytes): %s", bytes, cudaGetErrorString(e)); }
+        h->bricks_cap = bytes;
+    }
+    { const int e = build_grid_bricks(h->grid, h->grid_dtype, nx, ny, nz, h->bricks, h->stream);
+      if (e) return fail(h, SMR_ERR_CUDA, "grid bricks: %s", cudaGetErrorString((cudaError_t)e)); }
+    h->brick_version = h->grid_version;
+    h->use_bricks = true;
+    return 0;
+}
+
 KernelArgs base_args(smr_handle* h) {
     KernelArgs a{};
     a.counter = h->counter;
@@ -442,7 +477,8 @@ KernelArgs base_args(smr_handle* h) {
     }
     a.pos = h->pos; a.plo = h->plo; a.vel = h->vel; a.force = h->force;
     a.has_grid = h->has_grid ? 1 : 0;
-    a.grid.data = h->grid;
+    a.grid.data = h->use_bricks ? h->bricks : h->grid;
+    a.grid.brick = h->use_bricks ? 1 : 0;
     a.grid.dtype = h->grid_dtype;
     a.grid.nx = h->gdim[0]; a.grid.ny = h->gdim[1]; a.grid.nz = h->gdim[2];
     for (int k = 0; k < 3; k++) { a.grid.p0[k] = (float)h->gp0[k]; a.grid.inv_step[k] = (float)(1.0 / h->gstep[k]); }
@@ -460,6 +496,8 @@ KernelArgs base_args(smr_handle* h) {
     a.alpha_morse = h->nb.alpha_morse;
     a.rc2 = h->nb.rcut > 0 ? h->nb.rcut * h->nb.rcut : 3.0e38f;
     a.excl13 = h->nb.excl13 ? 1 : 0;
+    a.grid_prefetch = h->grid_prefetch;
+    a.smem_carveout = h->smem_carveout;
     return a;
 }
 
@@ -477,7 +515,7 @@ int latency_team_for(int requested, int n) {
 // under 1-3 exclusion, always the extended gather form), never from what it is batched with; segments group
 // equal (form, team) and are split wherever the segment's largest system would no longer fit.
 std::vector<Seg> group_by(smr_handle* h, std::vector<int>& ids, int form, int req_team = 0) {
-    struct Key { int form, team, n, nf; };
+    struct Key { int form, team, n, nf, tier; };
     auto key_of = [&](int s) {
         const SlotState& st = h->hs[s];
         const TopoDev& td = h->htd[st.topo];
@@ -502,11 +540,19 @@ std::vector<Seg> group_by(smr_handle* h, std::vector<int>& ids, int form, int re
         return Key{FORM_GATHER, std::max(td.team, n > 1024 ? 512 : 256), n, nf};
     };
     std::vector<Key> keys(h->max_systems);
-    for (int s : ids) keys[s] = key_of(s);
+    // occupancy tier: the blocks per SM a system's own shared memory allows under the register
+    // budget; systems of different tiers run in different segments, so a segment of small systems
+    // keeps its occupancy instead of taking the shared memory of the largest system of its team
+    for (int s : ids) {
+        Key k = key_of(s);
+        k.tier = h->occ_tiers ? relax_blocks_per_sm(team_smem_bytes(k.n, k.nf, k.team, k.form), k.team, k.form) : 0;
+        keys[s] = k;
+    }
     std::stable_sort(ids.begin(), ids.end(), [&](int a, int b) {
         const Key &x = keys[a], &y = keys[b];
         if (x.form != y.form) return x.form < y.form;
         if (x.team != y.team) return x.team < y.team;
+        if (x.tier != y.tier) return x.tier > y.tier;
         // systems that run at the same time then cover a small patch of the grid (L2 reuse)
         if (h->skey[a] != h->skey[b]) return h->skey[a] < h->skey[b];
         return x.n < y.n;
@@ -516,7 +562,7 @@ std::vector<Seg> group_by(smr_handle* h, std::vector<int>& ids, int form, int re
         const Key& k = keys[ids[i]];
         if (!segs.empty()) {
             Seg& g = segs.back();
-            if (g.form == k.form && g.team == k.team &&
+            if (g.form == k.form && g.team == k.team && keys[ids[g.begin]].tier == k.tier &&
                 (g.gstate || team_smem_bytes(std::max(g.nmax, k.n), std::max(g.nfmax, k.nf), k.team, k.form) <= h->smem_optin)) {
                 g.end = i + 1; g.nmax = std::max(g.nmax, k.n); g.nfmax = std::max(g.nfmax, k.nf);
                 continue;
@@ -636,6 +682,7 @@ int smr_destroy(smr_handle* h) {
     cudaFree(h->work); cudaFree(h->counter); cudaFree(h->ecomp); cudaFree(h->xfer);
     if (h->pinned) cudaFreeHost(h->pinned);
     if (h->grid) cudaFree(h->grid);
+    if (h->bricks) cudaFree(h->bricks);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->ev_fork) cudaEventDestroy(h->ev_fork);
@@ -681,8 +728,28 @@ int smr_set_tuning(smr_handle* h, int key, int value) {
         h->nbl_skin_ma = value;
         return SMR_OK;
     }
+    if (key == SMR_TUNE_SMEM_CARVEOUT) {
+        if (value < -1 || value > 100) return fail(h, SMR_ERR_ARG, "shared-memory carveout must be -1 or 0..100");
+        h->smem_carveout = value;
+        return SMR_OK;
+    }
+    if (key == SMR_TUNE_OCC_TIERS) {
+        if (value != 0 && value != 1) return fail(h, SMR_ERR_ARG, "occupancy tiers must be 0 or 1");
+        h->occ_tiers = value;
+        return SMR_OK;
+    }
+    if (key == SMR_TUNE_GRID_PREFETCH) {
+        if (value != 0 && value != 1) return fail(h, SMR_ERR_ARG, "grid prefetch must be 0 or 1");
+        h->grid_prefetch = value;
+        return SMR_OK;
+    }
+    if (key == SMR_TUNE_GRID_BRICKS) {
+        if (value < -1 || value > 1) return fail(h, SMR_ERR_ARG, "grid bricks must be -1 (auto), 0 or 1");
+        h->brick_mode = value;
+        return SMR_OK;
+    }
     if (key == SMR_TUNE_NBLIST_CAP) {
-        if (value < 32 || value > 4096) return fail(h, SMR_ERR_ARG, "neighbour-list capacity must be 32..4096");
+        if (value < 32 || value > 4096 || value % 4) return fail(h, SMR_ERR_ARG, "neighbour-list capacity must be a multiple of 4 in 32..4096");
         if (h->nbl_ready && value != h->nbl_cap) {           // rows change shape: drop the lists
             h->nbl_ready = false;
         }
@@ -699,6 +766,11 @@ int smr_get_tuning(smr_handle* h, int key, int* value) {
     if (key == SMR_TUNE_WATCHDOG_MS) { *value = (int)std::min(2.0e9, h->watchdog_s * 1e3); return SMR_OK; }
     if (key == SMR_TUNE_NBLIST_SKIN_MA) { *value = h->nbl_skin_ma; return SMR_OK; }
     if (key == SMR_TUNE_NBLIST_CAP) { *value = h->nbl_cap; return SMR_OK; }
+    if (key == SMR_TUNE_GRID_BRICKS) { *value = h->brick_mode; return SMR_OK; }
+    if (key == SMR_TUNE_GRID_BRICKS_ACTIVE) { *value = h->use_bricks ? 1 : 0; return SMR_OK; }
+    if (key == SMR_TUNE_GRID_PREFETCH) { *value = h->grid_prefetch; return SMR_OK; }
+    if (key == SMR_TUNE_SMEM_CARVEOUT) { *value = h->smem_carveout; return SMR_OK; }
+    if (key == SMR_TUNE_OCC_TIERS) { *value = h->occ_tiers; return SMR_OK; }
     return fail(h, SMR_ERR_ARG, "unknown tuning key %d", key);
 }
 
@@ -797,7 +869,7 @@ int smr_set_grid(smr_handle* h, const void* coef, int dtype, const float scale[4
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) { cudaFree(d); return fail(h, SMR_ERR_CUDA, "grid upload: %s", cudaGetErrorString(e)); }
     if (h->grid) cudaFree(h->grid);
-    h->grid = d; h->grid_dtype = dtype; h->has_grid = true;
+    h->grid = d; h->grid_version++; h->grid_dtype = dtype; h->has_grid = true;
     h->gdim[0] = nx; h->gdim[1] = ny; h->gdim[2] = nz;
     for (int k = 0; k < 3; k++) { h->gp0[k] = p0[k]; h->gstep[k] = step[k]; }
     for (int k = 0; k < 4; k++) h->gscale[k] = scale ? scale[k] : 1.f;
@@ -825,7 +897,7 @@ int smr_set_grid_device(smr_handle* h, const void* dev_coef, int dtype, const fl
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) { cudaFree(d); return fail(h, SMR_ERR_CUDA, "grid copy: %s", cudaGetErrorString(e)); }
     if (h->grid) cudaFree(h->grid);
-    h->grid = d; h->grid_dtype = dtype; h->has_grid = true;
+    h->grid = d; h->grid_version++; h->grid_dtype = dtype; h->has_grid = true;
     h->gdim[0] = nx; h->gdim[1] = ny; h->gdim[2] = nz;
     for (int k = 0; k < 3; k++) { h->gp0[k] = p0[k]; h->gstep[k] = step[k]; }
     for (int k = 0; k < 4; k++) h->gscale[k] = scale ? scale[k] : 1.f;
@@ -880,7 +952,7 @@ int smr_convert_grid(smr_handle* h, int dtype) {
     }
     CU(h, cudaStreamSynchronize(h->stream));
     if (out != h->grid) cudaFree(h->grid);
-    h->grid = out; h->grid_dtype = dtype;
+    h->grid = out; h->grid_version++; h->grid_dtype = dtype;
     if (dtype == SMR_GRID_F32) { for (int k = 0; k < 4; k++) h->gscale[k] = 1.f; h->gzscale.clear(); }
     else { int r = set_plane_scales(h, ps.data(), h->gdim[2]); if (r) return r; }
     return SMR_OK;
@@ -917,7 +989,7 @@ int smr_build_grid(smr_handle* h, int nions, const double* ions, const double* i
     cudaFree(dions); cudaFree(dre);
     if (r) { cudaFree(out); return fail(h, SMR_ERR_ARG, "grid build: %s", msg); }
     if (h->grid) cudaFree(h->grid);
-    h->grid = out; h->grid_dtype = SMR_GRID_F32; h->has_grid = true;
+    h->grid = out; h->grid_version++; h->grid_dtype = SMR_GRID_F32; h->has_grid = true;
     h->gdim[0] = nx; h->gdim[1] = ny; h->gdim[2] = nz;
     for (int k = 0; k < 3; k++) { h->gp0[k] = p0[k]; h->gstep[k] = step[k]; }
     for (int k = 0; k < 4; k++) h->gscale[k] = 1.f;
@@ -966,7 +1038,7 @@ int smr_grid_from_raw(smr_handle* h, const double* raw, int nx, int ny, int nz, 
     char msg[400] = {0};
     if (grid_from_raw_device(raw, nx, ny, nz, out, h->stream, msg, sizeof(msg))) { cudaFree(out); return fail(h, SMR_ERR_CUDA, "grid fit: %s", msg); }
     if (h->grid) cudaFree(h->grid);
-    h->grid = out; h->grid_dtype = SMR_GRID_F32; h->has_grid = true;
+    h->grid = out; h->grid_version++; h->grid_dtype = SMR_GRID_F32; h->has_grid = true;
     h->gdim[0] = nx; h->gdim[1] = ny; h->gdim[2] = nz;
     for (int k = 0; k < 3; k++) { h->gp0[k] = p0[k]; h->gstep[k] = step[k]; }
     for (int k = 0; k < 4; k++) h->gscale[k] = 1.f;
@@ -1361,6 +1433,7 @@ int smr_eval_forces(smr_handle* h, int nsys, const int* slot_ids, float* forces,
     for (int i = 0; i < nsys; i++) pos_in_input[slot_ids[i]] = i;
     cudaStream_t s = h->stream;
     CU(h, cudaMemcpyAsync(h->work, sorted.data(), nsys * 4, cudaMemcpyHostToDevice, s));
+    { int r = ensure_bricks(h); if (r) return r; }
     KernelArgs a = base_args(h);
     h->last_launches = 0;
     cudaEventRecord(h->ev0, s);
@@ -1527,6 +1600,7 @@ int smr_run_fire(smr_handle* h, int max_steps, int step_budget, const smr_fire_p
     }
     h->last_launches = 0;
     cudaStream_t s = h->stream;
+    { int r = ensure_bricks(h); if (r) return r; }
     KernelArgs a = base_args(h);
     a.fire = FireDev{p->dt0, p->dt_max, p->alpha0, p->f_inc, p->f_dec, p->f_alpha, p->fconv, p->flimit, p->n_min};
     a.step_budget = step_budget;

@@ -552,6 +552,44 @@ int grid_from_raw_device(const double* raw, int nx, int ny, int nz, float4* out,
     return fit_and_pack(paul, lond, coul, nx, ny, nz, out, buf, s, err, errlen);
 }
 
+// ---- brick copy for the stencil reads of the relax kernel (layout: smr_internal.h)
+namespace {
+template <typename V, int DY>
+__global__ void brick_kernel(const V* __restrict__ g, int nx, int ny, int nz, unsigned long long total, V* __restrict__ b) {
+    const unsigned long long t = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    const int e = (int)(t % (DY * 4));
+    unsigned long long br = t / (DY * 4);
+    const int nzb = nz - 3;
+    const int jz = (int)(br % nzb); br /= nzb;
+    const int iy = (int)(br % ny);
+    const int ix = (int)(br / ny);
+    const int dy = e >> 2, k = e & 3;
+    const int y = iy + dy >= ny ? iy + dy - ny : iy + dy;
+    b[t] = g[(size_t)(jz + k) + (size_t)nz * ((size_t)y + (size_t)ny * ix)];
+}
+}  // namespace
+
+size_t grid_brick_bytes(int nx, int ny, int nz) {
+    if (nx < 1 || ny < 4 || nz < 4) return 0;
+    const unsigned long long elems = (unsigned long long)nx * ny * (nz - 3) * 8;   // float4 elements (16-bit: 16 of 8 B)
+    if (elems * 2 >= (1ull << 32)) return 0;          // the kernel indexes 8-byte voxels with 32-bit offsets
+    return (size_t)elems * 16;
+}
+
+int build_grid_bricks(const void* grid, int dtype, int nx, int ny, int nz, void* bricks, cudaStream_t s) {
+    const size_t bytes = grid_brick_bytes(nx, ny, nz);
+    if (!bytes) return (int)cudaErrorInvalidValue;
+    if (dtype == GRID_F32) {
+        const unsigned long long total = bytes / 16;
+        brick_kernel<float4, 2><<<(unsigned)((total + 255) / 256), 256, 0, s>>>((const float4*)grid, nx, ny, nz, total, (float4*)bricks);
+    } else {
+        const unsigned long long total = bytes / 8;
+        brick_kernel<uint2, 4><<<(unsigned)((total + 255) / 256), 256, 0, s>>>((const uint2*)grid, nx, ny, nz, total, (uint2*)bricks);
+    }
+    return (int)cudaGetLastError();
+}
+
 }  // namespace smr
 
 // ============================================================================ allocation-free grid build

@@ -182,6 +182,32 @@ __device__ __forceinline__ void bspline(float u, float b[4], float d[4]) {
 
 __device__ __forceinline__ int imod(int i, int m) { int r = i % m; return r < 0 ? r + m : r; }
 
+// L2 prefetch of the brick lines of every atom's stencil (brick layout only): line l of an atom is
+// x column l / (NL / 4), y brick (l % (NL / 4)) * DY; one prefetch per line, lines spread over the team.
+// Cells are taken in FP32 (a line fetched for a cell the FP64 decision at a z bound moves is only
+// an unused prefetch); cells outside [1, nz-2) fetch nothing.
+template <int T, int GDT>
+__device__ __forceinline__ void grid_prefetch_l2(const GridView& g, const Smem& S, int N, int rank) {
+    constexpr int DY = GDT == GRID_F32 ? 2 : 4, NL = 16 / DY, VB = GDT == GRID_F32 ? 16 : 8;
+    const int nzb = g.nz - 3;
+    for (int t = rank; t < N * NL; t += T) {
+        const int i = t / NL, l = t % NL;
+        const float4 p = S.P()[i];
+        const float ux = (p.x - g.p0[0]) * g.inv_step[0], uy = (p.y - g.p0[1]) * g.inv_step[1];
+        const int iz = (int)((p.z - g.p0[2]) * g.inv_step[2]);
+        if (iz < 1 || iz >= g.nz - 2) continue;
+        int ix = (int)ux, iy = (int)uy;
+        if (ux < 0) ix--;
+        if (uy < 0) iy--;
+        const int xg = imod(ix - 1 + l / (NL / 4), g.nx);
+        const int yb = imod(iy - 1 + (l % (NL / 4)) * DY, g.ny);
+        const size_t e = (((size_t)xg * g.ny + yb) * nzb + (iz - 1)) * (size_t)(DY * 4);
+        const char* ptr = reinterpret_cast<const char*>(g.data) + e * VB;
+        asm volatile("prefetch.global.L2 [%0];" :: "l"(ptr));
+    }
+}
+
+
 // Cutoff decision for a pair whose FP32 r^2 lies within 1e-4 of rc^2: the squared distance from
 // the exact coordinate differences in FP64, as the CPU evaluators compute it.  Not inlined: the
 // rare path keeps its registers out of the partner loop.
@@ -562,6 +588,9 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
     constexpr bool PBC = FORM == FORM_GATHER_EXT;
     constexpr int BF = PBC ? FORM_GATHER : FORM;
     const bool pbc_bonds = PBC && lat != nullptr && TP(pbc_bonds) != 0;
+    // Grid lines into L2 ahead of phase D: positions do not change within a step, so the brick
+    // lines of every atom's stencil are requested now and arrive while phases A-C run
+    if (a.grid_prefetch && a.grid.brick && a.has_grid && !a.fold.on) grid_prefetch_l2<T, GDT>(a.grid, S, N, rank);
     // A: bonds and hneigh, one atom per rank (opencl/UFF.cl:141-322)
     if (pbc_bonds) {
         for (int i = rank; i < N; i += T) {
@@ -812,12 +841,20 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
                 const float4 pi = S.P()[i], qi = S.Q()[i], li = S.Lo()[i];
                 const int cnt = use_list ? a.nbl_cnt[ga0 + i] : -1;
                 if (cnt >= 0) {
-                    // partners within rc + skin, ascending; exclusions were removed at the build
-                    const unsigned short* row = a.nbl + (ga0 + i) * (size_t)a.nbl_cap;
-#pragma unroll 4
-                    for (int e = cp; e < cnt; e += Lp) {
-                        const int j = row[e];
-                        nb_pair<CUT>(a, pi, li, qi, S.P()[j], S.Lo()[j], S.Q()[j], false, fx, fy, fz, E);
+                    // partners within rc + skin, ascending; exclusions were removed at the build.
+                    // Lane cp takes runs of 4 consecutive partners, one 8-byte load each (rows
+                    // start on 512-byte boundaries); entries past the count weigh 0 and index the
+                    // atom itself, so a stale slot of the row is never dereferenced
+                    const ushort4* row4 = reinterpret_cast<const ushort4*>(a.nbl + (ga0 + i) * (size_t)a.nbl_cap);
+#pragma unroll 2
+                    for (int e = cp * 4; e < cnt; e += Lp * 4) {
+                        const ushort4 v = row4[e >> 2];
+                        const bool ok1 = e + 1 < cnt, ok2 = e + 2 < cnt, ok3 = e + 3 < cnt;
+                        const int j0 = v.x, j1 = ok1 ? (int)v.y : i, j2 = ok2 ? (int)v.z : i, j3 = ok3 ? (int)v.w : i;
+                        nb_pair<CUT>(a, pi, li, qi, S.P()[j0], S.Lo()[j0], S.Q()[j0], false, fx, fy, fz, E);
+                        nb_pair<CUT>(a, pi, li, qi, S.P()[j1], S.Lo()[j1], S.Q()[j1], !ok1, fx, fy, fz, E);
+                        nb_pair<CUT>(a, pi, li, qi, S.P()[j2], S.Lo()[j2], S.Q()[j2], !ok2, fx, fy, fz, E);
+                        nb_pair<CUT>(a, pi, li, qi, S.P()[j3], S.Lo()[j3], S.Q()[j3], !ok3, fx, fy, fz, E);
                     }
                 } else {
                     const short4 ng = S.Ng()[i];
@@ -936,22 +973,30 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
                     const float4 zs = g.zscale ? __ldg(g.zscale + (iz - 1 + kz)) : make_float4(g.scale[0], g.scale[1], g.scale[2], 1.f);
                     PLx *= zs.x; PLy *= zs.y; PLz *= zs.z;
                     // 32-bit voxel indices (the host keeps grids below 2^31 voxels): column offsets of
-                    // the 4 x and 4 y stencil rows, wrapped periodically, then one add per voxel
+                    // the 4 x and 4 y stencil rows, wrapped periodically, then one add per voxel.
+                    // Brick copy (smr_internal.h): stencil row pair / quad b of column x lies in the
+                    // 128-byte line of brick (x, y0 + b - b % DY, iz - 1), element (b % DY) * 4 + kz,
+                    // so the 4 lanes of an atom read aligned 64 B (fp32) or 32 B (16-bit) pieces of it
+                    constexpr int DY = GDT == GRID_F32 ? 2 : 4;
                     const int x0 = imod(ix - 1, g.nx), y0 = imod(iy - 1, g.ny);
-                    const int nyz = g.ny * g.nz;
+                    const int ystr = g.brick ? (g.nz - 3) * DY * 4 : g.nz;
+                    const int nyz = g.ny * ystr;
                     int yo[4];
 #pragma unroll
-                    for (int b = 0; b < 4; b++) { const int yg = y0 + b; yo[b] = (yg >= g.ny ? yg - g.ny : yg) * g.nz; }
-                    const int zoff = iz - 1 + kz;
+                    for (int b = 0; b < 4; b++) {
+                        const int yg = g.brick ? y0 + b - b % DY : y0 + b;
+                        yo[b] = (yg >= g.ny ? yg - g.ny : yg) * ystr + (g.brick ? (b % DY) * 4 : 0);
+                    }
+                    const int zoff = g.brick ? (iz - 1) * DY * 4 + kz : iz - 1 + kz;
                     float sE = 0.f, sX = 0.f, sY = 0.f;
 #pragma unroll
                     for (int ax = 0; ax < 4; ax++) {
                         const int xg = x0 + ax;
-                        const int xo = (xg >= g.nx ? xg - g.nx : xg) * nyz + zoff;
+                        const unsigned xo = (unsigned)(xg >= g.nx ? xg - g.nx : xg) * (unsigned)nyz + (unsigned)zoff;
                         float pE = 0.f, pY = 0.f;
 #pragma unroll
                         for (int b = 0; b < 4; b++) {
-                            const float4 v = load_voxel<GDT>(g.data, (unsigned)(xo + yo[b]));
+                            const float4 v = load_voxel<GDT>(g.data, (unsigned)xo + (unsigned)yo[b]);
                             const float cs = PLx * v.x + PLy * v.y + PLz * v.z;
                             pE += by[b] * cs; pY += dyw[b] * cs;
                         }
@@ -1210,7 +1255,7 @@ __device__ void run_system(const KernelArgs& a, const Smem& S, int w, int rank) 
 template <int T, int GDT, bool EVAL, int FORM, bool GS>
 // warp teams: 4 per block; a 40-atom system's shared memory allows 7 blocks per SM in the rounds
 // and gather forms and 6 in the owner form (slot pieces), which leaves it 85 registers
-__global__ void __launch_bounds__(T == 32 ? 128 : T, T == 32 ? (FORM == FORM_OWNER ? 6 : 7) : 1)
+__global__ void __launch_bounds__(T == 32 ? 128 : T, relax_min_blocks(T, FORM))
 relax_kernel(const KernelArgs a) {
     extern __shared__ __align__(16) char smem[];
     const int team = (T == 32) ? (threadIdx.x >> 5) : 0;
@@ -1256,6 +1301,11 @@ int launch_t(const KernelArgs& a, cudaStream_t s, int num_sms) {
     }
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return (int)e;
+    }
+    if (T > 32 && !GS) {
+        // block teams: the preferred split of the SM's L1 between shared memory and cache
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, a.smem_carveout);
         if (e != cudaSuccess) return (int)e;
     }
     if (occ < 0) {

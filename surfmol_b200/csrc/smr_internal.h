@@ -77,6 +77,7 @@ struct GridView {
     float inv_step[3];
     float scale[4];               // per-channel scale of the stored values (when zscale is null)
     const float4* zscale;         // 16-bit grids: per z plane and channel scale (null: scale[])
+    int brick;                    // 1: data is the brick copy (build_grid_bricks), not the z-fastest grid
     double p0z, stepz;            // z origin and step in FP64 (cell decisions at the grid's z bounds)
 };
 
@@ -115,6 +116,8 @@ struct KernelArgs {
     FoldedView fold;              // fold.on: the substrate is the folded surface, not the grid
     float R2damp, alpha_morse, rc2;
     int excl13;                   // 1: 1-3 pairs excluded too (getNonBond_GridFF_Bspline_ex2)
+    int grid_prefetch;            // 1: L2 prefetch of the brick lines at the start of each evaluation
+    int smem_carveout;            // block teams: preferred shared-memory carveout in percent (-1: driver default)
     FireDev fire;
     int phase_limit;              // this launch runs a system until SlotState::steps reaches min(target, phase_limit)
     int step_budget;              // a system reaching this many steps gets SMR_ST_MAXSTEPS (<=0: none)
@@ -209,6 +212,20 @@ enum SlotFlags { SLOT_PBC = 1, SLOT_CONS = 2, SLOT_THERM = 4 };
 enum KernelForm { FORM_ROUNDS = 0, FORM_GATHER = 1, FORM_OWNER = 2, FORM_GATHER_EXT = 3 };
 int launch_relax(const KernelArgs& a, int team, int form, int eval_only, cudaStream_t s, int num_sms, long long* launches);
 size_t team_smem_bytes(int nmax, int nfmax, int team, int form);
+// Minimum blocks per SM the relax kernel's __launch_bounds__ asks for: warp teams run 4 to a
+// 128-thread block at 72 registers (80 in the owner form), 7 (6) blocks; block teams take the
+// registers the compiler wants (measured: capping them at 128 or 96 for more resident teams
+// made the ragged workload 11-25 % slower, the extra teams thrashing L1 on their global reads).
+constexpr int relax_min_blocks(int T, int form) {
+    return T == 32 ? (form == FORM_OWNER ? 6 : 7) : 1;
+}
+// Blocks of one launch segment that fit on an SM by shared memory (228 KB per SM, 1 KB reserved
+// per block), capped at 16 (the occupancy tiers of group_by).
+inline int relax_blocks_per_sm(size_t smem_per_block, int T, int form) {
+    const int by_smem = (int)(233472 / (smem_per_block + 1024));
+    (void)T; (void)form;
+    return by_smem < 16 ? by_smem : 16;
+}
 
 // grid.cu
 struct GridBuildArgs {
@@ -225,5 +242,12 @@ int grid_from_raw_device(const double* raw, int nx, int ny, int nz, float4* out_
 // floats (host); decode takes them as a device table
 int encode_grid_16(const float4* src, void* dst, size_t nvox, int nz, int dtype, float* plane_scale_out, cudaStream_t s);
 int decode_grid_16(const void* src, float4* dst, size_t nvox, int nz, int dtype, const float4* d_plane_scale, cudaStream_t s);
+// Brick copy of a z-fastest grid for the relax kernel's stencil reads.  Brick (ix, iy, jz),
+// jz in [0, nz - 3), is one 128-byte line holding the voxels (iy + dy mod ny, jz + k), k < 4,
+// dy < grid_brick_rows(dtype) (2 rows of 16-byte float4 voxels, 4 rows of 8-byte 16-bit ones),
+// stored dy-major.  0 elements when the grid is too small or the copy would need 2^32 voxels.
+inline int grid_brick_rows(int dtype) { return dtype == GRID_F32 ? 2 : 4; }
+size_t grid_brick_bytes(int nx, int ny, int nz);
+int build_grid_bricks(const void* grid, int dtype, int nx, int ny, int nz, void* bricks, cudaStream_t s);
 
 }  // namespace smr

@@ -160,6 +160,7 @@ class RelaxMulti:
     """Many molecules relaxed by FIRE in parallel over one substrate grid, on one GPU."""
 
     def __init__(self, max_systems: int, max_atoms: int, device: int = 0):
+        self.max_systems = int(max_systems)
         self.L = N.lib()
         cfg = N.SmrConfig(device, int(max_systems), int(max_atoms))
         h = N.VP()
@@ -301,6 +302,29 @@ class RelaxMulti:
     def set_nb_lanes(self, lanes):
         """Lanes per atom in the NB partner loop (0: chosen from system size and team)."""
         self._chk(self.L.smr_set_tuning(self.h, 1, int(lanes)), "smr_set_tuning")
+
+    def set_grid_bricks(self, mode):
+        """Grid layout the relax kernel reads: -1 (default) the brick copy for grids larger than
+        128 MiB, 0 the z-fastest grid, 1 the brick copy always (results identical bit for bit)."""
+        self._chk(self.L.smr_set_tuning(self.h, 6, int(mode)), "smr_set_tuning")
+
+    def set_grid_prefetch(self, on=True):
+        """With the brick copy: request each evaluation's stencil lines into L2 at its start."""
+        self._chk(self.L.smr_set_tuning(self.h, 8, 1 if on else 0), "smr_set_tuning")
+
+    def set_smem_carveout(self, percent=-1):
+        """Block teams' preferred shared-memory share of L1 in percent (-1: driver default)."""
+        self._chk(self.L.smr_set_tuning(self.h, 9, int(percent)), "smr_set_tuning")
+
+    def set_occupancy_tiers(self, on=True):
+        """Split launch segments by the occupancy each system's size allows (default off)."""
+        self._chk(self.L.smr_set_tuning(self.h, 10, 1 if on else 0), "smr_set_tuning")
+
+    def grid_bricks_active(self) -> bool:
+        """True if the last relaxation or force evaluation read the brick copy of the grid."""
+        v = C.c_int()
+        self._chk(self.L.smr_get_tuning(self.h, 7, C.byref(v)), "smr_get_tuning")
+        return bool(v.value)
 
     def set_watchdog(self, ms):
         """Longest wait for device work per call (ms); a call that gives up raises SmrError (-6) and the

@@ -55,6 +55,18 @@ def max_over_ranks(value: float) -> float:
     return float(t.item())
 
 
+def sum_over_ranks(value: float) -> float:
+    """Sum of a float over all ranks of the default process group (the value itself without one)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(value)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(value)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def grid_slabs(nx: int, world: int) -> tuple[int, list[tuple[int, int]]]:
     """Equal x-slabs for a sharded grid build: width ceil(nx / world) and each rank's [x0, x0 + width);
     the last slabs may reach past nx (their extra planes are computed and dropped), so the slabs
