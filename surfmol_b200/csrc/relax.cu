@@ -272,20 +272,22 @@ __device__ __noinline__ float4 folded_part(const FoldedView f, float4 p, float4 
 }
 
 // One LJ + damped-Coulomb pair (getLJQH, opencl/UFF.cl:82-95) at separation (dx, dy, dz) added to
-// the force / energy of atom i; skipped pairs are evaluated at r^2 = 1 and weighted 0.
+// the force / energy of atom i.  qi.z carries the Coulomb constant (kCoulomb * Q_i, scaled once
+// per atom by the caller).  Skipped pairs are evaluated at r^2 = 1 with zero well depth and
+// charge product, so they add exactly 0.  fr = E0 u6 / r^2 (12 - 12 u6) - Ec / (r^2 + Rdamp^2).
 __device__ __forceinline__ void ljq_pair(float dx, float dy, float dz, bool skip, float4 qi, float4 qj, float R2damp,
                                          float& fx, float& fy, float& fz, float& E) {
     float r2 = dx * dx + dy * dy + dz * dz;
     r2 = skip ? 1.0f : r2;
-    const float R0 = qi.x + qj.x, E0 = qi.y * qj.y, Q = qi.z * qj.z;
+    const float R0 = qi.x + qj.x;
+    const float E0 = skip ? 0.0f : qi.y * qj.y, Q = skip ? 0.0f : qi.z * qj.z;
     const float rs = rsqrtf(r2 + R2damp);            // 1/sqrt(r^2 + Rdamp^2)
-    const float Ec = kCoulomb * Q * rs;
+    const float Ec = Q * rs;
     const float ir2 = 1.0f / r2;
     const float u2 = R0 * R0 * ir2, u6 = u2 * u2 * u2, vdW = u6 * E0;
-    const float w = skip ? 0.0f : 1.0f;
-    E += w * ((u6 - 2.0f) * vdW + Ec);
-    const float fr = w * (-12.0f * (u6 - 1.0f) * vdW * ir2 - Ec * (rs * rs));
-    fx += dx * fr; fy += dy * fr; fz += dz * fr;
+    E += fmaf(u6 - 2.0f, vdW, Ec);
+    const float fr = fmaf(vdW * ir2, fmaf(u6, -12.0f, 12.0f), -Ec * (rs * rs));
+    fx = fmaf(dx, fr, fx); fy = fmaf(dy, fr, fy); fz = fmaf(dz, fr, fz);
 }
 
 // 1-3 exclusion (getNonBond_GridFF_Bspline_ex2, UFF.cl:1722-1930, with the lists of
@@ -446,7 +448,9 @@ __device__ __forceinline__ float4 nb_atom_images(Smem S, float rc2, float R2damp
     const float4 A = __ldg(lat), B = __ldg(lat + 1), C = __ldg(lat + 2);
     const int nx = (int)A.w, ny = (int)B.w, nz = (int)C.w;
     const bool cut = rc2 < 1e37f;
-    const float4 pi = S.P()[i], li = S.Lo()[i], qi = S.Q()[i];
+    const float4 pi = S.P()[i], li = S.Lo()[i];
+    float4 qi = S.Q()[i];
+    qi.z *= kCoulomb;                                 // ljq_pair takes kCoulomb * Q_i
     float fx = 0.f, fy = 0.f, fz = 0.f, E = 0.f;
     for (int j = c; j < N; j += L) {
         if (j == i) continue;
@@ -838,7 +842,9 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
             const int i = i0 + rank / Lp, cp = rank & (Lp - 1);
             float fx = 0.f, fy = 0.f, fz = 0.f, E = 0.f;
             if (i < N) {
-                const float4 pi = S.P()[i], qi = S.Q()[i], li = S.Lo()[i];
+                const float4 pi = S.P()[i], li = S.Lo()[i];
+                float4 qi = S.Q()[i];
+                qi.z *= kCoulomb;                     // ljq_pair takes kCoulomb * Q_i
                 const int cnt = use_list ? a.nbl_cnt[ga0 + i] : -1;
                 if (cnt >= 0) {
                     // partners within rc + skin, ascending; exclusions were removed at the build.
