@@ -608,7 +608,9 @@ def run_ragged(args, ws, rank, local):
         gd = R.get_grid()
         og = O.Grid(gd["coef"], gd["p0"], gd["step"])
         threads = os.cpu_count() or 1
-        n = RAGGED["cpu_per_core"] * threads
+        # twice the reference arm's per-step sample: one batch's time is set by its slowest
+        # molecules, and this leg has one batch where the reference arm averages many
+        n = 2 * RAGGED["cpu_per_core"] * threads
         dt, c, _ = ragged_cpu_batch(w, og, list(range(n)), max_steps, threads)
         line["cpu_baseline"] = {"value": c / dt, "unit": "relaxed systems/s", "cores": threads, "kind": "port",
                                 "sample": f"{n} molecules of the workload in one OpenMP batch (FP64 oracle, one system per "
