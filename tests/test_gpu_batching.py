@@ -191,3 +191,30 @@ def test_nblist_forces_and_bitwise(setup, oracle, cap):
                 assert np.array_equal(o["pos"][k], runs[0]["pos"][k]) and o["steps"][k] == runs[0]["steps"][k] == 150
     finally:
         R.finish()
+
+
+def test_nblist_complete_while_molecules_move(setup):
+    """The lists stay complete between rebuilds: a list is rebuilt once an atom has moved more than
+    half the skin, so no pair's separation changes by more than the skin before it is (atoms of
+    these placements move up to ~3 A in 300 steps; one copy starts 2 A higher).  Every 60 FIRE
+    steps the next step's forces
+    (partner loop over the lists) equal an all-pairs evaluation at the same positions up to FP32
+    summation order; a pair missing inside the 10 A cutoff would add its Coulomb force (~1e-3 eV/A)."""
+    slab, dims, p0, step, mols = setup
+    big = [mols[4], mols[5], mols[6]]                       # 150-330 atoms
+    R = make_handle(8, 4000, slab, dims, p0, step, rcut=10.0)
+    try:
+        R.set_nblist(min_atoms=128, skin=1.0, cap=256)
+        tids = [R.add_molecule(Z, P, q) for Z, P, q in big]
+        starts = [m[1] for m in big] + [big[0][1] + np.array([0.0, 0.0, 2.0])]
+        s = R.add_systems(tids + [tids[0]], starts)
+        for _ in range(5):
+            R.run_fire(60, fconv=1e-9)
+            F_all, _ = R.eval_forces(s)                     # the evaluation entry point uses no lists
+            R.run_fire(1, fconv=1e-9)                       # forces at the same positions, over the lists
+            F_list = R.download(s, pos=False)["forces"]
+            for k in range(len(s)):
+                ref = F_all[k][:, :3].astype(np.float64)
+                assert np.abs(F_list[k][:, :3] - ref).max() < 2e-5 * max(1.0, np.abs(ref).max()), k
+    finally:
+        R.finish()
