@@ -205,6 +205,18 @@ int smr_grid_raw_slab(smr_handle* h, int nions, const double* ions, const double
 int smr_grid_from_raw(smr_handle* h, const double* raw, int nx, int ny, int nz, const double p0[3], const double step[3], int dtype);
 /* Re-encode the current grid to another storage dtype with per-channel scales (max|c| mapping). */
 int smr_convert_grid(smr_handle* h, int dtype);
+/* Split storage: the current FP32 grid becomes a 16-bit grid (dtype SMR_GRID_F16 or _BF16, per-plane
+ * scales as smr_convert_grid makes them) plus an FP32 copy of its planes [0, zsplit + 3).  An atom
+ * whose stencil starts below plane zsplit (cell iz - 1 < zsplit) is interpolated from the FP32
+ * copy, every other atom from the 16-bit grid.  Near the surface the channels are large and nearly
+ * cancel at a relaxed position, so 16-bit mantissas there cost ~4e-3 eV/A of force error (fp16);
+ * above it they cost far less than 1e-4 eV/A.  1 <= zsplit <= nz - 3.  smr_get_grid returns the
+ * 16-bit grid; any later set, build or conversion of the grid drops the FP32 copy.
+ * smr_get_grid_split: zsplit (0: no split) and, when lo_out is non-null, the FP32 planes
+ * (nx * ny * (zsplit + 3) * 4 floats, z-fastest, channel scales applied).  No counterpart in the
+ * reference (its grids are float32). */
+int smr_convert_grid_split(smr_handle* h, int dtype, int zsplit);
+int smr_get_grid_split(smr_handle* h, int* zsplit, float* lo_out);
 
 /* Molecule -> bonds by cutoff, UFF typing, terms and parameters (host, native), upload. */
 int smr_add_molecule(smr_handle* h, int natoms, const int* Z, const double* pos, const double* charges,

@@ -86,6 +86,8 @@ SIGNATURES = {
     "smr_build_grid": (C.c_int, [VP, C.c_int, DP, DP, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, DP, DP,
                                  C.POINTER(SmrGridBuildParams)]),
     "smr_convert_grid": (C.c_int, [VP, C.c_int]),
+    "smr_convert_grid_split": (C.c_int, [VP, C.c_int, C.c_int]),
+    "smr_get_grid_split": (C.c_int, [VP, IP, FP]),
     "smr_build_grid_static": (C.c_int, [C.c_int, DP, DP, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, DP, DP,
                                         C.POINTER(SmrGridBuildParamsStatic), VP, VP, C.c_char_p, C.c_int]),
     "smr_add_molecule": (C.c_int, [VP, C.c_int, IP, DP, DP, C.c_double, IP]),

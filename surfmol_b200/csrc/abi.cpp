@@ -141,6 +141,14 @@ struct smr_handle {
     size_t bricks_cap = 0;
     int brick_mode = -1;
     bool use_bricks = false;
+    // 16-bit grid with FP32 near-surface planes (smr_convert_grid_split): the planes
+    // [0, grid_zsplit + 3) of the FP32 grid it came from (z-fastest), their channel scales, and
+    // their brick copy (built with the grid's); grid_zsplit = 0: none
+    float4* grid_lo = nullptr;
+    int grid_zsplit = 0;
+    float glo_scale[4] = {1, 1, 1, 1};
+    void* bricks_lo = nullptr;
+    size_t bricks_lo_cap = 0;
     int grid_prefetch = 0;
     int smem_carveout = -1;             // block teams' preferred shared-memory carveout (%), -1 driver default
     int occ_tiers = 0;                  // split launch segments by the occupancy a system's size allows
@@ -455,6 +463,20 @@ int ensure_bricks(smr_handle* h) {
     }
     { const int e = build_grid_bricks(h->grid, h->grid_dtype, nx, ny, nz, h->bricks, h->stream);
       if (e) return fail(h, SMR_ERR_CUDA, "grid bricks: %s", cudaGetErrorString((cudaError_t)e)); }
+    if (h->grid_zsplit > 0) {
+        // the FP32 near-surface planes in the same layout
+        const int nzl = h->grid_zsplit + 3;
+        const size_t lb = grid_brick_bytes(nx, ny, nzl);
+        if (!lb) return fail(h, SMR_ERR_CAPACITY, "grid bricks of the FP32 planes cannot be indexed");
+        if (lb > h->bricks_lo_cap) {
+            if (h->bricks_lo) { CU(h, cudaStreamSynchronize(h->stream)); cudaFree(h->bricks_lo); h->bricks_lo = nullptr; h->bricks_lo_cap = 0; }
+            cudaError_t e = cudaMalloc(&h->bricks_lo, lb);
+            if (e != cudaSuccess) { h->bricks_lo = nullptr; return fail(h, SMR_ERR_CAPACITY, "grid bricks of the FP32 planes (%zu bytes): %s", lb, cudaGetErrorString(e)); }
+            h->bricks_lo_cap = lb;
+        }
+        const int e = build_grid_bricks(h->grid_lo, SMR_GRID_F32, nx, ny, nzl, h->bricks_lo, h->stream);
+        if (e) return fail(h, SMR_ERR_CUDA, "grid bricks of the FP32 planes: %s", cudaGetErrorString((cudaError_t)e));
+    }
     h->brick_version = h->grid_version;
     h->use_bricks = true;
     return 0;
@@ -485,6 +507,11 @@ KernelArgs base_args(smr_handle* h) {
     for (int k = 0; k < 4; k++) a.grid.scale[k] = h->has_grid ? h->gscale[k] : 1.f;
     a.grid.zscale = (h->has_grid && !h->gzscale.empty()) ? h->dzscale.d : nullptr;
     a.grid.p0z = h->gp0[2]; a.grid.stepz = h->gstep[2];
+    if (h->has_grid && h->grid_zsplit > 0) {
+        a.grid.lo = h->use_bricks ? h->bricks_lo : (const void*)h->grid_lo;
+        a.grid.zsplit = h->grid_zsplit; a.grid.lo_nz = h->grid_zsplit + 3;
+        for (int k = 0; k < 4; k++) a.grid.lo_scale[k] = h->glo_scale[k];
+    }
     if (h->fold_on) {
         a.fold.on = 1;
         a.fold.nx = h->fold_n[0]; a.fold.ny = h->fold_n[1]; a.fold.nz = h->fold_n[2];
@@ -683,6 +710,8 @@ int smr_destroy(smr_handle* h) {
     if (h->pinned) cudaFreeHost(h->pinned);
     if (h->grid) cudaFree(h->grid);
     if (h->bricks) cudaFree(h->bricks);
+    if (h->grid_lo) cudaFree(h->grid_lo);
+    if (h->bricks_lo) cudaFree(h->bricks_lo);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->ev_fork) cudaEventDestroy(h->ev_fork);
@@ -786,6 +815,12 @@ int smr_set_team_size(smr_handle* h, int max_atoms, int threads) {
 
 static size_t voxel_bytes(int dtype) { return dtype == SMR_GRID_F32 ? 16 : 8; }
 
+// forget the FP32 near-surface planes of a split grid (the grid is being replaced or re-encoded)
+static void drop_split(smr_handle* h) {
+    if (h->grid_lo) { cudaStreamSynchronize(h->stream); cudaFree(h->grid_lo); h->grid_lo = nullptr; }
+    h->grid_zsplit = 0;
+}
+
 // install per-plane scales (nz x 4 host floats; null: none) on the device
 static int set_plane_scales(smr_handle* h, const float* ps, int nz) {
     if (!ps) { h->gzscale.clear(); return SMR_OK; }
@@ -868,6 +903,7 @@ int smr_set_grid(smr_handle* h, const void* coef, int dtype, const float scale[4
     cudaError_t e = cudaMemcpyAsync(d, coef, bytes, cudaMemcpyHostToDevice, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) { cudaFree(d); return fail(h, SMR_ERR_CUDA, "grid upload: %s", cudaGetErrorString(e)); }
+    drop_split(h);
     if (h->grid) cudaFree(h->grid);
     h->grid = d; h->grid_version++; h->grid_dtype = dtype; h->has_grid = true;
     h->gdim[0] = nx; h->gdim[1] = ny; h->gdim[2] = nz;
@@ -896,6 +932,7 @@ int smr_set_grid_device(smr_handle* h, const void* dev_coef, int dtype, const fl
     cudaError_t e = cudaMemcpyAsync(d, dev_coef, bytes, cudaMemcpyDeviceToDevice, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) { cudaFree(d); return fail(h, SMR_ERR_CUDA, "grid copy: %s", cudaGetErrorString(e)); }
+    drop_split(h);
     if (h->grid) cudaFree(h->grid);
     h->grid = d; h->grid_version++; h->grid_dtype = dtype; h->has_grid = true;
     h->gdim[0] = nx; h->gdim[1] = ny; h->gdim[2] = nz;
@@ -949,12 +986,58 @@ int smr_convert_grid(smr_handle* h, int dtype) {
         ps.resize(4 * (size_t)h->gdim[2]);
         if (encode_grid_16(f32, out, nv, h->gdim[2], dtype, ps.data(), h->stream)) { cudaFree(out); return fail(h, SMR_ERR_CUDA, "grid encode failed"); }
         if ((void*)f32 != h->grid) cudaFree(f32);
+        // an FP32 source's values are its stored values times its channel scales
+        else for (size_t z = 0; z < (size_t)h->gdim[2]; z++) for (int c = 0; c < 4; c++) ps[4 * z + c] *= h->gscale[c];
     }
     CU(h, cudaStreamSynchronize(h->stream));
+    drop_split(h);
     if (out != h->grid) cudaFree(h->grid);
     h->grid = out; h->grid_version++; h->grid_dtype = dtype;
     if (dtype == SMR_GRID_F32) { for (int k = 0; k < 4; k++) h->gscale[k] = 1.f; h->gzscale.clear(); }
     else { int r = set_plane_scales(h, ps.data(), h->gdim[2]); if (r) return r; }
+    return SMR_OK;
+}
+
+int smr_convert_grid_split(smr_handle* h, int dtype, int zsplit) {
+    if (!h) return SMR_ERR_ARG;
+    SETTLE(h);
+    if (!h->has_grid) return fail(h, SMR_ERR_STATE, "no grid set");
+    if (h->grid_dtype != SMR_GRID_F32) return fail(h, SMR_ERR_STATE, "a split grid is made from an FP32 grid (current dtype %d)", h->grid_dtype);
+    if (dtype != SMR_GRID_F16 && dtype != SMR_GRID_BF16) return fail(h, SMR_ERR_ARG, "split grids store F16 or BF16 above the split");
+    const int nx = h->gdim[0], ny = h->gdim[1], nz = h->gdim[2];
+    if (zsplit < 1 || zsplit > nz - 3) return fail(h, SMR_ERR_ARG, "zsplit must be 1..%d (got %d)", nz - 3, zsplit);
+    const int nzl = zsplit + 3;
+    float4* lo = nullptr;
+    CU(h, cudaMalloc(&lo, (size_t)nx * ny * nzl * 16));
+    if (extract_low_planes((const float4*)h->grid, (size_t)nx * ny, nz, nzl, lo, h->stream) ||
+        cudaStreamSynchronize(h->stream) != cudaSuccess) {
+        cudaFree(lo);
+        return fail(h, SMR_ERR_CUDA, "copy of the FP32 planes failed");
+    }
+    float sc[4];
+    for (int k = 0; k < 4; k++) sc[k] = h->gscale[k];
+    const int r = smr_convert_grid(h, dtype);
+    if (r) { cudaFree(lo); return r; }
+    h->grid_lo = lo; h->grid_zsplit = zsplit;
+    for (int k = 0; k < 4; k++) h->glo_scale[k] = sc[k];
+    h->grid_version++;                                    // rebuild the brick copies
+    return SMR_OK;
+}
+
+int smr_get_grid_split(smr_handle* h, int* zsplit, float* lo_out) {
+    if (!h || !zsplit) return SMR_ERR_ARG;
+    SETTLE(h);
+    *zsplit = h->has_grid ? h->grid_zsplit : 0;
+    if (lo_out && *zsplit > 0) {
+        const size_t n = (size_t)h->gdim[0] * h->gdim[1] * (h->grid_zsplit + 3);
+        std::vector<float4> tmp(n);
+        CU(h, cudaMemcpyAsync(tmp.data(), h->grid_lo, n * 16, cudaMemcpyDeviceToHost, h->stream));
+        CU(h, cudaStreamSynchronize(h->stream));
+        for (size_t i = 0; i < n; i++) {
+            lo_out[4 * i] = tmp[i].x * h->glo_scale[0]; lo_out[4 * i + 1] = tmp[i].y * h->glo_scale[1];
+            lo_out[4 * i + 2] = tmp[i].z * h->glo_scale[2]; lo_out[4 * i + 3] = tmp[i].w * h->glo_scale[3];
+        }
+    }
     return SMR_OK;
 }
 
@@ -988,11 +1071,13 @@ int smr_build_grid(smr_handle* h, int nions, const double* ions, const double* i
     int r = build_grid_device(A, out, h->stream, msg, sizeof(msg));
     cudaFree(dions); cudaFree(dre);
     if (r) { cudaFree(out); return fail(h, SMR_ERR_ARG, "grid build: %s", msg); }
+    drop_split(h);
     if (h->grid) cudaFree(h->grid);
     h->grid = out; h->grid_version++; h->grid_dtype = SMR_GRID_F32; h->has_grid = true;
     h->gdim[0] = nx; h->gdim[1] = ny; h->gdim[2] = nz;
     for (int k = 0; k < 3; k++) { h->gp0[k] = p0[k]; h->gstep[k] = step[k]; }
     for (int k = 0; k < 4; k++) h->gscale[k] = 1.f;
+    h->gzscale.clear();                                   // a previous 16-bit grid's plane scales
     if (p->dtype != SMR_GRID_F32) return smr_convert_grid(h, p->dtype);
     return SMR_OK;
 }
@@ -1037,6 +1122,7 @@ int smr_grid_from_raw(smr_handle* h, const double* raw, int nx, int ny, int nz, 
     CU(h, cudaMalloc(&out, (size_t)nx * ny * nz * 16));
     char msg[400] = {0};
     if (grid_from_raw_device(raw, nx, ny, nz, out, h->stream, msg, sizeof(msg))) { cudaFree(out); return fail(h, SMR_ERR_CUDA, "grid fit: %s", msg); }
+    drop_split(h);
     if (h->grid) cudaFree(h->grid);
     h->grid = out; h->grid_version++; h->grid_dtype = SMR_GRID_F32; h->has_grid = true;
     h->gdim[0] = nx; h->gdim[1] = ny; h->gdim[2] = nz;
@@ -1529,7 +1615,9 @@ static void sig_args(std::vector<long long>& v, const KernelArgs& a) {
     P(a.grid.data); v.push_back(a.grid.dtype); v.push_back(a.grid.nx); v.push_back(a.grid.ny); v.push_back(a.grid.nz);
     for (int k = 0; k < 3; k++) { F(a.grid.p0[k]); F(a.grid.inv_step[k]); }
     for (int k = 0; k < 4; k++) F(a.grid.scale[k]);
-    P(a.grid.zscale); D(a.grid.p0z); D(a.grid.stepz);
+    P(a.grid.zscale); D(a.grid.p0z); D(a.grid.stepz); v.push_back(a.grid.brick);
+    P(a.grid.lo); v.push_back(a.grid.zsplit); v.push_back(a.grid.lo_nz);
+    for (int k = 0; k < 4; k++) F(a.grid.lo_scale[k]);
     v.push_back(a.has_grid); F(a.R2damp); F(a.alpha_morse); F(a.rc2);
     D(a.fire.dt0); D(a.fire.dt_max); D(a.fire.alpha0); D(a.fire.f_inc); D(a.fire.f_dec); D(a.fire.f_alpha);
     D(a.fire.fconv); D(a.fire.flimit); v.push_back(a.fire.n_min);

@@ -374,6 +374,23 @@ int decode_grid_16(const void* src, float4* dst, size_t nvox, int nz, int dtype,
 }
 
 namespace {
+__global__ void low_planes_kernel(size_t n, int nz, int nzl, const float4* __restrict__ src, float4* __restrict__ dst) {
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const size_t col = t / (size_t)nzl;
+    const int z = (int)(t - col * (size_t)nzl);
+    dst[t] = src[col * (size_t)nz + z];
+}
+}  // namespace
+
+int extract_low_planes(const float4* src, size_t nxy, int nz, int nzl, float4* dst, cudaStream_t s) {
+    if (nzl < 1 || nzl > nz) return -1;
+    const size_t n = nxy * (size_t)nzl;
+    low_planes_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, nz, nzl, src, dst);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+namespace {
 
 // Raw (unfitted) FP64 channels of the x-planes [x0, x0 + xs): Morse (Pauli, London) and Ewald-2D,
 // each xs * ny * nz values, z-fastest, into paul / lond / coul (device).

@@ -182,6 +182,45 @@ __device__ __forceinline__ void bspline(float u, float b[4], float d[4]) {
 
 __device__ __forceinline__ int imod(int i, int m) { int r = i % m; return r < 0 ? r + m : r; }
 
+// One lane's share of an atom's tricubic stencil over a grid array of nzs z planes: the voxels at
+// z offset kz of the 16 (x, y) columns of cell (ix, iy, iz), combined over the channels with the
+// prefactors PL, summed with the x / y weights: sE = sum bx by c, sX = sum dx by c, sY = sum bx dy c.
+// 32-bit voxel indices (the host keeps grids below 2^31 voxels): column offsets of the 4 x and 4 y
+// stencil rows, wrapped periodically, then one add per voxel.  Brick copy (smr_internal.h):
+// stencil row pair / quad b of column x lies in the 128-byte line of brick (x, y0 + b - b % DY,
+// iz - 1), element (b % DY) * 4 + kz, so the 4 lanes of an atom read aligned 64 B (fp32) or
+// 32 B (16-bit) pieces of it.
+template <int GDT>
+__device__ __forceinline__ void stencil_sums(const void* data, int brick, int nx, int ny, int nzs, int ix, int iy, int iz, int kz,
+                                             float PLx, float PLy, float PLz, const float bx[4], const float dxw[4],
+                                             const float by[4], const float dyw[4], float& sE, float& sX, float& sY) {
+    constexpr int DY = GDT == GRID_F32 ? 2 : 4;
+    const int x0 = imod(ix - 1, nx), y0 = imod(iy - 1, ny);
+    const int ystr = brick ? (nzs - 3) * DY * 4 : nzs;
+    const int nyz = ny * ystr;
+    int yo[4];
+#pragma unroll
+    for (int b = 0; b < 4; b++) {
+        const int yg = brick ? y0 + b - b % DY : y0 + b;
+        yo[b] = (yg >= ny ? yg - ny : yg) * ystr + (brick ? (b % DY) * 4 : 0);
+    }
+    const int zoff = brick ? (iz - 1) * DY * 4 + kz : iz - 1 + kz;
+#pragma unroll
+    for (int ax = 0; ax < 4; ax++) {
+        const int xg = x0 + ax;
+        const unsigned xo = (unsigned)(xg >= nx ? xg - nx : xg) * (unsigned)nyz + (unsigned)zoff;
+        float pE = 0.f, pY = 0.f;
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+            const float4 v = load_voxel<GDT>(data, (unsigned)xo + (unsigned)yo[b]);
+            const float cs = PLx * v.x + PLy * v.y + PLz * v.z;
+            pE += by[b] * cs; pY += dyw[b] * cs;
+        }
+        sE += bx[ax] * pE; sX += dxw[ax] * pE; sY += bx[ax] * pY;
+    }
+}
+
+
 // L2 prefetch of the brick lines of every atom's stencil (brick layout only): line l of an atom is
 // x column l / (NL / 4), y brick (l % (NL / 4)) * DY; one prefetch per line, lines spread over the team.
 // Cells are taken in FP32 (a line fetched for a cell the FP64 decision at a z bound moves is only
@@ -975,38 +1014,16 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
                     const float4 q = S.Q()[i];
                     const float ej = expf(a.alpha_morse * q.x);
                     float PLx = ej * ej * q.y, PLy = ej * q.y, PLz = q.z;
-                    // stored-value scales: per z plane (this lane reads one plane) or per channel
-                    const float4 zs = g.zscale ? __ldg(g.zscale + (iz - 1 + kz)) : make_float4(g.scale[0], g.scale[1], g.scale[2], 1.f);
-                    PLx *= zs.x; PLy *= zs.y; PLz *= zs.z;
-                    // 32-bit voxel indices (the host keeps grids below 2^31 voxels): column offsets of
-                    // the 4 x and 4 y stencil rows, wrapped periodically, then one add per voxel.
-                    // Brick copy (smr_internal.h): stencil row pair / quad b of column x lies in the
-                    // 128-byte line of brick (x, y0 + b - b % DY, iz - 1), element (b % DY) * 4 + kz,
-                    // so the 4 lanes of an atom read aligned 64 B (fp32) or 32 B (16-bit) pieces of it
-                    constexpr int DY = GDT == GRID_F32 ? 2 : 4;
-                    const int x0 = imod(ix - 1, g.nx), y0 = imod(iy - 1, g.ny);
-                    const int ystr = g.brick ? (g.nz - 3) * DY * 4 : g.nz;
-                    const int nyz = g.ny * ystr;
-                    int yo[4];
-#pragma unroll
-                    for (int b = 0; b < 4; b++) {
-                        const int yg = g.brick ? y0 + b - b % DY : y0 + b;
-                        yo[b] = (yg >= g.ny ? yg - g.ny : yg) * ystr + (g.brick ? (b % DY) * 4 : 0);
-                    }
-                    const int zoff = g.brick ? (iz - 1) * DY * 4 + kz : iz - 1 + kz;
                     float sE = 0.f, sX = 0.f, sY = 0.f;
-#pragma unroll
-                    for (int ax = 0; ax < 4; ax++) {
-                        const int xg = x0 + ax;
-                        const unsigned xo = (unsigned)(xg >= g.nx ? xg - g.nx : xg) * (unsigned)nyz + (unsigned)zoff;
-                        float pE = 0.f, pY = 0.f;
-#pragma unroll
-                        for (int b = 0; b < 4; b++) {
-                            const float4 v = load_voxel<GDT>(g.data, (unsigned)xo + (unsigned)yo[b]);
-                            const float cs = PLx * v.x + PLy * v.y + PLz * v.z;
-                            pE += by[b] * cs; pY += dyw[b] * cs;
-                        }
-                        sE += bx[ax] * pE; sX += dxw[ax] * pE; sY += bx[ax] * pY;
+                    if (GDT != GRID_F32 && iz - 1 < g.zsplit) {
+                        // a 16-bit grid's FP32 near-surface planes (the cell is uniform over the atom's lanes)
+                        PLx *= g.lo_scale[0]; PLy *= g.lo_scale[1]; PLz *= g.lo_scale[2];
+                        stencil_sums<GRID_F32>(g.lo, g.brick, g.nx, g.ny, g.lo_nz, ix, iy, iz, kz, PLx, PLy, PLz, bx, dxw, by, dyw, sE, sX, sY);
+                    } else {
+                        // stored-value scales: per z plane (this lane reads one plane) or per channel
+                        const float4 zs = g.zscale ? __ldg(g.zscale + (iz - 1 + kz)) : make_float4(g.scale[0], g.scale[1], g.scale[2], 1.f);
+                        PLx *= zs.x; PLy *= zs.y; PLz *= zs.z;
+                        stencil_sums<GDT>(g.data, g.brick, g.nx, g.ny, g.nz, ix, iy, iz, kz, PLx, PLy, PLz, bx, dxw, by, dyw, sE, sX, sY);
                     }
                     const float bzk = comp(make_float4(bz[0], bz[1], bz[2], bz[3]), kz);
                     const float dzk = comp(make_float4(dzw[0], dzw[1], dzw[2], dzw[3]), kz);

@@ -79,6 +79,13 @@ struct GridView {
     const float4* zscale;         // 16-bit grids: per z plane and channel scale (null: scale[])
     int brick;                    // 1: data is the brick copy (build_grid_bricks), not the z-fastest grid
     double p0z, stepz;            // z origin and step in FP64 (cell decisions at the grid's z bounds)
+    // 16-bit grids with FP32 near-surface planes (smr_convert_grid_split): a cell whose stencil
+    // starts below plane zsplit (iz - 1 < zsplit) reads the FP32 copy lo of the planes
+    // [0, lo_nz = zsplit + 3) instead, in the same layout as data (bricks or z-fastest), with
+    // the channel scales lo_scale; zsplit = 0: no copy
+    const void* lo;
+    int zsplit, lo_nz;
+    float lo_scale[4];
 };
 
 // folded-surface substrate (SurfaceFolded, crates/libs/surfff/src/lib.rs:126-351)
@@ -242,6 +249,8 @@ int grid_from_raw_device(const double* raw, int nx, int ny, int nz, float4* out_
 // floats (host); decode takes them as a device table
 int encode_grid_16(const float4* src, void* dst, size_t nvox, int nz, int dtype, float* plane_scale_out, cudaStream_t s);
 int decode_grid_16(const void* src, float4* dst, size_t nvox, int nz, int dtype, const float4* d_plane_scale, cudaStream_t s);
+// dst (nxy columns of nzl planes, z-fastest) = the planes [0, nzl) of src (nxy columns of nz planes)
+int extract_low_planes(const float4* src, size_t nxy, int nz, int nzl, float4* dst, cudaStream_t s);
 // Brick copy of a z-fastest grid for the relax kernel's stencil reads.  Brick (ix, iy, jz),
 // jz in [0, nz - 3), is one 128-byte line holding the voxels (iy + dy mod ny, jz + k), k < 4,
 // dy < grid_brick_rows(dtype) (2 rows of 16-byte float4 voxels, 4 rows of 8-byte 16-bit ones),

@@ -261,6 +261,27 @@ class RelaxMulti:
     def convert_grid(self, dtype):
         self._chk(self.L.smr_convert_grid(self.h, dtype), "smr_convert_grid")
 
+    def convert_grid_split(self, dtype, zsplit):
+        """The FP32 grid becomes a 16-bit grid plus an FP32 copy of its planes [0, zsplit + 3):
+        atoms whose stencil starts below plane zsplit read the FP32 copy."""
+        self._chk(self.L.smr_convert_grid_split(self.h, dtype, int(zsplit)), "smr_convert_grid_split")
+
+    def get_grid_split(self, planes=False):
+        """(zsplit, FP32 planes as an (nx, ny, zsplit + 3, 4) array or None)."""
+        zs = C.c_int()
+        self._chk(self.L.smr_get_grid_split(self.h, C.byref(zs), None), "smr_get_grid_split")
+        if not planes or zs.value == 0:
+            return zs.value, None
+        g = self.get_grid_dims()
+        lo = np.zeros((g[0], g[1], zs.value + 3, 4), np.float32)
+        self._chk(self.L.smr_get_grid_split(self.h, C.byref(zs), _p(lo, N.FP)), "smr_get_grid_split")
+        return zs.value, lo
+
+    def get_grid_dims(self):
+        dims = (C.c_int * 3)()
+        self._chk(self.L.smr_get_grid(self.h, None, None, None, dims, None, None), "smr_get_grid")
+        return tuple(dims)
+
     def set_surface_folded(self, surf):
         """Folded-surface substrate in place of the grid (a ``folded.FoldedSurface``, or None to go
         back to the grid): MolWorld's SurfaceFolded with its per-atom force clamp."""

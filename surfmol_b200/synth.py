@@ -6,8 +6,8 @@ for its inputs with the shapes of the relaxation configurations:
 * ``polyaromatic_40`` -- one 40-atom planar polyaromatic: a hexacene
   skeleton (26 ring sites at 1.40 A: 24 C + 2 pyridinic N on edge sites) with
   14 edge substituents (12 H at 1.09 A, 2 carbonyl O at 1.22 A).
-* ``ragged_molecule`` -- parallelogram hexagonal cores of a target size with
-  H capping, C:H:N:O near 60:30:5:5 (N pyridinic on edge sites, O carbonyl).
+* ``ragged_molecule`` -- compact convex hexagonal cores of a target size with
+  H capping, ~5 % N (pyridinic, edge sites) and ~5 % O (carbonyl).
 * ``rocksalt_slab`` -- (100) slab, a = 5.64 A, +-q ions, 4 ions per cell and
   layer, top layer at z = 0.
 
@@ -142,18 +142,66 @@ def polyaromatic_40(rng) -> Molecule:
     raise RuntimeError("could not generate the 40-atom polyaromatic")
 
 
-def ragged_molecule(rng, target: int) -> Molecule:
-    """Parallelogram core (1 or 2 hexagon rows) with H capping near ``target`` atoms.
+def convex_hexes(A: int, B: int, c1: int, c2: int):
+    """Axial hexagon centres of a convex benzenoid: the A x B parallelogram (0 <= q < A, 0 <= r < B)
+    without the corners q + r < c1 and q + r > c2.  Its edges are zigzag only (no bay, cove or
+    fjord regions), so with C-H = 1.09 A every non-bonded distance stays above 2.16 A."""
+    return [(q, r) for q in range(A) for r in range(B) if c1 <= q + r <= c2]
 
-    One row gives C:H ~ 2:1, two rows ~ 3:1; N (pyridinic, edge sites) and
-    carbonyl O each make ~5 % of the atoms."""
+
+def benzenoid_atoms(hexes) -> int:
+    """C + H of the benzenoid hydrocarbon on these hexagons: n_C = 4h + 2 - n_i, n_H = 2h + 4 - n_i,
+    n_i the carbons shared by three rings (one per triangle of mutually adjacent centres)."""
+    s = set(hexes)
+    ni = 0
+    for (q, r) in s:
+        if (q + 1, r) in s and (q, r + 1) in s:
+            ni += 1 + ((q + 1, r + 1) in s)
+    return 6 * len(s) + 6 - 2 * ni
+
+
+def _compact_shape(rng, target: int):
+    """A random convex benzenoid of about ``target`` atoms (C + H): aspect ratio log-uniform in
+    [1, 3], corner cuts uniform; its scale found by bisection on the atom count."""
+    rho = math.exp(rng.uniform(0.0, math.log(3.0)))
+    f1, f2 = rng.uniform(), rng.uniform()
+
+    def shape(sc):
+        A = max(1, int(round(sc * math.sqrt(rho))))
+        B = max(1, int(round(sc / math.sqrt(rho))))
+        m = min(A, B) - 1
+        c1, c2 = int(round(f1 * m)), A + B - 2 - int(round(f2 * m))
+        return A, B, c1, c2
+
+    lo, hi = 0.5, 2.0
+    while benzenoid_atoms(convex_hexes(*shape(hi))) < target:
+        hi *= 2.0
+    for _ in range(24):
+        mid = 0.5 * (lo + hi)
+        if benzenoid_atoms(convex_hexes(*shape(mid))) < target:
+            lo = mid
+        else:
+            hi = mid
+    a, b = shape(lo), shape(hi)
+    na, nb = benzenoid_atoms(convex_hexes(*a)), benzenoid_atoms(convex_hexes(*b))
+    return a if abs(na - target) <= abs(nb - target) else b
+
+
+def ragged_molecule(rng, target: int) -> Molecule:
+    """Compact hexagonal core with H capping near ``target`` atoms: a convex benzenoid (zigzag
+    edges, aspect ratio 1-3, corners cut at random, from benzene and acenes up to coronene-like
+    flakes), with ~5 % of the atoms pyridinic N on edge sites and ~5 % carbonyl O (together at
+    most a third of the edge sites).  Large flakes are carbon-rich: the edge, which carries every
+    H, N and O, grows like the square root of the size."""
     target = max(int(target), 12)
     for _ in range(1000):
-        B = 1 + int(rng.integers(2))
-        A = max(1, int(round((target - 6) / 6.0)) if B == 1 else int(round((target - 10) / 8.0)))
-        xy, adj = parallelogram_core(A, B)
-        tot = xy.shape[0] + int((adj.sum(1) == 2).sum())
-        m = _assemble(rng, xy, adj, n_N=int(round(0.05 * tot)), n_O=int(round(0.05 * tot)))
+        hexes = convex_hexes(*_compact_shape(rng, round(target / 0.95)))
+        xy, adj = _ring_graph(hexes)
+        nedge = int((adj.sum(1) == 2).sum())
+        tot = xy.shape[0] + nedge
+        # N and O each ~5 % of the atoms, together at most a third of the edge sites
+        n_sub = min(int(round(0.05 * tot)), nedge // 6)
+        m = _assemble(rng, xy, adj, n_N=n_sub, n_O=n_sub)
         if m is not None:
             return m
     raise RuntimeError("could not generate a ragged molecule")
