@@ -577,11 +577,19 @@ def run_ragged(args, ws, rank, local):
     hbm, peak_kind = peaks()
     grid_layout = "bricks" if R.grid_bricks_active() else "z-fastest"
     achieved = 1024.0 * atom_steps / args.steps / (ms_step * 1e-3) / 1e9
-    traffic = None
+    traffic, issue = None, None
     prof = os.path.join(ROOT, "profiles", f"relax_ragged_traffic_{grid_layout}.json")
     if os.path.exists(prof):
         pj = json.load(open(prof))
         traffic = pj["dram_bytes_per_atom_step"] * atom_steps / args.steps
+        # the bound the kernel actually meets: warp-instruction issue (ncu instructions per atom-step
+        # x atom-steps / time, against 4 schedulers x 148 SMs at the sampled SM clock)
+        mhz = clk.summary()["sm_mhz"] or 1965.0
+        if "warp_inst_per_atom_step" in pj:
+            rate = pj["warp_inst_per_atom_step"] * atom_steps / args.steps / (ms_step * 1e-3)
+            ipeak = 4 * 148 * mhz * 1e6
+            issue = {"achieved": rate, "peak": ipeak, "unit": "warp-instructions/s", "frac": rate / ipeak,
+                     "inst_per_atom_step": pj["warp_inst_per_atom_step"]}
     line = {"metric": METRIC, "value": value, "unit": "relaxed systems/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -598,7 +606,8 @@ def run_ragged(args, ws, rank, local):
                                                             "nb_lanes": tune.nb_lanes, "stages": tune.stages}},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "traffic": traffic, "peak_source": peak_kind,
-                         "algorithmic_bytes": "1024 B per atom-step (64 float4 grid voxels), state resident in shared memory"},
+                         "algorithmic_bytes": "1024 B per atom-step (64 float4 grid voxels), state resident in shared memory",
+                         "issue": issue},
             "e2e": {"value": conv_e2e / e2e_k / (t_e2e / e2e_k), "unit": "relaxed systems/s",
                     "h2d_bytes_per_step": int(16 * natoms.sum() + 76 * nsys), "d2h_bytes_per_step": int(16 * natoms.sum() + 128 * nsys)},
             "latency": {"batch_s": t_e2e / e2e_k},

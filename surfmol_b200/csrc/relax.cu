@@ -220,7 +220,6 @@ __device__ __forceinline__ void stencil_sums(const void* data, int brick, int nx
     }
 }
 
-
 // L2 prefetch of the brick lines of every atom's stencil (brick layout only): line l of an atom is
 // x column l / (NL / 4), y brick (l % (NL / 4)) * DY; one prefetch per line, lines spread over the team.
 // Cells are taken in FP32 (a line fetched for a cell the FP64 decision at a z bound moves is only
