@@ -370,6 +370,44 @@ __device__ __forceinline__ void nb_pair(const KernelArgs& a, float4 pi, float4 l
     ljq_pair(dx, dy, dz, excluded || out, qi, qj, a.R2damp, fx, fy, fz, E);
 }
 
+// Four pairs of atom i (partners j[k], exclusion flags ex[k]) added in the order k = 0..3, as four
+// nb_pair calls add them.  The FP64 cutoff decision is taken for the four behind one branch that
+// is almost never taken: with a branch per pair the compiler keeps each pair's arithmetic in its
+// own block and the pairs no longer overlap (measured: the per-pair form costs ~10 % of the step).
+template <bool CUT>
+__device__ __forceinline__ void nb_quad(const KernelArgs& a, const Smem& S, float4 pi, float4 li, float4 qi, const int j[4],
+                                        const bool ex[4], float& fx, float& fy, float& fz, float& E) {
+    float4 pj[4], lj[4], qj[4];
+    float dx[4], dy[4], dz[4];
+    bool out[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        pj[k] = S.P()[j[k]]; lj[k] = S.Lo()[j[k]]; qj[k] = S.Q()[j[k]];
+        dx[k] = (pj[k].x - pi.x) + (lj[k].x - li.x);
+        dy[k] = (pj[k].y - pi.y) + (lj[k].y - li.y);
+        dz[k] = (pj[k].z - pi.z) + (lj[k].z - li.z);
+        out[k] = false;
+    }
+    if (CUT) {
+        float r2[4];
+        bool band = false;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            r2[k] = dx[k] * dx[k] + dy[k] * dy[k] + dz[k] * dz[k];
+            out[k] = r2[k] > a.rc2;
+            band |= fabsf(r2[k] - a.rc2) < 1e-4f * a.rc2;
+        }
+        // at the cutoff: decide in FP64, so FP32 rounding never moves a pair across it
+        if (band) {
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                if (fabsf(r2[k] - a.rc2) < 1e-4f * a.rc2) out[k] = beyond_cutoff_fp64(pi, li, pj[k], lj[k], a.rc2);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) ljq_pair(dx[k], dy[k], dz[k], ex[k] || out[k], qi, qj[k], a.R2damp, fx, fy, fz, E);
+}
+
 // ------------------------------------------------------------------ periodic systems
 __device__ __forceinline__ int cell_f(int c, int k) { const int v = (c >> (4 * k)) & 15; return v >= 8 ? v - 16 : v; }
 
@@ -894,11 +932,16 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
                     for (int e = cp * 4; e < cnt; e += Lp * 4) {
                         const ushort4 v = row4[e >> 2];
                         const bool ok1 = e + 1 < cnt, ok2 = e + 2 < cnt, ok3 = e + 3 < cnt;
-                        const int j0 = v.x, j1 = ok1 ? (int)v.y : i, j2 = ok2 ? (int)v.z : i, j3 = ok3 ? (int)v.w : i;
-                        nb_pair<CUT>(a, pi, li, qi, S.P()[j0], S.Lo()[j0], S.Q()[j0], false, fx, fy, fz, E);
-                        nb_pair<CUT>(a, pi, li, qi, S.P()[j1], S.Lo()[j1], S.Q()[j1], !ok1, fx, fy, fz, E);
-                        nb_pair<CUT>(a, pi, li, qi, S.P()[j2], S.Lo()[j2], S.Q()[j2], !ok2, fx, fy, fz, E);
-                        nb_pair<CUT>(a, pi, li, qi, S.P()[j3], S.Lo()[j3], S.Q()[j3], !ok3, fx, fy, fz, E);
+                        const int jq[4] = {(int)v.x, ok1 ? (int)v.y : i, ok2 ? (int)v.z : i, ok3 ? (int)v.w : i};
+                        const bool xq[4] = {false, !ok1, !ok2, !ok3};
+                        if (T == 32) {
+                            // warp teams (72 registers): pair by pair, the grouped form spills
+#pragma unroll
+                            for (int k = 0; k < 4; k++)
+                                nb_pair<CUT>(a, pi, li, qi, S.P()[jq[k]], S.Lo()[jq[k]], S.Q()[jq[k]], xq[k], fx, fy, fz, E);
+                        } else {
+                            nb_quad<CUT>(a, S, pi, li, qi, jq, xq, fx, fy, fz, E);
+                        }
                     }
                 } else {
                     const short4 ng = S.Ng()[i];
@@ -923,10 +966,27 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
                             }
                         }
                     } else {
+                        if (T == 32) {
+                            // warp teams (72 registers): pair by pair, the grouped form spills
 #pragma unroll 4
-                        for (int j = cp; j < N; j += Lp) {
-                            const bool excl = small ? (bool)((ex >> j) & 1ull) : (j == i || j == ng.x || j == ng.y || j == ng.z || j == ng.w);
-                            nb_pair<CUT>(a, pi, li, qi, S.P()[j], S.Lo()[j], S.Q()[j], excl, fx, fy, fz, E);
+                            for (int j = cp; j < N; j += Lp) {
+                                const bool excl = small ? (bool)((ex >> j) & 1ull) : (j == i || j == ng.x || j == ng.y || j == ng.z || j == ng.w);
+                                nb_pair<CUT>(a, pi, li, qi, S.P()[j], S.Lo()[j], S.Q()[j], excl, fx, fy, fz, E);
+                            }
+                        } else
+                        // partners j = cp, cp + Lp, ... in groups of four; slots past N take the atom
+                        // itself, excluded (they add exactly 0)
+                        for (int j0 = cp; j0 < N; j0 += 4 * Lp) {
+                            int jq[4];
+                            bool xq[4];
+#pragma unroll
+                            for (int k = 0; k < 4; k++) {
+                                const int j = j0 + k * Lp;
+                                const bool in = j < N;
+                                jq[k] = in ? j : i;
+                                xq[k] = !in || (small ? (bool)((ex >> j) & 1ull) : (j == i || j == ng.x || j == ng.y || j == ng.z || j == ng.w));
+                            }
+                            nb_quad<CUT>(a, S, pi, li, qi, jq, xq, fx, fy, fz, E);
                         }
                     }
                 }

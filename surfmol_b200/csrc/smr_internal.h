@@ -220,11 +220,13 @@ enum KernelForm { FORM_ROUNDS = 0, FORM_GATHER = 1, FORM_OWNER = 2, FORM_GATHER_
 int launch_relax(const KernelArgs& a, int team, int form, int eval_only, cudaStream_t s, int num_sms, long long* launches);
 size_t team_smem_bytes(int nmax, int nfmax, int team, int form);
 // Minimum blocks per SM the relax kernel's __launch_bounds__ asks for: warp teams run 4 to a
-// 128-thread block at 72 registers (80 in the owner form), 7 (6) blocks; block teams take the
-// registers the compiler wants (measured: capping them at 128 or 96 for more resident teams
-// made the ragged workload 11-25 % slower, the extra teams thrashing L1 on their global reads).
+// 128-thread block at 72 registers (80 in the owner form), 7 (6) blocks; 64- and 128-thread teams
+// get the occupancy their shared memory allows for typical sizes (6 blocks up to 160 atoms, 3 up
+// to 448), i.e. at most 168 registers, which the NB loop's grouped pairs would otherwise exceed
+// (~187).  Lower caps for more resident teams were measured: 128 or 96 registers made the ragged
+// workload 11-25 % slower, the extra teams thrashing L1 on their global reads.
 constexpr int relax_min_blocks(int T, int form) {
-    return T == 32 ? (form == FORM_OWNER ? 6 : 7) : 1;
+    return T == 32 ? (form == FORM_OWNER ? 6 : 7) : T == 64 ? 6 : T == 128 ? 3 : 1;
 }
 // Blocks of one launch segment that fit on an SM by shared memory (228 KB per SM, 1 KB reserved
 // per block), capped at 16 (the occupancy tiers of group_by).
