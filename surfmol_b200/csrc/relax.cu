@@ -923,26 +923,34 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
                 qi.z *= kCoulomb;                     // ljq_pair takes kCoulomb * Q_i
                 const int cnt = use_list ? a.nbl_cnt[ga0 + i] : -1;
                 if (cnt >= 0) {
-                    // partners within rc + skin, ascending; exclusions were removed at the build.
-                    // Lane cp takes runs of 4 consecutive partners, one 8-byte load each (rows
-                    // start on 512-byte boundaries); entries past the count weigh 0 and index the
-                    // atom itself, so a stale slot of the row is never dereferenced
+                    // partners within rc + skin; exclusions were removed at the build.  Lane cp takes
+                    // runs of 4 entries, one 8-byte load each (rows start on 512-byte boundaries);
+                    // entries outside a run's count weigh 0 and index the atom itself, so a stale
+                    // slot of the row is never dereferenced.  Inner partners (front of the row)
+                    // stay inside the cutoff until the next rebuild: no cutoff test.  Shell partners
+                    // (back of the row) take the full test.
                     const ushort4* row4 = reinterpret_cast<const ushort4*>(a.nbl + (ga0 + i) * (size_t)a.nbl_cap);
-#pragma unroll 2
-                    for (int e = cp * 4; e < cnt; e += Lp * 4) {
+                    const int nin = cnt & 0xffff, nsh = cnt >> 16;
+                    auto run4 = [&](int e, int lo, int hi, auto cut_run) {
                         const ushort4 v = row4[e >> 2];
-                        const bool ok1 = e + 1 < cnt, ok2 = e + 2 < cnt, ok3 = e + 3 < cnt;
-                        const int jq[4] = {(int)v.x, ok1 ? (int)v.y : i, ok2 ? (int)v.z : i, ok3 ? (int)v.w : i};
-                        const bool xq[4] = {false, !ok1, !ok2, !ok3};
+                        const bool ok0 = e >= lo && e < hi, ok1 = e + 1 >= lo && e + 1 < hi;
+                        const bool ok2 = e + 2 >= lo && e + 2 < hi, ok3 = e + 3 >= lo && e + 3 < hi;
+                        const int jq[4] = {ok0 ? (int)v.x : i, ok1 ? (int)v.y : i, ok2 ? (int)v.z : i, ok3 ? (int)v.w : i};
+                        const bool xq[4] = {!ok0, !ok1, !ok2, !ok3};
+                        constexpr bool C = decltype(cut_run)::value;
                         if (T == 32) {
                             // warp teams (72 registers): pair by pair, the grouped form spills
 #pragma unroll
                             for (int k = 0; k < 4; k++)
-                                nb_pair<CUT>(a, pi, li, qi, S.P()[jq[k]], S.Lo()[jq[k]], S.Q()[jq[k]], xq[k], fx, fy, fz, E);
+                                nb_pair<C>(a, pi, li, qi, S.P()[jq[k]], S.Lo()[jq[k]], S.Q()[jq[k]], xq[k], fx, fy, fz, E);
                         } else {
-                            nb_quad<CUT>(a, S, pi, li, qi, jq, xq, fx, fy, fz, E);
+                            nb_quad<C>(a, S, pi, li, qi, jq, xq, fx, fy, fz, E);
                         }
-                    }
+                    };
+#pragma unroll 2
+                    for (int e = cp * 4; e < nin; e += Lp * 4) run4(e, 0, nin, std::integral_constant<bool, false>{});
+                    const int s0 = (a.nbl_cap - nsh) & ~3;
+                    for (int e = s0 + cp * 4; e < a.nbl_cap; e += Lp * 4) run4(e, a.nbl_cap - nsh, a.nbl_cap, std::integral_constant<bool, CUT>{});
                 } else {
                     const short4 ng = S.Ng()[i];
                     unsigned long long ex = 1ull << (i & 63);
@@ -1104,33 +1112,44 @@ __device__ void eval_forces(const KernelArgs& a, const Smem& S, const TopoDev* _
 #undef TP
 
 // ------------------------------------------------------------------ NB neighbour lists
-// Rows of partners within rc + skin in ascending order, one warp per atom: lane c tests partner
-// j0 + c and a ballot places the accepted ones.  Rows longer than nbl_cap mark the atom -2 (all
-// pairs).  Also records each atom's position at the build.
+// Rows of partners within rc + skin, one warp per atom: lane c tests partner j0 + c and ballots
+// place the accepted ones.  A row holds two runs: from its front, in ascending order, the inner
+// partners, those closer than rc - skin - 0.01 A, which stay inside the cutoff until the next
+// rebuild (each atom moves at most skin / 2 before one), so their pairs need no cutoff test; from
+// its back, in ascending order towards the front, the shell partners.  The count packs
+// inner | shell << 16; rows longer than nbl_cap mark the atom -2 (all pairs).  Also records each
+// atom's position at the build.
 template <int T>
 __device__ void build_nblist(const KernelArgs& a, const Smem& S, int N, size_t ga0, int rank) {
     const int lane = rank & 31, warp = rank >> 5;
     const float rl = sqrtf(a.rc2) + a.nbl_skin, rl2 = rl * rl;
+    const float ri = sqrtf(a.rc2) - a.nbl_skin - 0.01f, ri2 = ri > 0.f ? ri * ri : -1.f;
+    const int cap = a.nbl_cap;
     for (int i = warp; i < N; i += T / 32) {
         const float4 pi = S.P()[i], li = S.Lo()[i];
         const short4 ng = S.Ng()[i];
-        unsigned short* row = a.nbl + (ga0 + i) * (size_t)a.nbl_cap;
-        int base = 0;
+        unsigned short* row = a.nbl + (ga0 + i) * (size_t)cap;
+        int nin = 0, nsh = 0;
         for (int j0 = 0; j0 < N; j0 += 32) {
             const int j = j0 + lane;
-            bool inc = false;
+            bool inc = false, inner = false;
             if (j < N && j != i && j != ng.x && j != ng.y && j != ng.z && j != ng.w) {
                 const float4 pj = S.P()[j], lj = S.Lo()[j];
                 const float dx = (pj.x - pi.x) + (lj.x - li.x), dy = (pj.y - pi.y) + (lj.y - li.y), dz = (pj.z - pi.z) + (lj.z - li.z);
-                inc = dx * dx + dy * dy + dz * dz < rl2;
+                const float d2 = dx * dx + dy * dy + dz * dz;
+                inc = d2 < rl2;
+                inner = d2 < ri2;
             }
-            const unsigned m = __ballot_sync(FULL, inc);
-            const int pos = base + __popc(m & ((1u << lane) - 1u));
-            if (inc && pos < a.nbl_cap) row[pos] = (unsigned short)j;
-            base += __popc(m);
+            const unsigned below = (1u << lane) - 1u;
+            const unsigned mi = __ballot_sync(FULL, inner), ms = __ballot_sync(FULL, inc && !inner);
+            const int qi = nin + __popc(mi & below), qs = nsh + __popc(ms & below);
+            if (inner && qi < cap) row[qi] = (unsigned short)j;
+            else if (inc && !inner && qs < cap) row[cap - 1 - qs] = (unsigned short)j;
+            nin += __popc(mi);
+            nsh += __popc(ms);
         }
         if (lane == 0) {
-            a.nbl_cnt[ga0 + i] = base <= a.nbl_cap ? base : -2;
+            a.nbl_cnt[ga0 + i] = nin + nsh <= cap ? (nin | nsh << 16) : -2;
             a.nbl_ref[ga0 + i] = make_float4(pi.x + li.x, pi.y + li.y, pi.z + li.z, 0.f);
         }
     }
