@@ -155,8 +155,7 @@ def benzenoid_atoms(hexes) -> int:
     s = set(hexes)
     ni = 0
     for (q, r) in s:
-        if (q + 1, r) in s and (q, r + 1) in s:
-            ni += 1 + ((q + 1, r + 1) in s)
+        ni += ((q + 1, r) in s and (q, r + 1) in s) + ((q - 1, r) in s and (q, r - 1) in s)
     return 6 * len(s) + 6 - 2 * ni
 
 
@@ -195,7 +194,8 @@ def ragged_molecule(rng, target: int) -> Molecule:
     H, N and O, grows like the square root of the size."""
     target = max(int(target), 12)
     for _ in range(1000):
-        hexes = convex_hexes(*_compact_shape(rng, round(target / 0.95)))
+        # the pyridinic N (about 3 % of the atoms) replace edge CH: aim the core that much higher
+        hexes = convex_hexes(*_compact_shape(rng, round(target / 0.97)))
         xy, adj = _ring_graph(hexes)
         nedge = int((adj.sum(1) == 2).sum())
         tot = xy.shape[0] + nedge
