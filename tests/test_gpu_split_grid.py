@@ -6,7 +6,7 @@ those of the 16-bit grid above it, in the z-fastest layout and through the brick
 import numpy as np
 import pytest
 
-from tests.gpu_helpers import F_RTOL, small_slab_grid, build_device_grid, decode, molecule_on_slab
+from tests.gpu_helpers import F_RTOL, small_slab_grid, build_device_grid, molecule_on_slab
 
 pytestmark = pytest.mark.gpu
 
@@ -108,3 +108,36 @@ def test_split_grid_rejects_bad_requests(R):
     with pytest.raises(SmrError):
         R.convert_grid_split(1, 5)                   # needs an FP32 grid
     build_device_grid(R, slab, dims, p0, step, dtype=0)
+
+
+def test_graph_replay_follows_the_split(R):
+    """With graph replay on, relaxing on the plain 16-bit grid and then on its split form gives the
+    split form's own trajectory (the launch plan includes the FP32 copy, so the first plan's graph is
+    not replayed), and repeating the split call replays it bit for bit."""
+    slab, dims, p0, step = small_slab_grid(ncell=1, nlayers=2, nxy=20, nz=40, dz=0.25)
+    rng = np.random.default_rng(91)
+    mols = [molecule_on_slab(rng, n, slab, height=h) for n, h in ((40, 2.8), (60, 3.2))]
+    tids = [R.add_molecule(Z, P, q) for Z, P, q in mols]
+    slots = R.add_systems(tids, [m[1] for m in mols])
+    out = {}
+    try:
+        for graph in (False, True):
+            R.set_graph(graph)
+            for mode in ("f16", "split", "split"):
+                build_device_grid(R, slab, dims, p0, step, dtype=0)
+                if mode == "f16":
+                    R.convert_grid(1)
+                else:
+                    R.convert_grid_split(1, 20)
+                R.set_positions(slots, [m[1] for m in mols])
+                R.reset_fire(slots)
+                R.run_fire(60, step_budget=60, fconv=1e-9)
+                out.setdefault((graph, mode), []).append(R.download(slots)["pos"])
+        ref = out[(False, "split")][0]
+        for pos in out[(True, "split")] + out[(False, "split")][1:]:
+            for k in range(len(mols)):
+                assert np.array_equal(pos[k], ref[k])
+        assert any(not np.array_equal(out[(True, "f16")][0][k], ref[k]) for k in range(len(mols)))
+    finally:
+        R.set_graph(False)
+        R.remove_systems(slots)
